@@ -1,0 +1,139 @@
+/* C-ABI of the B200 slab Foldy-Lax solver (libmsc_b200.so).
+ *
+ * Solves (I - G0 T0) psi = psi0 for an M x M x N_z lattice of cubes, the
+ * operator of tmnestor/MultipleScatteringCalculations
+ * cubic_scattering/slab_scattering.py and slab_scattering_gpu.py.
+ *
+ * Conventions (the reference's): axis order (z, x, y), z down; 9 DOF per voxel
+ * [u_z, u_x, u_y, e_zz, e_xx, e_yy, 2e_xy, 2e_zy, 2e_zx]; fields are complex
+ * arrays laid out psi[N_z][M][M][9] (C order); `a` is the cube half-width.
+ *
+ * All pointers to arrays are DEVICE pointers on the plan's device unless stated.
+ * Complex numbers are (re, im) pairs: complex128 = 2 doubles, complex64 = 2 floats.
+ * Work is enqueued on the plan's stream; functions that return results to host
+ * memory (statistics, R_PP) synchronise that stream. Plans are not thread safe.
+ * Every function returns MSC_OK (0), a positive warning status, or a negative
+ * error status; msc_status_string() names it and msc_last_error() explains it.
+ */
+#ifndef MSC_H
+#define MSC_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum msc_status {
+  MSC_OK = 0,
+  MSC_NOT_CONVERGED = 1,     /* iteration limit reached above tolerance (reference: warnings.warn) */
+  MSC_BREAKDOWN = 2,         /* Krylov breakdown before convergence */
+  MSC_ERR_INVALID = -1,      /* invalid argument (reference: ValueError) */
+  MSC_ERR_UNSUPPORTED = -2,  /* size whose FFT length has a prime factor > 11 */
+  MSC_ERR_CUDA = -3,         /* CUDA runtime error */
+  MSC_ERR_NOMEM = -4,        /* device allocation failed */
+  MSC_ERR_STATE = -5,        /* call out of order (e.g. matvec before build_t0/build_g0) */
+  MSC_ERR_NONFINITE = -6     /* NaN/Inf met in the solve */
+};
+
+enum msc_precision { MSC_COMPLEX64 = 0, MSC_COMPLEX128 = 1 };
+enum msc_solver_precision { MSC_SOLVE_MIXED = 0, MSC_SOLVE_FP64 = 1 };
+enum msc_wave { MSC_WAVE_P = 0, MSC_WAVE_S = 1 };
+
+typedef struct msc_slab_desc {
+  int32_t M;         /* lateral cubes per side (SlabGeometry.M) */
+  int32_t N_z;       /* layers (SlabGeometry.N_z) */
+  double a;          /* cube half-width (SlabGeometry.a) */
+  double alpha;      /* background P speed (ReferenceMedium.alpha) */
+  double beta;       /* background S speed (ReferenceMedium.beta) */
+  double rho;        /* background density (ReferenceMedium.rho) */
+  int32_t periodic;  /* 1 = circular convolution over M x M (reference periodic=True) */
+  int32_t Lz;        /* padded z FFT length, 0 = automatic (>= 2 N_z - 1) */
+  int32_t Lxy;       /* padded lateral FFT length, 0 = automatic (>= 2M - 1; ignored if periodic) */
+} msc_slab_desc;
+
+typedef struct msc_solve_opts {
+  double tol;             /* relative residual target ||b - A x|| / ||b|| (gmres_tol) */
+  int32_t max_iter;       /* matvec budget (max_iter) */
+  int32_t restart;        /* GMRES restart length m (reference CPU path: scipy default 20) */
+  int32_t precision;      /* msc_solver_precision */
+  int32_t initial_guess;  /* 0 = Born (x0 = psi0), 1 = zero */
+  double inner_tol;       /* mixed precision: relative tolerance of each complex64 inner solve (0 = default) */
+} msc_solve_opts;
+
+typedef struct msc_solve_stats {
+  int32_t n_matvec;      /* operator applications of all precisions (reference: n_gmres_iter) */
+  int32_t n_matvec64;    /* of which complex128 */
+  int32_t n_outer;       /* refinement sweeps (mixed) or restart cycles (fp64) */
+  int32_t status;        /* msc_status of the solve */
+  double residual;       /* true relative residual in FP64 (reference: gmres_residual) */
+} msc_solve_stats;
+
+typedef struct msc_plan msc_plan;
+
+/* Create a plan for one slab geometry on the current CUDA device. `stream` is a
+ * cudaStream_t (NULL = legacy default stream). Replaces the setup of
+ * compute_slab_scattering_gpu (slab_scattering_gpu.py:158-226). */
+int msc_plan_create(const msc_slab_desc* desc, void* stream, msc_plan** plan);
+int msc_plan_destroy(msc_plan* plan);
+int msc_plan_set_stream(msc_plan* plan, void* stream);
+/* Padded FFT sizes chosen by the plan: out[0..2] = (Lz, Lx, Ly). */
+int msc_plan_fft_sizes(const msc_plan* plan, int32_t* out3);
+/* Device bytes currently held by the plan. */
+int64_t msc_plan_device_bytes(const msc_plan* plan);
+
+/* Per-voxel T0 from the contrasts dlam, dmu, drho (device, float64, N_z*M*M each,
+ * (N_z, M, M) C order) at angular frequency omega. Replaces compute_slab_tmatrices
+ * (slab_scattering.py:169-205) with compute_cube_tmatrix (effective_contrasts.py:454-532)
+ * and _sub_cell_tmatrix_9x9 (resonance_tmatrix.py:461-487). */
+int msc_build_t0(msc_plan* plan, const double* dlam, const double* dmu, const double* drho, double omega);
+/* T0 as 4 complex scalars per voxel, out (4, N_z, M, M) complex128 (device):
+ * T0 = diag(t_u I3, [t_l + t_d delta_ij] on the normal strains, t_s I3 on the shears). */
+int msc_t0_scalars(const msc_plan* plan, void* out);
+
+/* Set T0 directly from 4 complex scalars per voxel (the layout of msc_t0_scalars),
+ * e.g. extracted from user-supplied 9x9 T-matrices (reference T_local arrays). */
+int msc_set_t0_scalars(msc_plan* plan, const void* t4, double omega);
+
+/* G0 spectrum at omega. kpar = NULL: the reference's fold (periodic) or the plain
+ * linear convolution (aperiodic); kpar = 2 doubles (k_x, k_y): Bloch-phased periodic
+ * fold (the field is solved in the demodulated frame psi exp(-i k_par.x)).
+ * volume_averaged/n_orders as the reference. Replaces _build_slab_kernels
+ * (slab_scattering.py:267-351) and _build_slab_kernels_gpu (slab_scattering_gpu.py:34-92). */
+int msc_build_g0(msc_plan* plan, double omega, const double* kpar, int volume_averaged, int n_orders);
+
+/* Incident plane wave psi0 (complex128, (N_z, M, M, 9), device). Replaces
+ * _build_slab_incident_field (slab_scattering.py:426-478). */
+int msc_incident(msc_plan* plan, double omega, const double* k_hat, int wave_type, void* psi0);
+
+/* y = (I - G0 T0) x for x, y (N_z, M, M, 9) complex of the given precision
+ * (msc_precision). Replaces _slab_matvec_gpu (slab_scattering_gpu.py:95-155) and
+ * _slab_matvec (slab_scattering.py:359-418). x and y may not alias. */
+int msc_matvec(msc_plan* plan, const void* x, void* y, int precision);
+
+/* Solve (I - G0 T0) x = b; b, x complex128 (N_z, M, M, 9). Restarted GMRES with
+ * CGS2 Arnoldi and FP64 Givens/least squares; precision MIXED runs complex64
+ * inner solves inside FP64 iterative refinement. Replaces torch_gmres
+ * (torch_gmres.py:83-205) and the scipy gmres call (slab_scattering.py:539-552).
+ * Non-convergence returns MSC_NOT_CONVERGED with x the best iterate. */
+int msc_solve(msc_plan* plan, const void* b, void* x, const msc_solve_opts* opts, msc_solve_stats* stats);
+
+/* Specular periodic R_PP (host out[2] = re, im) of psi (complex128, device).
+ * bloch = 1 demodulates the sources by exp(-i k_par.x), k_par the plan's Bloch wavevector.
+ * Replaces slab_rpp_periodic (slab_scattering.py:672-735). */
+int msc_rpp_periodic(msc_plan* plan, const void* psi, double omega, double p, int bloch, double* out);
+
+/* Reflected far-field amplitudes (host out[6] = R_PP, R_PS, R_SP as re, im).
+ * Replaces slab_reflected_field (slab_scattering.py:589-669). */
+int msc_reflected_field(msc_plan* plan, const void* psi, double omega, const double* k_hat, double* out);
+
+const char* msc_status_string(int status);
+/* Message of the last error on this thread. */
+const char* msc_last_error(void);
+/* Library version string. */
+const char* msc_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* MSC_H */

@@ -1,0 +1,310 @@
+// C-ABI entry points of libmsc_b200.so (declared in include/msc.h).
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+
+#include "plan.cuh"
+
+namespace msc {
+
+static thread_local char g_err[512] = "";
+
+void set_error(const char* fmt, ...) {
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(g_err, sizeof(g_err), fmt, ap);
+  va_end(ap);
+}
+
+int dalloc(msc_plan* pl, DBuf& b, size_t bytes) {
+  if (b.p && b.bytes >= bytes) return MSC_OK;
+  if (b.p) dfree(pl, b);
+  if (bytes == 0) bytes = 16;
+  void* p = nullptr;
+  cudaError_t e = cudaMalloc(&p, bytes);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    set_error("cudaMalloc of %zu bytes failed: %s", bytes, cudaGetErrorString(e));
+    return MSC_ERR_NOMEM;
+  }
+  b.p = p;
+  b.bytes = bytes;
+  pl->bytes += (int64_t)bytes;
+  return MSC_OK;
+}
+
+void dfree(msc_plan* pl, DBuf& b) {
+  if (b.p) {
+    cudaFree(b.p);
+    pl->bytes -= (int64_t)b.bytes;
+  }
+  b.p = nullptr;
+  b.bytes = 0;
+}
+
+// Multiply an SoA field by exp(sign * i k_par . x) at the cube centres.
+__global__ void k_bloch(double2* v, int M, int nsite, double a, double kx, double ky, int sign) {
+  const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= 9LL * nsite) return;
+  const int s = (int)(e % nsite);
+  const int j = s % M, i = (s / M) % M;
+  const double d = 2.0 * a;
+  const double x = (i - (M - 1) / 2.0) * d, y = (j - (M - 1) / 2.0) * d;
+  double sn, cs;
+  sincos(sign * (kx * x + ky * y), &sn, &cs);
+  v[e] = v[e] * make_double2(cs, sn);
+}
+
+__global__ void k_narrow(const double2* __restrict__ a, float2* __restrict__ b, size_t n) {
+  const size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e < n) b[e] = make_float2((float)a[e].x, (float)a[e].y);
+}
+
+int launch_narrow(msc_plan* pl, const double2* a, float2* b, size_t n) {
+  k_narrow<<<ceil_div((long long)n, 256), 256, 0, pl->stream>>>(a, b, n);
+  MSC_CUDA(cudaGetLastError());
+  return MSC_OK;
+}
+
+int bloch_modulate(msc_plan* pl, double2* v, int sign) {
+  const Geo& g = pl->g;
+  k_bloch<<<ceil_div(9LL * g.nsite, 256), 256, 0, pl->stream>>>(v, g.M, g.nsite, pl->desc.a, pl->kpar[0], pl->kpar[1],
+                                                                sign);
+  MSC_CUDA(cudaGetLastError());
+  return MSC_OK;
+}
+
+// Smallest FFT length >= n whose factors are 2, 3, 5, 7.
+static int nice_length(int n) {
+  for (int L = std::max(n, 1);; ++L) {
+    int r = L;
+    for (int p : {2, 3, 5, 7})
+      while (r % p == 0) r /= p;
+    if (r == 1) return L;
+  }
+}
+
+}  // namespace msc
+
+using namespace msc;
+
+extern "C" {
+
+const char* msc_status_string(int s) {
+  switch (s) {
+    case MSC_OK: return "MSC_OK";
+    case MSC_NOT_CONVERGED: return "MSC_NOT_CONVERGED";
+    case MSC_BREAKDOWN: return "MSC_BREAKDOWN";
+    case MSC_ERR_INVALID: return "MSC_ERR_INVALID";
+    case MSC_ERR_UNSUPPORTED: return "MSC_ERR_UNSUPPORTED";
+    case MSC_ERR_CUDA: return "MSC_ERR_CUDA";
+    case MSC_ERR_NOMEM: return "MSC_ERR_NOMEM";
+    case MSC_ERR_STATE: return "MSC_ERR_STATE";
+    case MSC_ERR_NONFINITE: return "MSC_ERR_NONFINITE";
+    default: return "MSC_UNKNOWN";
+  }
+}
+
+const char* msc_last_error(void) { return g_err; }
+const char* msc_version(void) { return "msc_b200 0.1.0 (sm_100a)"; }
+
+int msc_plan_create(const msc_slab_desc* d, void* stream, msc_plan** out) {
+  if (!d || !out) {
+    set_error("null argument");
+    return MSC_ERR_INVALID;
+  }
+  *out = nullptr;
+  if (d->M < 1) { set_error("M must be >= 1, got %d", d->M); return MSC_ERR_INVALID; }
+  if (d->N_z < 1) { set_error("N_z must be >= 1, got %d", d->N_z); return MSC_ERR_INVALID; }
+  if (!(d->a > 0)) { set_error("a must be > 0, got %g", d->a); return MSC_ERR_INVALID; }
+  if (!(d->alpha > 0) || !(d->beta > 0) || !(d->rho > 0)) {
+    set_error("alpha, beta, rho must be positive");
+    return MSC_ERR_INVALID;
+  }
+  if (!(d->alpha > d->beta)) {
+    set_error("alpha must exceed beta (Poisson ratio below 1/2)");
+    return MSC_ERR_INVALID;
+  }
+  const long long nsite = (long long)d->N_z * d->M * d->M;
+  if (9LL * nsite >= (1LL << 31)) {
+    set_error("lattice too large: 9*N_z*M*M must be < 2^31");
+    return MSC_ERR_INVALID;
+  }
+  msc_plan* pl = new msc_plan();
+  pl->desc = *d;
+  pl->stream = (cudaStream_t)stream;
+  cudaGetDevice(&pl->device);
+  Geo& g = pl->g;
+  g.M = d->M;
+  g.Nz = d->N_z;
+  g.nsite = (int)nsite;
+  int Lz = d->Lz > 0 ? d->Lz : nice_length(2 * d->N_z - 1);
+  if (Lz < 2 * d->N_z - 1) {
+    delete pl;
+    set_error("Lz=%d is below 2*N_z-1=%d", Lz, 2 * d->N_z - 1);
+    return MSC_ERR_INVALID;
+  }
+  int Lxy;
+  if (d->periodic) Lxy = d->M;
+  else {
+    Lxy = d->Lxy > 0 ? d->Lxy : nice_length(2 * d->M - 1);
+    if (Lxy < 2 * d->M - 1) {
+      delete pl;
+      set_error("Lxy=%d is below 2*M-1=%d", Lxy, 2 * d->M - 1);
+      return MSC_ERR_INVALID;
+    }
+  }
+  g.Lz = Lz;
+  g.Lx = g.Ly = Lxy;
+  g.Hy = Lxy / 2 + 1;
+  g.half = 1;
+  if (!make_fft_plan(Lz, &pl->fz) || !make_fft_plan(Lxy, &pl->fxy)) {
+    delete pl;
+    set_error("FFT lengths (Lz=%d, Lxy=%d) need prime factors <= 11 and length <= 4096", Lz, Lxy);
+    return MSC_ERR_UNSUPPORTED;
+  }
+  // shared memory of the column kernel: (Lz + Lz*(2*9*8+1)) complex128
+  if ((size_t)(Lz + (size_t)Lz * 145) * 16 > 227 * 1024) {
+    delete pl;
+    set_error("Lz=%d exceeds the column kernel's shared memory (N_z <= 48)", Lz);
+    return MSC_ERR_UNSUPPORTED;
+  }
+  int s = build_twiddles(pl);
+  if (s == MSC_OK) s = dalloc(pl, pl->W64, sizeof(double2) * ws_elems(g));
+  if (s == MSC_OK) s = dalloc(pl, pl->W32, sizeof(float2) * ws_elems(g));
+  if (s != MSC_OK) {
+    msc_plan_destroy(pl);
+    return s;
+  }
+  *out = pl;
+  return MSC_OK;
+}
+
+int msc_plan_destroy(msc_plan* pl) {
+  if (!pl) return MSC_OK;
+  if (pl->stream) cudaStreamSynchronize(pl->stream);
+  else cudaDeviceSynchronize();
+  gmres_free(pl);
+  DBuf* bufs[] = {&pl->tw64_z, &pl->tw64_xy, &pl->tw32_z, &pl->tw32_xy, &pl->t4_64, &pl->t4_32, &pl->khat64,
+                  &pl->khat32, &pl->va_blocks, &pl->W64, &pl->W32, &pl->f64a, &pl->f64b, &pl->f32a, &pl->f32b,
+                  &pl->red};
+  for (DBuf* b : bufs) dfree(pl, *b);
+  delete pl;
+  return MSC_OK;
+}
+
+int msc_plan_set_stream(msc_plan* pl, void* stream) {
+  if (!pl) { set_error("null plan"); return MSC_ERR_INVALID; }
+  pl->stream = (cudaStream_t)stream;
+  return MSC_OK;
+}
+
+int msc_plan_fft_sizes(const msc_plan* pl, int32_t* o) {
+  if (!pl || !o) { set_error("null argument"); return MSC_ERR_INVALID; }
+  o[0] = pl->g.Lz;
+  o[1] = pl->g.Lx;
+  o[2] = pl->g.Ly;
+  return MSC_OK;
+}
+
+int64_t msc_plan_device_bytes(const msc_plan* pl) { return pl ? pl->bytes : 0; }
+
+int msc_build_t0(msc_plan* pl, const double* dlam, const double* dmu, const double* drho, double omega) {
+  if (!pl || !dlam || !dmu || !drho) { set_error("null argument"); return MSC_ERR_INVALID; }
+  if (!(omega > 0)) { set_error("omega must be > 0, got %g", omega); return MSC_ERR_INVALID; }
+  MSC_TRY(launch_t0(pl, dlam, dmu, drho, omega));
+  pl->has_t0 = true;
+  pl->omega_t0 = omega;
+  return MSC_OK;
+}
+
+int msc_t0_scalars(const msc_plan* pl, void* out) {
+  if (!pl || !out) { set_error("null argument"); return MSC_ERR_INVALID; }
+  if (!pl->has_t0) { set_error("build_t0 first"); return MSC_ERR_STATE; }
+  MSC_CUDA(cudaMemcpyAsync(out, pl->t4_64.p, sizeof(double2) * 4 * pl->g.nsite, cudaMemcpyDeviceToDevice, pl->stream));
+  return MSC_OK;
+}
+
+int msc_set_t0_scalars(msc_plan* pl, const void* t4, double omega) {
+  if (!pl || !t4) { set_error("null argument"); return MSC_ERR_INVALID; }
+  const size_t n = (size_t)4 * pl->g.nsite;
+  MSC_TRY(dalloc(pl, pl->t4_64, sizeof(double2) * n));
+  MSC_TRY(dalloc(pl, pl->t4_32, sizeof(float2) * n));
+  MSC_CUDA(cudaMemcpyAsync(pl->t4_64.p, t4, sizeof(double2) * n, cudaMemcpyDeviceToDevice, pl->stream));
+  MSC_TRY(launch_narrow(pl, (const double2*)pl->t4_64.p, (float2*)pl->t4_32.p, n));
+  pl->has_t0 = true;
+  pl->omega_t0 = omega;
+  return MSC_OK;
+}
+
+int msc_build_g0(msc_plan* pl, double omega, const double* kpar, int volume_averaged, int n_orders) {
+  if (!pl) { set_error("null plan"); return MSC_ERR_INVALID; }
+  if (!(omega > 0)) { set_error("omega must be > 0, got %g", omega); return MSC_ERR_INVALID; }
+  if (n_orders < 0) { set_error("n_orders must be >= 0"); return MSC_ERR_INVALID; }
+  if (kpar && !pl->desc.periodic) {
+    set_error("a Bloch wavevector needs a periodic plan");
+    return MSC_ERR_INVALID;
+  }
+  pl->bloch = kpar != nullptr;
+  pl->kpar[0] = kpar ? kpar[0] : 0.0;
+  pl->kpar[1] = kpar ? kpar[1] : 0.0;
+  MSC_TRY(launch_g0(pl, omega, kpar, volume_averaged ? 1 : 0, n_orders));
+  pl->has_g0 = true;
+  pl->omega_g0 = omega;
+  pl->va = volume_averaged ? 1 : 0;
+  pl->n_orders = n_orders;
+  return MSC_OK;
+}
+
+int msc_incident(msc_plan* pl, double omega, const double* k_hat, int wave_type, void* psi0) {
+  if (!pl || !k_hat || !psi0) { set_error("null argument"); return MSC_ERR_INVALID; }
+  return launch_incident(pl, omega, k_hat, wave_type, (double2*)psi0, nullptr, false);
+}
+
+int msc_matvec(msc_plan* pl, const void* x, void* y, int precision) {
+  if (!pl || !x || !y) { set_error("null argument"); return MSC_ERR_INVALID; }
+  if (x == y) { set_error("x and y may not alias"); return MSC_ERR_INVALID; }
+  const size_t n = field_elems(pl->g);
+  if (precision == MSC_COMPLEX128) {
+    MSC_TRY(dalloc(pl, pl->f64a, sizeof(double2) * n));
+    MSC_TRY(dalloc(pl, pl->f64b, sizeof(double2) * n));
+    MSC_TRY((launch_ref_to_soa<double, double>(pl, (const double2*)x, (double2*)pl->f64a.p)));
+    MSC_TRY(launch_matvec<double>(pl, (const double2*)pl->f64a.p, nullptr, (double2*)pl->f64b.p, nullptr));
+    MSC_TRY((launch_soa_to_ref<double, double>(pl, (const double2*)pl->f64b.p, (double2*)y)));
+  } else if (precision == MSC_COMPLEX64) {
+    MSC_TRY(dalloc(pl, pl->f32a, sizeof(float2) * n));
+    MSC_TRY(dalloc(pl, pl->f32b, sizeof(float2) * n));
+    MSC_TRY((launch_ref_to_soa<float, float>(pl, (const float2*)x, (float2*)pl->f32a.p)));
+    MSC_TRY(launch_matvec<float>(pl, (const float2*)pl->f32a.p, nullptr, (float2*)pl->f32b.p, nullptr));
+    MSC_TRY((launch_soa_to_ref<float, float>(pl, (const float2*)pl->f32b.p, (float2*)y)));
+  } else {
+    set_error("precision must be 0 (complex64) or 1 (complex128)");
+    return MSC_ERR_INVALID;
+  }
+  return MSC_OK;
+}
+
+int msc_solve(msc_plan* pl, const void* b, void* x, const msc_solve_opts* o, msc_solve_stats* st) {
+  if (!pl || !b || !x || !o) { set_error("null argument"); return MSC_ERR_INVALID; }
+  if (o->precision != MSC_SOLVE_MIXED && o->precision != MSC_SOLVE_FP64) {
+    set_error("precision must be mixed (0) or fp64 (1)");
+    return MSC_ERR_INVALID;
+  }
+  if (o->initial_guess != 0 && o->initial_guess != 1) {
+    set_error("initial_guess must be 0 (born) or 1 (zero)");
+    return MSC_ERR_INVALID;
+  }
+  return solve(pl, (const double2*)b, (double2*)x, o, st);
+}
+
+int msc_rpp_periodic(msc_plan* pl, const void* psi, double omega, double p, int bloch, double* out) {
+  if (!pl || !psi || !out) { set_error("null argument"); return MSC_ERR_INVALID; }
+  return rpp_periodic(pl, (const double2*)psi, omega, p, bloch, out);
+}
+
+int msc_reflected_field(msc_plan* pl, const void* psi, double omega, const double* k_hat, double* out) {
+  if (!pl || !psi || !k_hat || !out) { set_error("null argument"); return MSC_ERR_INVALID; }
+  return reflected_field(pl, (const double2*)psi, omega, k_hat, out);
+}
+
+}  // extern "C"

@@ -1,0 +1,648 @@
+// Restarted GMRES(m) with CGS2 Arnoldi on the device, and the mixed-precision
+// driver: complex64 inner solves inside FP64 iterative refinement.
+//
+// Replaces torch_gmres (tmnestor/MultipleScatteringCalculations
+// cubic_scattering/torch_gmres.py:83-205) and the scipy.sparse.linalg.gmres call of
+// compute_slab_scattering (slab_scattering.py:539-552). Differences by design:
+//  * the Givens rotation is the unitary complex one, G = [[c, s], [-conj(s), c]],
+//    c = |a|/r, s = (a/|a|) conj(b)/r (the reference's torch_gmres drops the
+//    conjugates, which is not unitary for complex Hessenberg entries);
+//  * restarted with a fixed basis of m+1 vectors; Hessenberg, rotations and the
+//    least-squares solve are FP64 on the device;
+//  * Krylov vectors are stored unnormalised with a per-vector FP64 scale
+//    (V_i = s_i v_i), so normalisation costs no pass over memory;
+//  * the host checks convergence one Arnoldi step behind the GPU: the kernels of
+//    a step enqueued after convergence see the device `done` flag and return.
+#include <algorithm>
+#include <cmath>
+#include <vector>
+
+#include "plan.cuh"
+
+namespace msc {
+
+template <typename T>
+int launch_fft_contig(msc_plan* pl, const cx<T>* in, cx<T>* out, long long nlines, long long in_stride,
+                      long long out_stride, int n_in, int n_out, const FftPlan1D& f, const cx<T>* tw, int dir,
+                      const int* done);
+
+struct GState {
+  int done;       // cycle finished
+  int converged;  // |g_{j+1}| <= tol_abs
+  int status;     // msc_status of the cycle
+  int k;          // columns in the least-squares solution
+  double tol_abs; // target on |g_{j+1}|
+  double beta;    // initial residual norm of the cycle
+  double res;     // current residual estimate
+  int counter[4]; // last-block reduction counters
+};
+
+struct GmresWork {
+  int m = 0;
+  size_t n = 0;
+  DBuf V32, V64;          // (m+1) x n Krylov basis
+  DBuf x64, r64, ax64;    // FP64 iterate, residual, A x
+  DBuf d32, r32;          // inner correction and right-hand side (complex64)
+  DBuf state;             // GState
+  DBuf hess;              // H[(m+1) x m], cs[m], sn[m], g[m+1], y[m], scale[m+1], h1[m+1], h2[m+1], nrm[2]
+  DBuf part;              // partial sums [NB][33]
+  GState* hstate = nullptr;  // pinned host mirror
+  cudaEvent_t ev[2] = {nullptr, nullptr};
+};
+
+constexpr int NB = 592;     // blocks of the multi-vector kernels (4 per SM)
+constexpr int NTH = 256;
+constexpr int PLD = 33;     // partials leading dimension (<= 32 vectors + norm)
+
+struct HessPtr {
+  double2* H;
+  double* cs;
+  double2* sn;
+  double2* g;
+  double2* y;
+  double* scale;
+  double2* h1;
+  double2* h2;
+  double2* nrm;   // [4]: 0 = GMRES cycle norms, 1 = outer residual
+};
+
+static HessPtr hess_ptrs(GmresWork* gw) {
+  const int m = gw->m;
+  char* p = (char*)gw->hess.p;
+  HessPtr h;
+  h.nrm = (double2*)p; p += sizeof(double2) * 4;
+  h.H = (double2*)p; p += sizeof(double2) * (size_t)(m + 1) * m;
+  h.sn = (double2*)p; p += sizeof(double2) * m;
+  h.g = (double2*)p; p += sizeof(double2) * (m + 1);
+  h.y = (double2*)p; p += sizeof(double2) * m;
+  h.h1 = (double2*)p; p += sizeof(double2) * (m + 1);
+  h.h2 = (double2*)p; p += sizeof(double2) * (m + 1);
+  h.cs = (double*)p; p += sizeof(double) * m;
+  h.scale = (double*)p; p += sizeof(double) * (m + 1);
+  return h;
+}
+static size_t hess_bytes(int m) {
+  return sizeof(double2) * ((size_t)(m + 1) * m + m + (m + 1) + m + 2 * (m + 1) + 4) + sizeof(double) * (m + m + 1);
+}
+
+// ---- block reduction of NV complex partials; last block reduces over blocks -----------
+// sums[i] (i < nv) are this thread's partials. The final values land in out[i].
+template <int NV>
+__device__ void reduce_to(double2* sums, int nv, double2* __restrict__ part, int* counter, double2* out) {
+  __shared__ double2 sh[NTH / 32][NV];
+  __shared__ bool last;
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+#pragma unroll
+  for (int i = 0; i < NV; ++i) {
+    if (i < nv) {
+      double2 v = sums[i];
+      for (int o = 16; o > 0; o >>= 1) {
+        v.x += __shfl_xor_sync(0xffffffffu, v.x, o);
+        v.y += __shfl_xor_sync(0xffffffffu, v.y, o);
+      }
+      if (l == 0) sh[w][i] = v;
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x < nv) {
+    double2 v = make_double2(0, 0);
+    for (int k = 0; k < NTH / 32; ++k) v += sh[k][threadIdx.x];
+    part[(size_t)blockIdx.x * PLD + threadIdx.x] = v;
+  }
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) last = (atomicAdd(counter, 1) == (int)gridDim.x - 1);
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  for (int i = w; i < nv; i += NTH / 32) {
+    double2 v = make_double2(0, 0);
+    for (int b = l; b < (int)gridDim.x; b += 32) v += ((volatile double2*)part)[(size_t)b * PLD + i];
+    for (int o = 16; o > 0; o >>= 1) {
+      v.x += __shfl_xor_sync(0xffffffffu, v.x, o);
+      v.y += __shfl_xor_sync(0xffffffffu, v.y, o);
+    }
+    if (l == 0) out[i] = v;
+  }
+  if (threadIdx.x == 0) *counter = 0;
+}
+
+// out[i] = sum_k conj(s_i V_i[k]) w[k], i < nv
+template <typename T, int NV>
+__global__ void __launch_bounds__(NTH) k_mdot(const cx<T>* __restrict__ V, size_t n, int nv, const double* scale,
+                                              const cx<T>* __restrict__ w, double2* part, int* counter, double2* out,
+                                              const int* done) {
+  if (done && *done) return;
+  double2 acc[NV];
+#pragma unroll
+  for (int i = 0; i < NV; ++i) acc[i] = make_double2(0, 0);
+  for (size_t k = (size_t)blockIdx.x * NTH + threadIdx.x; k < n; k += (size_t)gridDim.x * NTH) {
+    const double2 wk = to_d(w[k]);
+#pragma unroll
+    for (int i = 0; i < NV; ++i)
+      if (i < nv) {
+        const double2 v = to_d(V[(size_t)i * n + k]);
+        acc[i].x += v.x * wk.x + v.y * wk.y;
+        acc[i].y += v.x * wk.y - v.y * wk.x;
+      }
+  }
+#pragma unroll
+  for (int i = 0; i < NV; ++i)
+    if (i < nv) {
+      const double s = scale ? scale[i] : 1.0;
+      acc[i].x *= s;
+      acc[i].y *= s;
+    }
+  reduce_to<NV>(acc, nv, part, counter, out);
+}
+
+// w -= sum_i coef_i s_i V_i (i < nv); optionally out_norm = ||w||^2 (in .x)
+template <typename T, int NV, bool NORM>
+__global__ void __launch_bounds__(NTH) k_maxpy(const cx<T>* __restrict__ V, size_t n, int nv, const double* scale,
+                                               const double2* coef, cx<T>* __restrict__ w, double2* part, int* counter,
+                                               double2* out_norm, const int* done) {
+  if (done && *done) return;
+  __shared__ double2 cf[NV];
+  if (threadIdx.x < NV) {
+    const double s = (scale && threadIdx.x < nv) ? scale[threadIdx.x] : 1.0;
+    cf[threadIdx.x] = threadIdx.x < nv ? make_double2(s * coef[threadIdx.x].x, s * coef[threadIdx.x].y)
+                                       : make_double2(0, 0);
+  }
+  __syncthreads();
+  double2 nrm = make_double2(0, 0);
+  for (size_t k = (size_t)blockIdx.x * NTH + threadIdx.x; k < n; k += (size_t)gridDim.x * NTH) {
+    double2 wk = to_d(w[k]);
+#pragma unroll
+    for (int i = 0; i < NV; ++i)
+      if (i < nv) {
+        const double2 v = to_d(V[(size_t)i * n + k]);
+        const double2 c = cf[i];
+        wk.x -= c.x * v.x - c.y * v.y;
+        wk.y -= c.x * v.y + c.y * v.x;
+      }
+    const cx<T> o = from_d<cx<T>>(wk);
+    w[k] = o;
+    if (NORM) {
+      const double2 od = to_d(o);
+      nrm.x += od.x * od.x + od.y * od.y;
+    }
+  }
+  if (NORM) {
+    double2 a[1] = {nrm};
+    reduce_to<1>(a, 1, part, counter, out_norm);
+  }
+}
+
+// ||v||^2 -> out.x ; optionally also r = b - ax written first (when b != null)
+template <typename T>
+__global__ void __launch_bounds__(NTH) k_resid_norm(const cx<T>* __restrict__ b, const cx<T>* __restrict__ ax,
+                                                    cx<T>* __restrict__ r, size_t n, double2* part, int* counter,
+                                                    double2* out) {
+  double2 nrm = make_double2(0, 0);
+  for (size_t k = (size_t)blockIdx.x * NTH + threadIdx.x; k < n; k += (size_t)gridDim.x * NTH) {
+    cx<T> v;
+    if (ax) {
+      v = b[k] - ax[k];
+      r[k] = v;
+    } else {
+      v = b[k];
+    }
+    const double2 d = to_d(v);
+    nrm.x += d.x * d.x + d.y * d.y;
+  }
+  double2 a[1] = {nrm};
+  reduce_to<1>(a, 1, part, counter, out);
+}
+
+// cycle start: beta = sqrt(nrm), scale[0] = 1/beta, g = (beta, 0, ...)
+__global__ void k_cycle_init(GState* st, HessPtr h, int m, double tol_abs) {
+  if (threadIdx.x != 0) return;
+  const double beta = sqrt(h.nrm[0].x);
+  st->beta = beta;
+  st->res = beta;
+  st->tol_abs = tol_abs;
+  st->k = 0;
+  st->status = MSC_OK;
+  st->converged = 0;
+  st->done = 0;
+  for (int i = 0; i <= m; ++i) h.g[i] = make_double2(0, 0);
+  h.g[0] = make_double2(beta, 0);
+  h.scale[0] = beta > 0 ? 1.0 / beta : 0.0;
+  if (!(beta == beta) || isinf(beta)) {
+    st->status = MSC_ERR_NONFINITE;
+    st->done = 1;
+  } else if (beta <= tol_abs || beta == 0.0) {
+    st->converged = 1;
+    st->done = 1;
+  }
+}
+
+__device__ __forceinline__ double cabs_(double2 a) { return hypot(a.x, a.y); }
+
+// Column j of H from the two CGS passes, rotations, residual estimate, and (when the
+// cycle ends) the back substitution.
+__global__ void k_givens(GState* st, HessPtr h, int m, int j) {
+  if (threadIdx.x != 0 || st->done) return;
+  double2* Hc = h.H + (size_t)j * (m + 1);
+  for (int i = 0; i <= j; ++i) Hc[i] = h.h1[i] + h.h2[i];
+  const double hn = sqrt(h.nrm[0].x);
+  Hc[j + 1] = make_double2(hn, 0);
+  h.scale[j + 1] = hn > 0 ? 1.0 / hn : 0.0;
+  for (int i = 0; i < j; ++i) {
+    const double c = h.cs[i];
+    const double2 s = h.sn[i];
+    const double2 a = Hc[i], b = Hc[i + 1];
+    Hc[i] = c * a + s * b;
+    Hc[i + 1] = c * b - conj_(s) * a;
+  }
+  const double2 a = Hc[j];
+  const double bb = hn;
+  const double aa = cabs_(a);
+  double c;
+  double2 s;
+  if (bb == 0.0) {
+    c = 1.0;
+    s = make_double2(0, 0);
+  } else if (aa == 0.0) {
+    c = 0.0;
+    s = make_double2(1, 0);
+    Hc[j] = make_double2(bb, 0);
+  } else {
+    const double r = hypot(aa, bb);
+    c = aa / r;
+    const double2 ph = make_double2(a.x / aa, a.y / aa);
+    s = make_double2(ph.x * bb / r, ph.y * bb / r);  // (a/|a|) conj(b)/r with b real
+    Hc[j] = make_double2(ph.x * r, ph.y * r);
+  }
+  Hc[j + 1] = make_double2(0, 0);
+  h.cs[j] = c;
+  h.sn[j] = s;
+  const double2 gj = h.g[j];
+  h.g[j] = c * gj;
+  h.g[j + 1] = make_double2(0, 0) - conj_(s) * gj;
+  const double res = cabs_(h.g[j + 1]);
+  st->res = res;
+  bool end = false;
+  if (!(res == res) || isinf(res)) {
+    st->status = MSC_ERR_NONFINITE;
+    end = true;
+  } else if (res <= st->tol_abs) {
+    st->converged = 1;
+    end = true;
+  } else if (hn <= 1e-300 * (st->beta > 0 ? st->beta : 1.0)) {
+    st->status = MSC_BREAKDOWN;  // invariant subspace: the solution is exact in it
+    end = true;
+  } else if (j + 1 == m) {
+    end = true;
+  }
+  if (end) {
+    const int k = j + 1;
+    st->k = k;
+    for (int i = k - 1; i >= 0; --i) {
+      double2 v = h.g[i];
+      for (int q = i + 1; q < k; ++q) v -= h.H[(size_t)q * (m + 1) + i] * h.y[q];
+      const double2 d = h.H[(size_t)i * (m + 1) + i];
+      const double dd = d.x * d.x + d.y * d.y;
+      h.y[i] = dd > 0 ? make_double2((v.x * d.x + v.y * d.y) / dd, (v.y * d.x - v.x * d.y) / dd) : make_double2(0, 0);
+    }
+    st->done = 1;
+  }
+}
+
+// x += sum_{i<k} y_i s_i V_i, with k from the state
+template <typename T, typename TX, int NV>
+__global__ void __launch_bounds__(NTH) k_update_x(cx<TX>* __restrict__ x, const cx<T>* __restrict__ V, size_t n,
+                                                  const double* scale, const double2* y, const GState* st) {
+  __shared__ double2 cf[NV];
+  const int k = st->k;
+  if (threadIdx.x < NV)
+    cf[threadIdx.x] = threadIdx.x < k ? scale[threadIdx.x] * y[threadIdx.x] : make_double2(0, 0);
+  __syncthreads();
+  if (k == 0) return;
+  for (size_t e = (size_t)blockIdx.x * NTH + threadIdx.x; e < n; e += (size_t)gridDim.x * NTH) {
+    double2 xv = to_d(x[e]);
+#pragma unroll
+    for (int i = 0; i < NV; ++i)
+      if (i < k) {
+        const double2 v = to_d(V[(size_t)i * n + e]);
+        xv += cf[i] * v;
+      }
+    x[e] = from_d<cx<TX>>(xv);
+  }
+}
+
+// x64 += c * d32 ; out32 = (complex64)(r64 * inv)
+__global__ void k_axpy_mixed(double2* __restrict__ x, const float2* __restrict__ d, size_t n, const double* c) {
+  const double cc = *c;
+  for (size_t e = (size_t)blockIdx.x * NTH + threadIdx.x; e < n; e += (size_t)gridDim.x * NTH) {
+    const float2 v = d[e];
+    x[e].x += cc * v.x;
+    x[e].y += cc * v.y;
+  }
+}
+__global__ void k_to32_scaled(const double2* __restrict__ r, float2* __restrict__ o, size_t n, const double* nrm2) {
+  const double inv = 1.0 / sqrt(*nrm2);
+  for (size_t e = (size_t)blockIdx.x * NTH + threadIdx.x; e < n; e += (size_t)gridDim.x * NTH)
+    o[e] = make_float2((float)(r[e].x * inv), (float)(r[e].y * inv));
+}
+__global__ void k_sqrt(const double* a, double* b) {
+  if (threadIdx.x == 0) *b = sqrt(*a);
+}
+
+// ---- host side ---------------------------------------------------------------------------
+static int nv_bucket(int nv) { return nv <= 4 ? 4 : nv <= 8 ? 8 : nv <= 16 ? 16 : 32; }
+
+template <typename T>
+static int mdot(msc_plan* pl, GmresWork* gw, const cx<T>* V, int nv, const double* scale, const cx<T>* w, double2* out,
+                const int* done) {
+  GState* st = (GState*)gw->state.p;
+  double2* part = (double2*)gw->part.p;
+  const int nb = std::min<long long>(NB, ceil_div((long long)gw->n, NTH));
+#define L_(NV) k_mdot<T, NV><<<nb, NTH, 0, pl->stream>>>(V, gw->n, nv, scale, w, part, &st->counter[0], out, done)
+  switch (nv_bucket(nv)) {
+    case 4: L_(4); break;
+    case 8: L_(8); break;
+    case 16: L_(16); break;
+    default: L_(32); break;
+  }
+#undef L_
+  MSC_CUDA(cudaGetLastError());
+  return MSC_OK;
+}
+
+template <typename T, bool NORM>
+static int maxpy(msc_plan* pl, GmresWork* gw, const cx<T>* V, int nv, const double* scale, const double2* coef,
+                 cx<T>* w, double2* out_norm, const int* done) {
+  GState* st = (GState*)gw->state.p;
+  double2* part = (double2*)gw->part.p;
+  const int nb = std::min<long long>(NB, ceil_div((long long)gw->n, NTH));
+#define L_(NV) \
+  k_maxpy<T, NV, NORM><<<nb, NTH, 0, pl->stream>>>(V, gw->n, nv, scale, coef, w, part, &st->counter[1], out_norm, done)
+  switch (nv_bucket(nv)) {
+    case 4: L_(4); break;
+    case 8: L_(8); break;
+    case 16: L_(16); break;
+    default: L_(32); break;
+  }
+#undef L_
+  MSC_CUDA(cudaGetLastError());
+  return MSC_OK;
+}
+
+template <typename T>
+static int resid_norm(msc_plan* pl, GmresWork* gw, const cx<T>* b, const cx<T>* ax, cx<T>* r, double* out_nrm2) {
+  GState* st = (GState*)gw->state.p;
+  const int nb = std::min<long long>(NB, ceil_div((long long)gw->n, NTH));
+  k_resid_norm<T><<<nb, NTH, 0, pl->stream>>>(b, ax, r, gw->n, (double2*)gw->part.p, &st->counter[2],
+                                             (double2*)out_nrm2);
+  MSC_CUDA(cudaGetLastError());
+  return MSC_OK;
+}
+
+static int ensure_work(msc_plan* pl, int m) {
+  if (!pl->gw) pl->gw = new GmresWork();
+  GmresWork* gw = pl->gw;
+  const size_t n = field_elems(pl->g);
+  if (gw->m >= m && gw->n == n) return MSC_OK;
+  gw->m = std::max(m, gw->m);
+  gw->n = n;
+  const size_t vb = (size_t)(gw->m + 1) * n;
+  MSC_TRY(dalloc(pl, gw->V32, sizeof(float2) * vb));
+  MSC_TRY(dalloc(pl, gw->V64, sizeof(double2) * vb));
+  MSC_TRY(dalloc(pl, gw->x64, sizeof(double2) * n));
+  MSC_TRY(dalloc(pl, gw->r64, sizeof(double2) * n));
+  MSC_TRY(dalloc(pl, gw->ax64, sizeof(double2) * n));
+  MSC_TRY(dalloc(pl, gw->d32, sizeof(float2) * n));
+  MSC_TRY(dalloc(pl, gw->r32, sizeof(float2) * n));
+  MSC_TRY(dalloc(pl, gw->hess, hess_bytes(gw->m)));
+  MSC_TRY(dalloc(pl, gw->part, sizeof(double2) * (size_t)NB * PLD));
+  if (!gw->state.p) {
+    MSC_TRY(dalloc(pl, gw->state, sizeof(GState)));
+    MSC_CUDA(cudaMemsetAsync(gw->state.p, 0, sizeof(GState), pl->stream));
+    MSC_CUDA(cudaMallocHost((void**)&gw->hstate, sizeof(GState) * 2));
+    MSC_CUDA(cudaEventCreateWithFlags(&gw->ev[0], cudaEventDisableTiming));
+    MSC_CUDA(cudaEventCreateWithFlags(&gw->ev[1], cudaEventDisableTiming));
+  }
+  return MSC_OK;
+}
+
+void gmres_free(msc_plan* pl) {
+  GmresWork* gw = pl->gw;
+  if (!gw) return;
+  dfree(pl, gw->V32); dfree(pl, gw->V64); dfree(pl, gw->x64); dfree(pl, gw->r64); dfree(pl, gw->ax64);
+  dfree(pl, gw->d32); dfree(pl, gw->r32); dfree(pl, gw->state); dfree(pl, gw->hess); dfree(pl, gw->part);
+  if (gw->hstate) cudaFreeHost(gw->hstate);
+  for (auto& e : gw->ev)
+    if (e) cudaEventDestroy(e);
+  delete gw;
+  pl->gw = nullptr;
+}
+
+// One restarted GMRES(m) solve of A x = rhs in precision T (x in/out, same precision).
+// Stops when the residual estimate <= tol_abs or after max_mv operator applications.
+// Returns the number of matvecs used in *n_mv and the final estimate in *res.
+template <typename T>
+static int gmres_core(msc_plan* pl, int m, const cx<T>* rhs, cx<T>* x, bool x_zero, double tol_abs, int max_mv,
+                      int* n_mv, double* res, int* status) {
+  GmresWork* gw = pl->gw;
+  GState* st = (GState*)gw->state.p;
+  HessPtr h = hess_ptrs(gw);
+  const size_t n = gw->n;
+  cx<T>* V = (cx<T>*)(sizeof(T) == 8 ? gw->V64.p : gw->V32.p);
+  const int* done = &st->done;
+  int used = 0;
+  *status = MSC_NOT_CONVERGED;
+  bool first = true;
+  while (true) {
+    // V0 = rhs - A x  (or rhs when x == 0 on the first cycle)
+    if (first && x_zero) {
+      MSC_CUDA(cudaMemcpyAsync(V, rhs, sizeof(cx<T>) * n, cudaMemcpyDeviceToDevice, pl->stream));
+      MSC_TRY(resid_norm<T>(pl, gw, V, nullptr, nullptr, &h.nrm[0].x));
+    } else {
+      if (used >= max_mv) break;
+      MSC_TRY(launch_matvec<T>(pl, x, nullptr, V + n, nullptr));  // A x into V[1] as scratch
+      ++used;
+      MSC_TRY(resid_norm<T>(pl, gw, rhs, V + n, V, &h.nrm[0].x));
+    }
+    first = false;
+    k_cycle_init<<<1, 32, 0, pl->stream>>>(st, h, m, tol_abs);
+    MSC_CUDA(cudaGetLastError());
+    int enq = 0;  // steps enqueued in this cycle
+    bool cycle_over = false;
+    // state after cycle init
+    MSC_CUDA(cudaMemcpyAsync(&gw->hstate[0], st, sizeof(GState), cudaMemcpyDeviceToHost, pl->stream));
+    MSC_CUDA(cudaEventRecord(gw->ev[0], pl->stream));
+    int pending = 0;  // index of the event holding the newest state
+    for (int j = 0; j < m && !cycle_over; ++j) {
+      if (used + 1 > max_mv) break;
+      // Arnoldi step j: w = A v_j into V[j+1]
+      MSC_TRY(launch_matvec<T>(pl, V + (size_t)j * n, h.scale + j, V + (size_t)(j + 1) * n, done));
+      ++used;
+      ++enq;
+      cx<T>* w = V + (size_t)(j + 1) * n;
+      MSC_TRY(mdot<T>(pl, gw, V, j + 1, h.scale, w, h.h1, done));
+      MSC_TRY((maxpy<T, false>(pl, gw, V, j + 1, h.scale, h.h1, w, nullptr, done)));
+      MSC_TRY(mdot<T>(pl, gw, V, j + 1, h.scale, w, h.h2, done));
+      MSC_TRY((maxpy<T, true>(pl, gw, V, j + 1, h.scale, h.h2, w, &h.nrm[0], done)));
+      k_givens<<<1, 32, 0, pl->stream>>>(st, h, m, j);
+      MSC_CUDA(cudaGetLastError());
+      const int slot = (pending + 1) & 1;
+      MSC_CUDA(cudaMemcpyAsync(&gw->hstate[slot], st, sizeof(GState), cudaMemcpyDeviceToHost, pl->stream));
+      MSC_CUDA(cudaEventRecord(gw->ev[slot], pl->stream));
+      // check the state of the previous step (lagged by one step)
+      MSC_CUDA(cudaEventSynchronize(gw->ev[pending]));
+      if (gw->hstate[pending].done) {
+        cycle_over = true;  // step j early-exits on the device
+        --used;             // ... and applies no operator
+      }
+      pending = slot;
+    }
+    if (!cycle_over) {
+      MSC_CUDA(cudaEventSynchronize(gw->ev[pending]));
+    }
+    // cycles that ended at step j (and not before) are visible in the newest state
+    MSC_CUDA(cudaStreamSynchronize(pl->stream));
+    GState cur;
+    MSC_CUDA(cudaMemcpy(&cur, st, sizeof(GState), cudaMemcpyDeviceToHost));
+    // x += V y (k columns)
+    if (cur.k > 0) {
+      const int nb = std::min<long long>(NB, ceil_div((long long)n, NTH));
+      k_update_x<T, T, 32><<<nb, NTH, 0, pl->stream>>>(x, V, n, h.scale, h.y, st);
+      MSC_CUDA(cudaGetLastError());
+    }
+    *res = cur.res;
+    if (cur.status == MSC_ERR_NONFINITE) {
+      *status = MSC_ERR_NONFINITE;
+      break;
+    }
+    if (cur.converged) {
+      *status = MSC_OK;
+      break;
+    }
+    if (cur.status == MSC_BREAKDOWN) {
+      *status = MSC_OK;
+      break;
+    }
+    if (used >= max_mv) break;
+    if (enq == 0) break;
+  }
+  *n_mv = used;
+  return MSC_OK;
+}
+
+int solve(msc_plan* pl, const double2* b_ref, double2* x_ref, const msc_solve_opts* o, msc_solve_stats* stats) {
+  if (!pl->has_t0 || !pl->has_g0) {
+    set_error("solve needs build_t0 and build_g0 first");
+    return MSC_ERR_STATE;
+  }
+  const int m = std::max(1, std::min(o->restart > 0 ? o->restart : 30, 32));
+  MSC_TRY(ensure_work(pl, m));
+  GmresWork* gw = pl->gw;
+  HessPtr h = hess_ptrs(gw);
+  const size_t n = gw->n;
+  double2* x = (double2*)gw->x64.p;
+  double2* r = (double2*)gw->r64.p;
+  double2* ax = (double2*)gw->ax64.p;
+  double2* b = (double2*)pl->f64a.p;
+  MSC_TRY(dalloc(pl, pl->f64a, sizeof(double2) * n));
+  b = (double2*)pl->f64a.p;
+  MSC_TRY(launch_ref_to_soa<double, double>(pl, b_ref, b));
+  if (pl->bloch) {
+    // the solve runs in the demodulated frame; b arrives physical
+    MSC_TRY(bloch_modulate(pl, b, -1));
+  }
+  if (o->initial_guess == 0)
+    MSC_CUDA(cudaMemcpyAsync(x, b, sizeof(double2) * n, cudaMemcpyDeviceToDevice, pl->stream));
+  else
+    MSC_CUDA(cudaMemsetAsync(x, 0, sizeof(double2) * n, pl->stream));
+  // ||b||
+  double* dn = &h.nrm[1].x;  // outer ||.||^2 (h.nrm[1].y is scratch of the reduction)
+  MSC_TRY(resid_norm<double>(pl, gw, b, nullptr, nullptr, dn));
+  double bn2 = 0;
+  MSC_CUDA(cudaMemcpyAsync(&bn2, dn, sizeof(double), cudaMemcpyDeviceToHost, pl->stream));
+  MSC_CUDA(cudaStreamSynchronize(pl->stream));
+  const double bnorm = std::sqrt(bn2);
+  msc_solve_stats s{};
+  s.status = MSC_NOT_CONVERGED;
+  const double tol = o->tol > 0 ? o->tol : 1e-6;
+  const int max_mv = o->max_iter > 0 ? o->max_iter : 500;
+  if (bnorm == 0.0) {
+    MSC_CUDA(cudaMemsetAsync(x, 0, sizeof(double2) * n, pl->stream));
+    s.status = MSC_OK;
+    s.residual = 0.0;
+  } else if (o->precision == MSC_SOLVE_FP64) {
+    int used = 0, st = 0;
+    double est = 0;
+    MSC_TRY(gmres_core<double>(pl, m, b, x, o->initial_guess != 0, tol * bnorm, max_mv, &used, &est, &st));
+    s.n_matvec = used;
+    s.n_matvec64 = used;
+    s.status = st;
+    // true residual
+    MSC_TRY(launch_matvec<double>(pl, x, nullptr, ax, nullptr));
+    s.n_matvec += 1;
+    s.n_matvec64 += 1;
+    MSC_TRY(resid_norm<double>(pl, gw, b, ax, r, dn));
+    double rn2 = 0;
+    MSC_CUDA(cudaMemcpyAsync(&rn2, dn, sizeof(double), cudaMemcpyDeviceToHost, pl->stream));
+    MSC_CUDA(cudaStreamSynchronize(pl->stream));
+    s.residual = std::sqrt(rn2) / bnorm;
+    if (s.status != MSC_ERR_NONFINITE) s.status = s.residual <= tol ? MSC_OK : MSC_NOT_CONVERGED;
+  } else {
+    // mixed: FP64 refinement around complex64 GMRES
+    const double inner = o->inner_tol > 0 ? o->inner_tol : 1e-5;
+    float2* d = (float2*)gw->d32.p;
+    float2* r32 = (float2*)gw->r32.p;
+    int used = 0;  // complex64 Krylov matvecs (the budget); FP64 residuals count apart
+    double res = 0;
+    int outer = 0;
+    while (true) {
+      MSC_TRY(launch_matvec<double>(pl, x, nullptr, ax, nullptr));
+      ++s.n_matvec64;
+      MSC_TRY(resid_norm<double>(pl, gw, b, ax, r, dn));
+      double rn2 = 0;
+      MSC_CUDA(cudaMemcpyAsync(&rn2, dn, sizeof(double), cudaMemcpyDeviceToHost, pl->stream));
+      MSC_CUDA(cudaStreamSynchronize(pl->stream));
+      res = std::sqrt(rn2) / bnorm;
+      if (!(res == res)) {
+        s.status = MSC_ERR_NONFINITE;
+        break;
+      }
+      if (res <= tol) {
+        s.status = MSC_OK;
+        break;
+      }
+      if (used >= max_mv) break;
+      // inner: A d = r / ||r|| in complex64, relative target `inner` (or what is left to reach tol)
+      k_to32_scaled<<<std::min<long long>(NB, ceil_div((long long)n, NTH)), NTH, 0, pl->stream>>>(r, r32, n, dn);
+      MSC_CUDA(cudaMemsetAsync(d, 0, sizeof(float2) * n, pl->stream));
+      const double target = std::max(inner, 0.5 * tol / res);
+      int iu = 0, ist = 0;
+      double est = 0;
+      MSC_TRY(gmres_core<float>(pl, m, r32, d, true, target, max_mv - used, &iu, &est, &ist));
+      used += iu;
+      ++outer;
+      if (ist == MSC_ERR_NONFINITE) {
+        s.status = MSC_ERR_NONFINITE;
+        break;
+      }
+      // x += ||r|| d
+      k_sqrt<<<1, 32, 0, pl->stream>>>(dn, dn);
+      k_axpy_mixed<<<std::min<long long>(NB, ceil_div((long long)n, NTH)), NTH, 0, pl->stream>>>(x, d, n, dn);
+      MSC_CUDA(cudaGetLastError());
+      if (iu == 0) break;
+    }
+    s.n_matvec = used + s.n_matvec64;
+    s.n_outer = outer;
+    s.residual = res;
+  }
+  // x back to the caller's layout (and physical frame)
+  if (pl->bloch) {
+    MSC_TRY(bloch_modulate(pl, x, +1));
+  }
+  MSC_TRY(launch_soa_to_ref<double, double>(pl, x, x_ref));
+  MSC_CUDA(cudaStreamSynchronize(pl->stream));
+  if (stats) *stats = s;
+  return s.status;
+}
+
+}  // namespace msc

@@ -1,0 +1,75 @@
+// Common device helpers of the slab Foldy-Lax solver: complex arithmetic on
+// float2/double2, status codes, launch helpers.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "../../include/msc.h"
+
+namespace msc {
+
+// ---- complex element type per real type -----------------------------------
+template <typename T> struct CxT;
+template <> struct CxT<float> { using type = float2; };
+template <> struct CxT<double> { using type = double2; };
+template <typename T> using cx = typename CxT<T>::type;
+
+template <typename T> __host__ __device__ __forceinline__ cx<T> mk(T a, T b) { cx<T> r; r.x = a; r.y = b; return r; }
+__host__ __device__ __forceinline__ float2 operator+(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
+__host__ __device__ __forceinline__ float2 operator-(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+__host__ __device__ __forceinline__ float2 operator*(float2 a, float2 b) {
+  return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+__host__ __device__ __forceinline__ float2 operator*(float s, float2 a) { return make_float2(s * a.x, s * a.y); }
+__host__ __device__ __forceinline__ double2 operator+(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
+__host__ __device__ __forceinline__ double2 operator-(double2 a, double2 b) { return make_double2(a.x - b.x, a.y - b.y); }
+__host__ __device__ __forceinline__ double2 operator*(double2 a, double2 b) {
+  return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+__host__ __device__ __forceinline__ double2 operator*(double s, double2 a) { return make_double2(s * a.x, s * a.y); }
+__host__ __device__ __forceinline__ float2& operator+=(float2& a, float2 b) { a.x += b.x; a.y += b.y; return a; }
+__host__ __device__ __forceinline__ double2& operator+=(double2& a, double2 b) { a.x += b.x; a.y += b.y; return a; }
+__host__ __device__ __forceinline__ float2& operator-=(float2& a, float2 b) { a.x -= b.x; a.y -= b.y; return a; }
+__host__ __device__ __forceinline__ double2& operator-=(double2& a, double2 b) { a.x -= b.x; a.y -= b.y; return a; }
+
+template <typename C> __host__ __device__ __forceinline__ C conj_(C a) { a.y = -a.y; return a; }
+// a * conj(b)
+template <typename C> __host__ __device__ __forceinline__ C mul_conj(C a, C b) {
+  C r; r.x = a.x * b.x + a.y * b.y; r.y = a.y * b.x - a.x * b.y; return r;
+}
+// conj(a) * b
+template <typename C> __host__ __device__ __forceinline__ C conj_mul(C a, C b) {
+  C r; r.x = a.x * b.x + a.y * b.y; r.y = a.x * b.y - a.y * b.x; return r;
+}
+// multiply by +i (s = +1) or -i (s = -1)
+template <int S, typename C> __host__ __device__ __forceinline__ C mul_i(C a) {
+  C r;
+  if (S > 0) { r.x = -a.y; r.y = a.x; } else { r.x = a.y; r.y = -a.x; }
+  return r;
+}
+// fused a += b * c
+template <typename C> __host__ __device__ __forceinline__ void fma_(C& a, C b, C c) {
+  a.x = fma(b.x, c.x, a.x); a.x = fma(-b.y, c.y, a.x);
+  a.y = fma(b.x, c.y, a.y); a.y = fma(b.y, c.x, a.y);
+}
+__device__ __forceinline__ void fma_(float2& a, float2 b, float2 c) {
+  a.x = fmaf(b.x, c.x, a.x); a.x = fmaf(-b.y, c.y, a.x);
+  a.y = fmaf(b.x, c.y, a.y); a.y = fmaf(b.y, c.x, a.y);
+}
+
+template <typename C> __device__ __forceinline__ C czero() { C r; r.x = 0; r.y = 0; return r; }
+
+__device__ __forceinline__ float2 to_c(double2 a, float2*) { return make_float2((float)a.x, (float)a.y); }
+__device__ __forceinline__ double2 to_c(double2 a, double2*) { return a; }
+__device__ __forceinline__ double2 to_d(float2 a) { return make_double2(a.x, a.y); }
+__device__ __forceinline__ double2 to_d(double2 a) { return a; }
+template <typename C> __device__ __forceinline__ C from_d(double2 a) { return to_c(a, (C*)nullptr); }
+
+// Streaming loads (ld.global.cs: evict-first) for data read exactly once per
+// matvec, such as the kernel spectrum, so it does not displace reusable lines.
+__device__ __forceinline__ float2 ld_stream(const float2* p) { return __ldcs(p); }
+__device__ __forceinline__ double2 ld_stream(const double2* p) { return __ldcs(p); }
+
+inline int ceil_div(long long a, long long b) { return (int)((a + b - 1) / b); }
+
+}  // namespace msc

@@ -1,0 +1,112 @@
+// Internal plan state shared by the translation units of libmsc_b200.so.
+#pragma once
+#include <algorithm>
+#include <string>
+#include <vector>
+
+#include "fft_smem.cuh"
+#include "msc_common.cuh"
+
+namespace msc {
+
+// Lattice and padded FFT grid. Internal field vectors are component-major
+// ("SoA"): v[c][n][i][j], c = 0..8, site = (n*M + i)*M + j.
+struct Geo {
+  int M, Nz;
+  int Lz, Lx, Ly;  // padded FFT lengths (Lx = Ly)
+  int Hy;          // stored spectrum lines ky in [0, Hy): Ly/2 + 1 (half), Ly (full)
+  int half;        // 1: half-space spectrum, columns k and -k share K(-k) = S K(k) S
+  int nsite;       // Nz*M*M
+};
+
+void set_error(const char* fmt, ...);
+
+#define MSC_CUDA(...)                                                                           \
+  do {                                                                                          \
+    cudaError_t e_ = (__VA_ARGS__);                                                             \
+    if (e_ != cudaSuccess) {                                                                    \
+      ::msc::set_error("%s:%d %s: %s", __FILE__, __LINE__, #__VA_ARGS__, cudaGetErrorString(e_)); \
+      return MSC_ERR_CUDA;                                                                      \
+    }                                                                                           \
+  } while (0)
+
+#define MSC_TRY(...)           \
+  do {                         \
+    int s_ = (__VA_ARGS__);    \
+    if (s_ < 0) return s_;     \
+  } while (0)
+
+// Device buffer owned by a plan.
+struct DBuf {
+  void* p = nullptr;
+  size_t bytes = 0;
+};
+
+struct GmresWork;
+
+}  // namespace msc
+
+struct msc_plan {
+  msc_slab_desc desc;
+  msc::Geo g;
+  cudaStream_t stream = nullptr;
+  int device = 0;
+  msc::FftPlan1D fz, fxy;
+  // twiddles exp(-2 pi i t / L) for Lz and Lxy
+  msc::DBuf tw64_z, tw64_xy, tw32_z, tw32_xy;
+  // T0
+  bool has_t0 = false;
+  double omega_t0 = 0;
+  msc::DBuf t4_64, t4_32;  // [4][nsite]
+  // G0 spectrum [E][Hy][Lx][Lz]
+  bool has_g0 = false;
+  int E = 0;               // 45 (symmetric form) or 81 (full, volume averaged)
+  int va = 0, n_orders = 2;
+  double omega_g0 = 0;
+  bool bloch = false;
+  double kpar[2] = {0, 0};
+  msc::DBuf khat64, khat32;
+  msc::DBuf va_blocks;     // [26][81] double
+  // matvec workspace [9][Nz][Ly][Lx]
+  msc::DBuf W64, W32;
+  // boundary scratch: SoA copies of in/out fields
+  msc::DBuf f64a, f64b, f32a, f32b;
+  // reduction scratch (partials, results)
+  msc::DBuf red;
+  // GMRES workspace (lazily grown)
+  msc::GmresWork* gw = nullptr;
+  int64_t bytes = 0;
+};
+
+namespace msc {
+
+int dalloc(msc_plan* pl, DBuf& b, size_t bytes);
+void dfree(msc_plan* pl, DBuf& b);
+
+// ---- launches (all enqueue on pl->stream) ------------------------------------
+int build_twiddles(msc_plan* pl);
+int launch_t0(msc_plan* pl, const double* dlam, const double* dmu, const double* drho, double omega);
+int launch_g0(msc_plan* pl, double omega, const double* kpar, int va, int n_orders);
+int launch_incident(msc_plan* pl, double omega, const double* k_hat, int wave, double2* ref_out, double2* soa_out,
+                    bool demod);
+// layout conversion between the reference layout (site-major, 9 DOF inner) and SoA
+template <typename Tin, typename Tout>
+int launch_ref_to_soa(msc_plan* pl, const cx<Tin>* in, cx<Tout>* out);
+template <typename Tin, typename Tout>
+int launch_soa_to_ref(msc_plan* pl, const cx<Tin>* in, cx<Tout>* out);
+// y = x - G0 T0 (scale * x), SoA; scale may be null (1). done may be null.
+template <typename T>
+int launch_matvec(msc_plan* pl, const cx<T>* x, const double* scale, cx<T>* y, const int* done);
+
+int rpp_periodic(msc_plan* pl, const double2* psi_ref, double omega, double p, int bloch, double* out);
+int reflected_field(msc_plan* pl, const double2* psi_ref, double omega, const double* k_hat, double* out);
+int solve(msc_plan* pl, const double2* b_ref, double2* x_ref, const msc_solve_opts* o, msc_solve_stats* st);
+void gmres_free(msc_plan* pl);
+// v *= exp(sign i k_par . x) at the cube centres (SoA complex128 field)
+int bloch_modulate(msc_plan* pl, double2* v, int sign);
+
+inline size_t field_elems(const Geo& g) { return (size_t)9 * g.nsite; }
+inline size_t ws_elems(const Geo& g) { return (size_t)9 * g.Nz * g.Ly * g.Lx; }
+inline size_t khat_elems(const Geo& g, int E) { return (size_t)E * g.Hy * g.Lx * g.Lz; }
+
+}  // namespace msc

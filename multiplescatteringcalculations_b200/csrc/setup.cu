@@ -1,0 +1,392 @@
+// Per-frequency setup on the device: twiddle tables, T0 (4 scalars per voxel),
+// the incident plane wave, layout conversions, and the G0 spectrum build.
+#include <algorithm>
+
+#include "physics.cuh"
+#include "plan.cuh"
+
+namespace msc {
+
+template <typename T>
+int launch_fft_contig(msc_plan* pl, const cx<T>* in, cx<T>* out, long long nlines, long long in_stride,
+                      long long out_stride, int n_in, int n_out, const FftPlan1D& f, const cx<T>* tw, int dir,
+                      const int* done);
+
+// ---- twiddles ------------------------------------------------------------------------
+__global__ void k_twiddles(double2* t64, float2* t32, int L) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= L) return;
+  double s, c;
+  sincospi(2.0 * (double)t / (double)L, &s, &c);
+  t64[t] = make_double2(c, -s);
+  t32[t] = make_float2((float)c, (float)-s);
+}
+
+int build_twiddles(msc_plan* pl) {
+  const int Lz = pl->g.Lz, Lxy = pl->g.Lx;
+  MSC_TRY(dalloc(pl, pl->tw64_z, sizeof(double2) * Lz));
+  MSC_TRY(dalloc(pl, pl->tw32_z, sizeof(float2) * Lz));
+  MSC_TRY(dalloc(pl, pl->tw64_xy, sizeof(double2) * Lxy));
+  MSC_TRY(dalloc(pl, pl->tw32_xy, sizeof(float2) * Lxy));
+  k_twiddles<<<ceil_div(Lz, 128), 128, 0, pl->stream>>>((double2*)pl->tw64_z.p, (float2*)pl->tw32_z.p, Lz);
+  k_twiddles<<<ceil_div(Lxy, 128), 128, 0, pl->stream>>>((double2*)pl->tw64_xy.p, (float2*)pl->tw32_xy.p, Lxy);
+  MSC_CUDA(cudaGetLastError());
+  return MSC_OK;
+}
+
+// ---- T0 --------------------------------------------------------------------------------
+__global__ void k_t0(const double* __restrict__ dl, const double* __restrict__ dm, const double* __restrict__ dr,
+                     double2* __restrict__ t64, float2* __restrict__ t32, int nsite, double omega, double a,
+                     double alpha, double beta, double rho) {
+  __shared__ CubeConst cc;
+  if (threadIdx.x == 0) cc = cube_constants(omega, a, alpha, beta, rho);
+  __syncthreads();
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= nsite) return;
+  double2 t[4];
+  t0_voxel(cc, omega, a, dl[s], dm[s], dr[s], t);
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    t64[(size_t)q * nsite + s] = t[q];
+    t32[(size_t)q * nsite + s] = make_float2((float)t[q].x, (float)t[q].y);
+  }
+}
+
+int launch_t0(msc_plan* pl, const double* dlam, const double* dmu, const double* drho, double omega) {
+  const Geo& g = pl->g;
+  MSC_TRY(dalloc(pl, pl->t4_64, sizeof(double2) * 4 * g.nsite));
+  MSC_TRY(dalloc(pl, pl->t4_32, sizeof(float2) * 4 * g.nsite));
+  k_t0<<<ceil_div(g.nsite, 256), 256, 0, pl->stream>>>(dlam, dmu, drho, (double2*)pl->t4_64.p, (float2*)pl->t4_32.p,
+                                                       g.nsite, omega, pl->desc.a, pl->desc.alpha, pl->desc.beta,
+                                                       pl->desc.rho);
+  MSC_CUDA(cudaGetLastError());
+  return MSC_OK;
+}
+
+// ---- incident plane wave (slab_scattering.py:426-478) ---------------------------------
+struct IncVec {
+  double kh[3], pol[3], k;
+};
+
+__global__ void k_incident(double2* ref_out, double2* soa_out, int M, int Nz, double a, IncVec iv, int demod,
+                           double kx, double ky) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  const int nsite = Nz * M * M;
+  if (s >= nsite) return;
+  const int j = s % M, i = (s / M) % M, n = s / (M * M);
+  const double d = 2.0 * a;
+  const double z = (n + 0.5) * d, x = (i - (M - 1) / 2.0) * d, y = (j - (M - 1) / 2.0) * d;
+  double ph = iv.k * (iv.kh[0] * z + iv.kh[1] * x + iv.kh[2] * y);
+  if (demod) ph -= kx * x + ky * y;
+  double sp, cp;
+  sincos(ph, &sp, &cp);
+  const double2 e = make_double2(cp, sp);
+  double2 v[9];
+  for (int q = 0; q < 3; ++q) v[q] = make_double2(iv.pol[q], 0.0);
+  // eps_pq = (i k / 2)(kh_p pol_q + pol_p kh_q); Voigt with engineering shear
+  for (int al = 0; al < 6; ++al) {
+    const int p = voigt_p(al), q = voigt_q(al);
+    double re = 0.5 * iv.k * (iv.kh[p] * iv.pol[q] + iv.pol[p] * iv.kh[q]);
+    if (p != q) re *= 2.0;
+    v[3 + al] = make_double2(0.0, re);
+  }
+  for (int c = 0; c < 9; ++c) {
+    const double2 w = v[c] * e;
+    if (ref_out) ref_out[(size_t)s * 9 + c] = w;
+    if (soa_out) soa_out[(size_t)c * nsite + s] = w;
+  }
+}
+
+int launch_incident(msc_plan* pl, double omega, const double* k_hat, int wave, double2* ref_out, double2* soa_out,
+                    bool demod) {
+  const double nrm = sqrt(k_hat[0] * k_hat[0] + k_hat[1] * k_hat[1] + k_hat[2] * k_hat[2]);
+  if (!(nrm > 0)) {
+    set_error("k_hat must be a nonzero 3-vector");
+    return MSC_ERR_INVALID;
+  }
+  IncVec iv;
+  for (int q = 0; q < 3; ++q) iv.kh[q] = k_hat[q] / nrm;
+  if (wave == MSC_WAVE_P) {
+    iv.k = omega / pl->desc.alpha;
+    for (int q = 0; q < 3; ++q) iv.pol[q] = iv.kh[q];
+  } else if (wave == MSC_WAVE_S) {
+    iv.k = omega / pl->desc.beta;
+    // SV: cross = k_hat x z_hat; pol = cross x k_hat normalised; vertical incidence -> x
+    const double zh[3] = {1, 0, 0};
+    double cr[3] = {iv.kh[1] * zh[2] - iv.kh[2] * zh[1], iv.kh[2] * zh[0] - iv.kh[0] * zh[2],
+                    iv.kh[0] * zh[1] - iv.kh[1] * zh[0]};
+    const double cn = sqrt(cr[0] * cr[0] + cr[1] * cr[1] + cr[2] * cr[2]);
+    if (cn < 1e-10) {
+      iv.pol[0] = 0; iv.pol[1] = 1; iv.pol[2] = 0;
+    } else {
+      double p[3] = {cr[1] * iv.kh[2] - cr[2] * iv.kh[1], cr[2] * iv.kh[0] - cr[0] * iv.kh[2],
+                     cr[0] * iv.kh[1] - cr[1] * iv.kh[0]};
+      const double pn = sqrt(p[0] * p[0] + p[1] * p[1] + p[2] * p[2]);
+      for (int q = 0; q < 3; ++q) iv.pol[q] = p[q] / pn;
+    }
+  } else {
+    set_error("wave_type must be 'P' or 'S', got code %d", wave);
+    return MSC_ERR_INVALID;
+  }
+  const Geo& g = pl->g;
+  k_incident<<<ceil_div(g.nsite, 256), 256, 0, pl->stream>>>(ref_out, soa_out, g.M, g.Nz, pl->desc.a, iv, demod ? 1 : 0,
+                                                            pl->kpar[0], pl->kpar[1]);
+  MSC_CUDA(cudaGetLastError());
+  return MSC_OK;
+}
+
+// ---- layout conversion (reference [site][9] <-> SoA [9][site]) -------------------------
+template <typename Tin, typename Tout>
+__global__ void k_ref_to_soa(const cx<Tin>* __restrict__ in, cx<Tout>* __restrict__ out, int nsite) {
+  const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= 9LL * nsite) return;
+  const int s = (int)(e / 9), c = (int)(e % 9);
+  const cx<Tin> v = in[e];
+  out[(size_t)c * nsite + s] = mk<Tout>((Tout)v.x, (Tout)v.y);
+}
+template <typename Tin, typename Tout>
+__global__ void k_soa_to_ref(const cx<Tin>* __restrict__ in, cx<Tout>* __restrict__ out, int nsite) {
+  const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= 9LL * nsite) return;
+  const int s = (int)(e / 9), c = (int)(e % 9);
+  const cx<Tin> v = in[(size_t)c * nsite + s];
+  out[e] = mk<Tout>((Tout)v.x, (Tout)v.y);
+}
+template <typename Tin, typename Tout>
+int launch_ref_to_soa(msc_plan* pl, const cx<Tin>* in, cx<Tout>* out) {
+  const long long n = 9LL * pl->g.nsite;
+  k_ref_to_soa<Tin, Tout><<<ceil_div(n, 256), 256, 0, pl->stream>>>(in, out, pl->g.nsite);
+  MSC_CUDA(cudaGetLastError());
+  return MSC_OK;
+}
+template <typename Tin, typename Tout>
+int launch_soa_to_ref(msc_plan* pl, const cx<Tin>* in, cx<Tout>* out) {
+  const long long n = 9LL * pl->g.nsite;
+  k_soa_to_ref<Tin, Tout><<<ceil_div(n, 256), 256, 0, pl->stream>>>(in, out, pl->g.nsite);
+  MSC_CUDA(cudaGetLastError());
+  return MSC_OK;
+}
+template int launch_ref_to_soa<double, double>(msc_plan*, const double2*, double2*);
+template int launch_ref_to_soa<double, float>(msc_plan*, const double2*, float2*);
+template int launch_ref_to_soa<float, float>(msc_plan*, const float2*, float2*);
+template int launch_soa_to_ref<double, double>(msc_plan*, const double2*, double2*);
+template int launch_soa_to_ref<float, float>(msc_plan*, const float2*, float2*);
+template int launch_soa_to_ref<float, double>(msc_plan*, const float2*, double2*);
+
+// ---- G0 spectrum -----------------------------------------------------------------------
+__global__ void k_va_blocks(double* out, double alpha, double beta, double rho, double omega, int n_orders) {
+  const int t = threadIdx.x;
+  if (t >= 27 || t == 13) return;
+  const int R[3] = {t / 9 - 1, (t / 3) % 3 - 1, t % 3 - 1};
+  const int slot = t < 13 ? t : t - 1;
+  va_block(R, alpha, beta, rho, omega, n_orders, out + slot * 81);
+}
+
+__device__ __forceinline__ int va_slot(int dz, int dx, int dy) {
+  const int t = (dz + 1) * 9 + (dx + 1) * 3 + (dy + 1);
+  return t < 13 ? t : t - 1;
+}
+
+// Lattice offsets of padded index u along an axis of length L for a lattice of n:
+// aperiodic: u < n -> u; u > L - n -> u - L; periodic (L == n): u and u - n (u > 0).
+__device__ __forceinline__ int axis_offsets(int u, int L, int n, bool periodic, int* o) {
+  if (periodic) {
+    o[0] = u;
+    if (u > 0) { o[1] = u - n; return 2; }
+    return 1;
+  }
+  if (u < n) { o[0] = u; return 1; }
+  if (u > L - n) { o[0] = u - L; return 1; }
+  return 0;
+}
+
+struct G0Params {
+  Geo g;
+  double d, omega, alpha, beta, rho;
+  int periodic, va, E;
+  int bloch;
+  double kx, ky;   // Bloch wavevector (rad/m)
+  double scale;    // 1/(Lz Lx Ly)
+};
+
+// Spatial kernel entry e at padded point (z, y, x): sum over the images of the
+// point (or volume-averaged) propagator; SYM stores (K D)_ij for i <= j.
+__global__ void k_g0_spatial(double2* __restrict__ Ks, const double* __restrict__ vab, G0Params p) {
+  const Geo& g = p.g;
+  const long long npts = (long long)g.Lz * g.Ly * g.Lx;
+  const long long gid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const int e = blockIdx.y;
+  if (gid >= npts) return;
+  const int x = (int)(gid % g.Lx);
+  const int y = (int)((gid / g.Lx) % g.Ly);
+  const int z = (int)(gid / ((long long)g.Lx * g.Ly));
+  int a, b;
+  if (p.E == 45) {
+    int ee = e, i = 0;
+    while (ee >= 9 - i) { ee -= 9 - i; ++i; }
+    a = i;
+    b = i + ee;
+  } else {
+    a = e / 9;
+    b = e % 9;
+  }
+  int oz[2], ox[2], oy[2];
+  const int nz = axis_offsets(z, g.Lz, g.Nz, false, oz);
+  const int nx = axis_offsets(x, g.Lx, g.M, p.periodic, ox);
+  const int ny = axis_offsets(y, g.Ly, g.M, p.periodic, oy);
+  double2 acc = make_double2(0, 0);
+  for (int iz = 0; iz < nz; ++iz)
+    for (int ix = 0; ix < nx; ++ix)
+      for (int iy = 0; iy < ny; ++iy) {
+        const int dz = oz[iz], dx = ox[ix], dy = oy[iy];
+        if (dz == 0 && dx == 0 && dy == 0) continue;  // self term
+        double2 v;
+        if (p.va && abs(dz) <= 1 && abs(dx) <= 1 && abs(dy) <= 1) {
+          v = make_double2(vab[va_slot(dz, dx, dy) * 81 + a * 9 + b], 0.0);
+        } else {
+          PointProp pp;
+          pp.init(dz * p.d, dx * p.d, dy * p.d, p.omega, p.alpha, p.beta, p.rho);
+          v = pp.entry(a, b);
+        }
+        if (p.bloch) {
+          double s, c;
+          sincos(-(p.kx * dx + p.ky * dy) * p.d, &s, &c);
+          v = v * make_double2(c, s);
+        }
+        acc += v;
+      }
+  double f = p.scale;
+  if (p.E == 45 && b >= 6) f *= 2.0;  // (K D)_ij = K_ij D_j
+  Ks[(size_t)e * npts + gid] = make_double2(f * acc.x, f * acc.y);
+}
+
+// Strided line FFT: element idx of column col in slab (s1, s2) is at
+// base + s1*S1 + s2*S2 + idx*es + col. Output either in place (idx < n_out) or,
+// when TRANS, to out[(s2*O2 + s1*O1 + col) * L + idx] (and a complex64 copy).
+template <typename T, int DIR, int KMAX, bool TRANS>
+__global__ void __launch_bounds__(256) k_fft_strided(cx<T>* data, long long es, int ncol, long long S1, long long S2,
+                                                     int n_in, int n_out, FftPlan1D pl, const cx<T>* __restrict__ twg,
+                                                     cx<T>* out, float2* out32, long long O1, long long O2) {
+  constexpr int TC = 128 / (int)sizeof(cx<T>);
+  constexpr int P = TC + 1;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  cx<T>* tw = reinterpret_cast<cx<T>*>(smem_raw);
+  cx<T>* tile = tw + pl.L;
+  const int tid = threadIdx.x, nthr = blockDim.x;
+  const int col0 = blockIdx.x * TC;
+  const int nc = min(TC, ncol - col0);
+  const long long base = (long long)blockIdx.y * S1 + (long long)blockIdx.z * S2 + col0;
+  for (int t = tid; t < pl.L; t += nthr) tw[t] = twg[t];
+  for (int it = tid; it < TC * pl.L; it += nthr) {
+    const int t = it % TC, idx = it / TC;
+    tile[idx * P + t] = (t < nc && idx < n_in) ? data[base + idx * es + t] : czero<cx<T>>();
+  }
+  __syncthreads();
+  fft_tile<DIR, KMAX>(tile, P, TC, pl, tw, tid, nthr);
+  if (!TRANS) {
+    for (int it = tid; it < TC * n_out; it += nthr) {
+      const int t = it % TC, idx = it / TC;
+      if (t < nc) data[base + idx * es + t] = tile[idx * P + t];
+    }
+  } else {
+    const long long ob = (long long)blockIdx.z * O2 + (long long)blockIdx.y * O1 + col0;
+    for (int it = tid; it < TC * pl.L; it += nthr) {
+      const int idx = it % pl.L, t = it / pl.L;
+      if (t < nc) {
+        const cx<T> v = tile[idx * P + t];
+        out[(ob + t) * pl.L + idx] = v;
+        if (out32) out32[(ob + t) * pl.L + idx] = make_float2((float)v.x, (float)v.y);
+      }
+    }
+  }
+}
+
+template <bool TRANS>
+static int launch_fft_strided64(msc_plan* pl, double2* data, long long es, int ncol, long long S1, int n1, long long S2,
+                                int n2, int n_in, int n_out, const FftPlan1D& f, const double2* tw, double2* out,
+                                float2* out32, long long O1, long long O2) {
+  constexpr int TC = 8;
+  const int nthr = 256;
+  const size_t sm = sizeof(double2) * ((size_t)f.L + (size_t)f.L * (TC + 1));
+  const int kmax = fft_kmax_needed(f, TC, nthr);
+  dim3 grid((unsigned)((ncol + TC - 1) / TC), (unsigned)n1, (unsigned)n2);
+#define CALL(K)                                                                                               \
+  {                                                                                                           \
+    auto kern = k_fft_strided<double, -1, K, TRANS>;                                                          \
+    MSC_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));               \
+    kern<<<grid, nthr, sm, pl->stream>>>(data, es, ncol, S1, S2, n_in, n_out, f, tw, out, out32, O1, O2);     \
+  }
+  if (kmax <= 1) CALL(1) else if (kmax <= 2) CALL(2) else if (kmax <= 4) CALL(4) else if (kmax <= 8) CALL(8) else {
+    set_error("strided FFT needs KMAX=%d", kmax);
+    return MSC_ERR_UNSUPPORTED;
+  }
+#undef CALL
+  MSC_CUDA(cudaGetLastError());
+  return MSC_OK;
+}
+
+int launch_g0(msc_plan* pl, double omega, const double* kpar, int va, int n_orders) {
+  // The Bloch-phased kernel loses the parity K(-r) = S K(r) S, so its spectrum is
+  // stored on the full (kx, ky) plane; otherwise on the half plane ky <= Ly/2.
+  pl->g.half = kpar ? 0 : 1;
+  pl->g.Hy = pl->g.half ? pl->g.Ly / 2 + 1 : pl->g.Ly;
+  const Geo& g = pl->g;
+  const int E = va ? 81 : 45;
+  if (pl->khat64.p && pl->E != E) {
+    dfree(pl, pl->khat64);
+    dfree(pl, pl->khat32);
+  }
+  pl->E = E;
+  MSC_TRY(dalloc(pl, pl->khat64, sizeof(double2) * khat_elems(g, E)));
+  MSC_TRY(dalloc(pl, pl->khat32, sizeof(float2) * khat_elems(g, E)));
+  MSC_TRY(dalloc(pl, pl->va_blocks, sizeof(double) * 26 * 81));
+  const long long npts = (long long)g.Lz * g.Ly * g.Lx;
+  DBuf ks;
+  MSC_TRY(dalloc(pl, ks, sizeof(double2) * (size_t)E * npts));
+  if (va) {
+    k_va_blocks<<<1, 32, 0, pl->stream>>>((double*)pl->va_blocks.p, pl->desc.alpha, pl->desc.beta, pl->desc.rho, omega,
+                                          n_orders);
+    MSC_CUDA(cudaGetLastError());
+  }
+  G0Params p;
+  p.g = g;
+  p.d = 2.0 * pl->desc.a;
+  p.omega = omega;
+  p.alpha = pl->desc.alpha;
+  p.beta = pl->desc.beta;
+  p.rho = pl->desc.rho;
+  p.periodic = pl->desc.periodic;
+  p.va = va;
+  p.E = E;
+  p.bloch = kpar != nullptr;
+  p.kx = kpar ? kpar[0] : 0.0;
+  p.ky = kpar ? kpar[1] : 0.0;
+  p.scale = 1.0 / ((double)g.Lz * g.Lx * g.Ly);
+  dim3 grid((unsigned)ceil_div(npts, 128), (unsigned)E);
+  k_g0_spatial<<<grid, 128, 0, pl->stream>>>((double2*)ks.p, (const double*)pl->va_blocks.p, p);
+  MSC_CUDA(cudaGetLastError());
+  double2* K = (double2*)ks.p;
+  const double2* twxy = (const double2*)pl->tw64_xy.p;
+  const double2* twz = (const double2*)pl->tw64_z.p;
+  // x pass (contiguous lines), in place
+  int s = launch_fft_contig<double>(pl, K, K, (long long)E * g.Lz * g.Ly, g.Lx, g.Lx, g.Lx, g.Lx, pl->fxy, twxy, -1,
+                                    nullptr);
+  // y pass: axis stride Lx, columns x, slabs (z, e); keep ky < Hy
+  if (s == MSC_OK)
+    s = launch_fft_strided64<false>(pl, K, g.Lx, g.Lx, (long long)g.Ly * g.Lx, g.Lz, (long long)g.Lz * g.Ly * g.Lx, E,
+                                    g.Ly, g.Hy, pl->fxy, twxy, nullptr, nullptr, 0, 0);
+  // z pass: axis stride Ly*Lx, columns kx, slabs (ky < Hy, e); transposed store to khat[e][ky][kx][kz]
+  if (s == MSC_OK)
+    s = launch_fft_strided64<true>(pl, K, (long long)g.Ly * g.Lx, g.Lx, g.Lx, g.Hy, (long long)g.Lz * g.Ly * g.Lx, E,
+                                   g.Lz, g.Lz, pl->fz, twz, (double2*)pl->khat64.p, (float2*)pl->khat32.p, g.Lx,
+                                   (long long)g.Hy * g.Lx);
+  // the scratch is released after the stream drains (cudaFreeAsync keeps stream order)
+  if (ks.p) {
+    cudaFreeAsync(ks.p, pl->stream);
+    pl->bytes -= (int64_t)ks.bytes;
+    ks.p = nullptr;
+  }
+  return s;
+}
+
+}  // namespace msc

@@ -1,0 +1,546 @@
+"""Slab Foldy-Lax solver on B200: the reference-facing Python API.
+
+A drop-in for ``cubic_scattering.slab_scattering_gpu.compute_slab_scattering_gpu``
+and the helpers callers use with it (tmnestor/MultipleScatteringCalculations
+``cubic_scattering/slab_scattering.py`` and ``slab_scattering_gpu.py``): the same
+dataclasses, argument names, conventions and errors, with every numeric step
+running in the hand-written sm_100a kernels of ``libmsc_b200.so``. PyTorch
+provides device memory and the stream; it computes nothing here.
+
+Conventions (the reference's): axes (z, x, y) with z down; 9 DOF per voxel
+[u_z, u_x, u_y, e_zz, e_xx, e_yy, 2e_xy, 2e_zy, 2e_zx]; fields (N_z, M, M, 9);
+``SlabGeometry.a`` is the cube half-width, d = 2a.
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+import warnings
+from dataclasses import dataclass, field
+from typing import Callable
+
+import numpy as np
+import torch
+from numpy.typing import NDArray
+
+from . import _native as N
+
+__all__ = [
+    "MaterialContrast",
+    "ReferenceMedium",
+    "SlabGeometry",
+    "SlabMaterial",
+    "SlabPlan",
+    "SlabResult",
+    "compute_slab_scattering_gpu",
+    "compute_slab_tmatrices",
+    "gaussian_random_field_material",
+    "random_slab_material",
+    "slab_reflected_field",
+    "slab_rpp_periodic",
+    "uniform_slab_material",
+]
+
+
+# ---------------------------------------------------------------------------
+# Data types (effective_contrasts.py:40-68, slab_scattering.py:40-161)
+# ---------------------------------------------------------------------------
+
+
+@dataclass
+class ReferenceMedium:
+    """Isotropic elastic background: P speed alpha, S speed beta, density rho."""
+
+    alpha: float
+    beta: float
+    rho: float
+
+    @property
+    def lam(self) -> float:
+        return self.rho * (self.alpha**2 - 2 * self.beta**2)
+
+    @property
+    def mu(self) -> float:
+        return self.rho * self.beta**2
+
+
+@dataclass
+class MaterialContrast:
+    """Isotropic contrast (Delta lambda, Delta mu in Pa; Delta rho in kg/m^3)."""
+
+    Dlambda: float
+    Dmu: float
+    Drho: float
+
+
+@dataclass
+class SlabGeometry:
+    """M x M x N_z lattice of cubes of half-width a (slab_scattering.py:40-99)."""
+
+    M: int
+    N_z: int
+    a: float
+
+    def __post_init__(self) -> None:
+        if self.M < 1:
+            raise ValueError(f"M must be >= 1, got {self.M}")
+        if self.N_z < 1:
+            raise ValueError(f"N_z must be >= 1, got {self.N_z}")
+        if self.a <= 0:
+            raise ValueError(f"a must be > 0, got {self.a}")
+
+    @property
+    def d(self) -> float:
+        return 2.0 * self.a
+
+    @property
+    def n_cubes(self) -> int:
+        return self.M * self.M * self.N_z
+
+    def cube_centre(self, lz: int, i: int, j: int) -> NDArray[np.floating]:
+        d = self.d
+        return np.array([(lz + 0.5) * d, (i - (self.M - 1) / 2.0) * d, (j - (self.M - 1) / 2.0) * d])
+
+    def all_centres(self) -> NDArray[np.floating]:
+        d = self.d
+        z = (np.arange(self.N_z) + 0.5) * d
+        x = (np.arange(self.M) - (self.M - 1) / 2.0) * d
+        zz, xx, yy = np.meshgrid(z, x, x, indexing="ij")
+        return np.stack([zz, xx, yy], axis=-1)
+
+
+@dataclass
+class SlabMaterial:
+    """Per-cube contrasts, each (N_z, M, M) (slab_scattering.py:102-133)."""
+
+    Dlambda: NDArray
+    Dmu: NDArray
+    Drho: NDArray
+    ref: ReferenceMedium
+
+    def __post_init__(self) -> None:
+        if self.Dlambda.shape != self.Dmu.shape or self.Dlambda.shape != self.Drho.shape:
+            raise ValueError(
+                f"Contrast array shapes must match: Dlambda={self.Dlambda.shape}, "
+                f"Dmu={self.Dmu.shape}, Drho={self.Drho.shape}"
+            )
+        if self.Dlambda.ndim != 3:
+            raise ValueError(f"Contrast arrays must be 3D (N_z, M, M), got ndim={self.Dlambda.ndim}")
+
+
+@dataclass
+class SlabResult:
+    """Solved slab (slab_scattering.py:136-161). ``t0`` (extra) holds the four
+    T0 scalars per voxel (4, N_z, M, M) so callers need not rebuild T0; ``stats``
+    (extra) has the solver counters."""
+
+    psi: NDArray
+    psi0: NDArray
+    geometry: SlabGeometry
+    material: SlabMaterial
+    omega: float
+    k_hat: NDArray
+    wave_type: str
+    n_gmres_iter: int
+    gmres_residual: float
+    periodic: bool = False
+    t0: NDArray | None = None
+    bloch: bool = False
+    stats: dict = field(default_factory=dict)
+
+
+# ---------------------------------------------------------------------------
+# Plan: one geometry on one device
+# ---------------------------------------------------------------------------
+
+
+def _device(device) -> torch.device:
+    if device is None:
+        if not torch.cuda.is_available():
+            raise RuntimeError("compute_slab_scattering_gpu needs a CUDA device (sm_100a); none is available")
+        return torch.device("cuda", torch.cuda.current_device())
+    device = torch.device(device)
+    if device.type != "cuda":
+        raise ValueError(f"this solver runs on CUDA devices only, got device={device}")
+    if device.index is None:
+        device = torch.device("cuda", torch.cuda.current_device())
+    return device
+
+
+def _ptr(t: torch.Tensor) -> int:
+    return t.data_ptr()
+
+
+class SlabPlan:
+    """Owns a native plan (FFT sizes, T0, G0 spectrum, workspaces) for one slab
+    geometry and background medium on one CUDA device."""
+
+    def __init__(self, geometry: SlabGeometry, ref: ReferenceMedium, *, periodic: bool = False, device=None,
+                 Lz: int = 0, Lxy: int = 0):
+        self.lib = N.load()
+        self.geometry = geometry
+        self.ref = ref
+        self.periodic = bool(periodic)
+        self.device = _device(device)
+        self._handle = C.c_void_p()
+        with torch.cuda.device(self.device):
+            self.stream = torch.cuda.current_stream(self.device)
+            desc = N.SlabDesc(geometry.M, geometry.N_z, float(geometry.a), float(ref.alpha), float(ref.beta),
+                              float(ref.rho), int(self.periodic), int(Lz), int(Lxy))
+            N.check(self.lib.msc_plan_create(C.byref(desc), C.c_void_p(self.stream.cuda_stream),
+                                             C.byref(self._handle)), "msc_plan_create")
+        self.omega: float | None = None
+        self.kpar: tuple[float, float] | None = None
+
+    @property
+    def handle(self) -> C.c_void_p:
+        if not self._handle:
+            raise RuntimeError("plan was released")
+        return self._handle
+
+    def close(self) -> None:
+        if getattr(self, "_handle", None):
+            self.lib.msc_plan_destroy(self._handle)
+            self._handle = C.c_void_p()
+
+    def __del__(self):  # pragma: no cover - finaliser
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def fft_sizes(self) -> tuple[int, int, int]:
+        out = (C.c_int32 * 3)()
+        N.check(self.lib.msc_plan_fft_sizes(self.handle, out), "msc_plan_fft_sizes")
+        return tuple(out)
+
+    def device_bytes(self) -> int:
+        return int(self.lib.msc_plan_device_bytes(self.handle))
+
+    def _dev(self, a, dtype) -> torch.Tensor:
+        if isinstance(a, torch.Tensor):
+            return a.to(device=self.device, dtype=dtype).contiguous()
+        return torch.from_numpy(np.ascontiguousarray(a)).to(device=self.device, dtype=dtype)
+
+    def build_t0(self, material: SlabMaterial, omega: float) -> None:
+        g = self.geometry
+        shp = (g.N_z, g.M, g.M)
+        for arr in (material.Dlambda, material.Dmu, material.Drho):
+            if tuple(arr.shape) != shp:
+                raise ValueError(f"material arrays must have shape {shp}, got {tuple(arr.shape)}")
+        dl = self._dev(material.Dlambda, torch.float64)
+        dm = self._dev(material.Dmu, torch.float64)
+        dr = self._dev(material.Drho, torch.float64)
+        N.check(self.lib.msc_build_t0(self.handle, _ptr(dl), _ptr(dm), _ptr(dr), float(omega)), "msc_build_t0")
+        self._keep = (dl, dm, dr)
+        self.omega = float(omega)
+
+    def set_t0_scalars(self, t4, omega: float) -> None:
+        t = self._dev(t4, torch.complex128)
+        N.check(self.lib.msc_set_t0_scalars(self.handle, _ptr(t), float(omega)), "msc_set_t0_scalars")
+        self._keep_t4 = t
+
+    def t0_scalars(self) -> torch.Tensor:
+        g = self.geometry
+        out = torch.empty((4, g.N_z, g.M, g.M), dtype=torch.complex128, device=self.device)
+        N.check(self.lib.msc_t0_scalars(self.handle, _ptr(out)), "msc_t0_scalars")
+        return out
+
+    def build_g0(self, omega: float, *, kpar=None, volume_averaged: bool = False, n_orders: int = 2) -> None:
+        kp = None
+        if kpar is not None:
+            kp = (C.c_double * 2)(float(kpar[0]), float(kpar[1]))
+        N.check(self.lib.msc_build_g0(self.handle, float(omega), kp, int(bool(volume_averaged)), int(n_orders)),
+                "msc_build_g0")
+        self.kpar = None if kpar is None else (float(kpar[0]), float(kpar[1]))
+
+    def incident(self, omega: float, k_hat, wave_type: str) -> torch.Tensor:
+        if wave_type not in ("P", "S"):
+            raise ValueError(f"wave_type must be 'P' or 'S', got '{wave_type}'")
+        g = self.geometry
+        kh = (C.c_double * 3)(*[float(v) for v in np.asarray(k_hat, dtype=float).ravel()[:3]])
+        out = torch.empty((g.N_z, g.M, g.M, 9), dtype=torch.complex128, device=self.device)
+        N.check(self.lib.msc_incident(self.handle, float(omega), kh, N.MSC_WAVE_P if wave_type == "P" else N.MSC_WAVE_S,
+                                      _ptr(out)), "msc_incident")
+        return out
+
+    def matvec(self, x: torch.Tensor, precision: str = "complex128") -> torch.Tensor:
+        """(I - G0 T0) x for x (N_z, M, M, 9) on the device."""
+        dt = torch.complex128 if precision == "complex128" else torch.complex64
+        xx = x.to(device=self.device, dtype=dt).contiguous()
+        y = torch.empty_like(xx)
+        N.check(self.lib.msc_matvec(self.handle, _ptr(xx), _ptr(y),
+                                    N.MSC_COMPLEX128 if dt == torch.complex128 else N.MSC_COMPLEX64), "msc_matvec")
+        return y
+
+    def solve(self, b: torch.Tensor, *, tol: float, max_iter: int, restart: int = 30, precision: str = "mixed",
+              initial_guess: str = "born", inner_tol: float = 0.0, x: torch.Tensor | None = None):
+        """Solve (I - G0 T0) x = b; returns (x, stats dict)."""
+        if precision not in ("mixed", "fp64"):
+            raise ValueError(f"precision must be 'mixed' or 'fp64', got {precision!r}")
+        bb = b.to(device=self.device, dtype=torch.complex128).contiguous()
+        xx = torch.empty_like(bb) if x is None else x
+        opts = N.SolveOpts(float(tol), int(max_iter), int(restart),
+                           N.MSC_SOLVE_MIXED if precision == "mixed" else N.MSC_SOLVE_FP64,
+                           0 if initial_guess == "born" else 1, float(inner_tol))
+        st = N.SolveStats()
+        status = N.check(self.lib.msc_solve(self.handle, _ptr(bb), _ptr(xx), C.byref(opts), C.byref(st)), "msc_solve")
+        stats = {"n_matvec": st.n_matvec, "n_matvec64": st.n_matvec64, "n_outer": st.n_outer, "status": status,
+                 "residual": st.residual}
+        return xx, stats
+
+    def rpp_periodic(self, psi: torch.Tensor, omega: float, p: float = 0.0, bloch: bool = False) -> complex:
+        pp = psi.to(device=self.device, dtype=torch.complex128).contiguous()
+        out = (C.c_double * 2)()
+        N.check(self.lib.msc_rpp_periodic(self.handle, _ptr(pp), float(omega), float(p), int(bool(bloch)), out),
+                "msc_rpp_periodic")
+        return complex(out[0], out[1])
+
+    def reflected_field(self, psi: torch.Tensor, omega: float, k_hat) -> tuple[complex, complex, complex]:
+        pp = psi.to(device=self.device, dtype=torch.complex128).contiguous()
+        kh = (C.c_double * 3)(*[float(v) for v in np.asarray(k_hat, dtype=float).ravel()[:3]])
+        out = (C.c_double * 6)()
+        N.check(self.lib.msc_reflected_field(self.handle, _ptr(pp), float(omega), kh, out), "msc_reflected_field")
+        return complex(out[0], out[1]), complex(out[2], out[3]), complex(out[4], out[5])
+
+
+# ---------------------------------------------------------------------------
+# T0 in the reference's (N_z, M, M, 9, 9) form
+# ---------------------------------------------------------------------------
+
+
+def t0_expand(t4: NDArray) -> NDArray:
+    """(4, ...) scalars -> (..., 9, 9) T-matrices."""
+    t_u, t_l, t_d, t_s = t4
+    T = np.zeros(t_u.shape + (9, 9), dtype=complex)
+    for i in range(3):
+        T[..., i, i] = t_u
+        T[..., 6 + i, 6 + i] = t_s
+        for j in range(3):
+            T[..., 3 + i, 3 + j] = t_l + (t_d if i == j else 0.0)
+    return T
+
+
+def t0_compress(T: NDArray) -> NDArray:
+    """(..., 9, 9) T-matrices of the cube form -> (4, ...) scalars."""
+    T = np.asarray(T)
+    t_l = T[..., 3, 4]
+    return np.stack([T[..., 0, 0], t_l, T[..., 3, 3] - t_l, T[..., 6, 6]])
+
+
+def compute_slab_tmatrices(geometry: SlabGeometry, material: SlabMaterial, omega: float, *, device=None) -> NDArray:
+    """Per-cube 9x9 T-matrices (N_z, M, M, 9, 9), built on the GPU (replaces
+    ``compute_slab_tmatrices``, slab_scattering.py:169-205)."""
+    plan = SlabPlan(geometry, material.ref, device=device)
+    try:
+        plan.build_t0(material, omega)
+        t4 = plan.t0_scalars().cpu().numpy()
+    finally:
+        plan.close()
+    return t0_expand(t4)
+
+
+# ---------------------------------------------------------------------------
+# Solve (slab_scattering_gpu.py:158-266)
+# ---------------------------------------------------------------------------
+
+
+def _bloch_kpar(omega: float, ref: ReferenceMedium, k_hat, wave_type: str) -> tuple[float, float]:
+    kh = np.asarray(k_hat, dtype=float)
+    kh = kh / np.linalg.norm(kh)
+    k = omega / (ref.alpha if wave_type == "P" else ref.beta)
+    return float(k * kh[1]), float(k * kh[2])
+
+
+def compute_slab_scattering_gpu(
+    geometry: SlabGeometry,
+    material: SlabMaterial,
+    omega: float,
+    k_hat: NDArray,
+    wave_type: str = "P",
+    gmres_tol: float = 1e-6,
+    max_iter: int = 500,
+    initial_guess: str = "born",
+    device=None,
+    dtype=None,
+    *,
+    volume_averaged: bool = False,
+    n_orders: int = 2,
+    periodic: bool = False,
+    restart: int = 30,
+    precision: str = "mixed",
+    preconditioner=None,
+    bloch: bool = False,
+    inner_tol: float = 0.0,
+    plan: SlabPlan | None = None,
+) -> SlabResult:
+    """Solve (I - G0 T0) psi = psi0 on the GPU.
+
+    Arguments as the reference's ``compute_slab_scattering_gpu``; keyword-only
+    additions: ``restart`` (GMRES(m)), ``precision`` ("mixed": complex64 inner
+    GMRES inside FP64 iterative refinement, "fp64": plain complex128 GMRES),
+    ``bloch`` (periodic only: Bloch-phased lateral fold for oblique incidence;
+    False is the reference's phase-free fold), ``inner_tol`` and ``plan`` (reuse
+    a plan of the same geometry). ``dtype`` is accepted for compatibility
+    (complex64 or complex128); the arithmetic is set by ``precision`` and the
+    returned field is always complex128 with its FP64 true residual.
+    ``preconditioner`` must be None.
+    """
+    if wave_type not in ("P", "S"):
+        raise ValueError(f"wave_type must be 'P' or 'S', got '{wave_type}'")
+    if dtype is not None and dtype not in (torch.complex64, torch.complex128):
+        raise ValueError(f"dtype must be torch.complex64 or torch.complex128, got {dtype}")
+    if preconditioner is not None:
+        raise ValueError("preconditioner must be None in this version")
+    if bloch and not periodic:
+        raise ValueError("bloch=True needs periodic=True")
+    own = plan is None
+    if own:
+        plan = SlabPlan(geometry, material.ref, periodic=periodic, device=device)
+    elif plan.periodic != bool(periodic) or plan.geometry != geometry:
+        raise ValueError("plan geometry/periodicity does not match the problem")
+    try:
+        kp = _bloch_kpar(omega, material.ref, k_hat, wave_type) if bloch else None
+        plan.build_t0(material, omega)
+        plan.build_g0(omega, kpar=kp, volume_averaged=volume_averaged, n_orders=n_orders)
+        psi0 = plan.incident(omega, k_hat, wave_type)
+        x, st = plan.solve(psi0, tol=gmres_tol, max_iter=max_iter, restart=restart, precision=precision,
+                           initial_guess=initial_guess, inner_tol=inner_tol)
+        if st["residual"] > gmres_tol:
+            warnings.warn(
+                f"GPU GMRES did not converge: rel_res={st['residual']:.2e} after {st['n_matvec']} matvecs",
+                stacklevel=2,
+            )
+        t4 = plan.t0_scalars()
+        psi = x.cpu().numpy()
+        res = SlabResult(
+            psi=psi,
+            psi0=psi0.cpu().numpy(),
+            geometry=geometry,
+            material=material,
+            omega=float(omega),
+            k_hat=np.asarray(k_hat, dtype=float),
+            wave_type=wave_type,
+            n_gmres_iter=int(st["n_matvec"]),
+            gmres_residual=float(st["residual"]),
+            periodic=bool(periodic),
+            t0=t4.cpu().numpy(),
+            bloch=bool(bloch),
+            stats=st,
+        )
+        return res
+    finally:
+        if own:
+            plan.close()
+
+
+# ---------------------------------------------------------------------------
+# Observables (slab_scattering.py:589-735)
+# ---------------------------------------------------------------------------
+
+
+def _observable_plan(result: SlabResult, T_local, device) -> SlabPlan:
+    plan = SlabPlan(result.geometry, result.material.ref, periodic=result.periodic, device=device)
+    t4 = t0_compress(T_local) if np.ndim(T_local) == 5 else np.asarray(T_local)
+    plan.set_t0_scalars(t4, result.omega)
+    if result.bloch:
+        plan.build_g0(result.omega, kpar=_bloch_kpar(result.omega, result.material.ref, result.k_hat,
+                                                     result.wave_type))
+    return plan
+
+
+def slab_rpp_periodic(result: SlabResult, T_local, *, p: float = 0.0, device=None) -> complex:
+    """Specular P->P reflection of a periodic slab by the Weyl sum (replaces
+    ``slab_rpp_periodic``, slab_scattering.py:672-735). ``T_local`` is the
+    (N_z, M, M, 9, 9) T-matrices or the (4, N_z, M, M) scalars. For a result
+    solved with ``bloch=True`` the sources are demodulated by the Bloch phase."""
+    plan = _observable_plan(result, T_local, device)
+    try:
+        return plan.rpp_periodic(torch.from_numpy(np.ascontiguousarray(result.psi)), result.omega, p, result.bloch)
+    finally:
+        plan.close()
+
+
+def slab_reflected_field(result: SlabResult, T_local, *, device=None) -> tuple[complex, complex, complex]:
+    """(R_PP, R_PS, R_SP) far-field amplitudes per unit area (replaces
+    ``slab_reflected_field``, slab_scattering.py:589-669)."""
+    plan = _observable_plan(result, T_local, device)
+    try:
+        return plan.reflected_field(torch.from_numpy(np.ascontiguousarray(result.psi)), result.omega, result.k_hat)
+    finally:
+        plan.close()
+
+
+# ---------------------------------------------------------------------------
+# Material generators (slab_scattering.py:791-852) and the Gaussian random field
+# ---------------------------------------------------------------------------
+
+
+def random_slab_material(geometry: SlabGeometry, ref: ReferenceMedium, contrast: MaterialContrast,
+                         phi: float | Callable[[int], float], seed: int | None = None) -> SlabMaterial:
+    """Binary random slab: each cube is an inclusion with probability phi
+    (per layer if callable), drawn layer by layer from default_rng(seed) exactly
+    as the reference does, so the same seed gives the same material."""
+    rng = np.random.default_rng(seed)
+    shape = (geometry.N_z, geometry.M, geometry.M)
+    dl = np.zeros(shape)
+    dm = np.zeros(shape)
+    dr = np.zeros(shape)
+    for lz in range(geometry.N_z):
+        p = phi(lz) if callable(phi) else phi
+        mask = rng.random((geometry.M, geometry.M)) < p
+        dl[lz, mask] = contrast.Dlambda
+        dm[lz, mask] = contrast.Dmu
+        dr[lz, mask] = contrast.Drho
+    return SlabMaterial(Dlambda=dl, Dmu=dm, Drho=dr, ref=ref)
+
+
+def uniform_slab_material(geometry: SlabGeometry, ref: ReferenceMedium, contrast: MaterialContrast) -> SlabMaterial:
+    """Every cube with the same contrast."""
+    shape = (geometry.N_z, geometry.M, geometry.M)
+    return SlabMaterial(Dlambda=np.full(shape, contrast.Dlambda), Dmu=np.full(shape, contrast.Dmu),
+                        Drho=np.full(shape, contrast.Drho), ref=ref)
+
+
+def uniform_random_material(geometry: SlabGeometry, ref: ReferenceMedium, fraction: float,
+                            seed: int | None = None) -> SlabMaterial:
+    """i.i.d. U(-fraction, fraction) relative contrasts of (lambda0, mu0, rho0),
+    drawn in that order, each (N_z, M, M), from default_rng(seed)."""
+    rng = np.random.default_rng(seed)
+    shp = (geometry.N_z, geometry.M, geometry.M)
+    dl = rng.uniform(-fraction, fraction, shp) * ref.lam
+    dm = rng.uniform(-fraction, fraction, shp) * ref.mu
+    dr = rng.uniform(-fraction, fraction, shp) * ref.rho
+    return SlabMaterial(Dlambda=dl, Dmu=dm, Drho=dr, ref=ref)
+
+
+def gaussian_random_field(shape: tuple[int, int, int], correlation_length: float, rng: np.random.Generator,
+                          ) -> NDArray:
+    """Zero-mean unit-variance Gaussian random field on (N_z, M, M) with
+    covariance exp(-r^2 / l^2) (l in cells): white noise filtered by sqrt(S(k)),
+    S(k) = exp(-k^2 l^2 / 4); periodic in x and y, z padded by 3 l so the field
+    does not wrap vertically."""
+    nz, m1, m2 = shape
+    pad = int(np.ceil(3.0 * correlation_length))
+    Lz = nz + pad
+    w = rng.standard_normal((Lz, m1, m2))
+    kz = 2 * np.pi * np.fft.fftfreq(Lz)
+    kx = 2 * np.pi * np.fft.fftfreq(m1)
+    ky = 2 * np.pi * np.fft.fftfreq(m2)
+    k2 = kz[:, None, None] ** 2 + kx[None, :, None] ** 2 + ky[None, None, :] ** 2
+    f = np.fft.ifftn(np.fft.fftn(w) * np.exp(-k2 * correlation_length**2 / 8.0)).real[:nz]
+    f = f - f.mean()
+    sd = f.std()
+    return f / sd if sd > 0 else f
+
+
+def gaussian_random_field_material(geometry: SlabGeometry, ref: ReferenceMedium, *, correlation_length: float,
+                                   std: float, seed: int | None = None, clip: float = 0.9) -> SlabMaterial:
+    """Contrasts Delta lambda, Delta mu, Delta rho as independent Gaussian random
+    fields (drawn in that order from default_rng(seed)) of relative standard
+    deviation ``std`` and correlation length ``correlation_length`` cells,
+    clipped to +-``clip`` of (lambda0, mu0, rho0) so the medium stays positive."""
+    rng = np.random.default_rng(seed)
+    shp = (geometry.N_z, geometry.M, geometry.M)
+    fr = [np.clip(std * gaussian_random_field(shp, correlation_length, rng), -clip, clip) for _ in range(3)]
+    return SlabMaterial(Dlambda=fr[0] * ref.lam, Dmu=fr[1] * ref.mu, Drho=fr[2] * ref.rho, ref=ref)

@@ -1,0 +1,273 @@
+"""GPU parity of the CUDA path (through the C-ABI) with the oracle and the
+reference's golden fixtures. Tolerances follow the reference tests
+(tests/test_slab_scattering.py:259-273, 663-718; test_slab_scattering_gpu.py:45-141):
+complex128 operator rtol 1e-10; complex64 operator rtol 2e-5 (FP32 FFT/accumulate);
+solves judged by the FP64 true residual and the relative error of psi and R_PP.
+"""
+
+import numpy as np
+import pytest
+import torch
+from numpy.testing import assert_allclose
+
+from oracle import slab_oracle as O
+
+pytestmark = pytest.mark.gpu
+
+if not torch.cuda.is_available():  # pragma: no cover
+    pytest.skip("needs a CUDA device", allow_module_level=True)
+
+from multiplescatteringcalculations_b200 import (  # noqa: E402
+    MaterialContrast,
+    ReferenceMedium,
+    SlabGeometry,
+    SlabMaterial,
+    SlabPlan,
+    compute_slab_scattering_gpu,
+    compute_slab_tmatrices,
+    random_slab_material,
+    slab_reflected_field,
+    slab_rpp_periodic,
+    t0_expand,
+    uniform_random_material,
+    uniform_slab_material,
+)
+
+REF = ReferenceMedium(5000.0, 3000.0, 2500.0)
+CONTRAST = MaterialContrast(2e9, 1e9, 100.0)
+OMEGA = 0.05 * REF.beta / 1.0
+KZ = np.array([1.0, 0.0, 0.0])
+
+
+def _medium(z):
+    return ReferenceMedium(*[float(v) for v in z["medium"]])
+
+
+def _rel(a, b):
+    return np.linalg.norm(np.asarray(a) - np.asarray(b)) / max(np.linalg.norm(np.asarray(b)), 1e-300)
+
+
+# ---- building blocks ----------------------------------------------------------------
+
+
+def test_t0_matches_reference(golden):
+    z = golden("t0.npz")
+    ref = _medium(z)
+    for (om, a, dl, dm, dr), T in zip(z["cases"], z["T"]):
+        g = SlabGeometry(1, 1, float(a))
+        mat = SlabMaterial(np.full((1, 1, 1), dl), np.full((1, 1, 1), dm), np.full((1, 1, 1), dr), ref)
+        got = compute_slab_tmatrices(g, mat, float(om))[0, 0, 0]
+        assert_allclose(got, T, rtol=1e-13, atol=1e-300 + 1e-15 * np.abs(T).max())
+
+
+def test_incident_matches_reference(golden):
+    z = golden("incident.npz")
+    ref = _medium(z)
+    plan = SlabPlan(SlabGeometry(3, 2, float(z["a"])), ref)
+    for i, kh in enumerate(z["dirs"]):
+        for w in ("P", "S"):
+            got = plan.incident(float(z["omega"]), kh, w).cpu().numpy()
+            assert_allclose(got, z[f"psi0_{i}_{w}"], rtol=1e-13, atol=1e-15)
+    with pytest.raises(ValueError, match="wave_type"):
+        plan.incident(float(z["omega"]), KZ, "X")
+
+
+@pytest.mark.parametrize("M,Nz", [(3, 2), (2, 3)])
+@pytest.mark.parametrize("per", [0, 1])
+def test_matvec_matches_reference(golden, M, Nz, per):
+    z = golden("matvec_small.npz")
+    ref = _medium(z)
+    g = SlabGeometry(M, Nz, float(z["a"]))
+    mat = SlabMaterial(z[f"dlam_M{M}_Nz{Nz}"], z[f"dmu_M{M}_Nz{Nz}"], z[f"drho_M{M}_Nz{Nz}"], ref)
+    plan = SlabPlan(g, ref, periodic=bool(per))
+    plan.build_t0(mat, float(z["omega"]))
+    plan.build_g0(float(z["omega"]))
+    x = torch.from_numpy(z[f"x_M{M}_Nz{Nz}"].reshape(Nz, M, M, 9))
+    y = plan.matvec(x, "complex128").cpu().numpy().ravel()
+    assert_allclose(y, z[f"y_M{M}_Nz{Nz}_p{per}"], rtol=1e-10)
+    y32 = plan.matvec(x, "complex64").cpu().numpy().ravel()
+    assert _rel(y32, z[f"y_M{M}_Nz{Nz}_p{per}"]) < 2e-6
+
+
+@pytest.mark.parametrize("M,Nz,per,va", [
+    (8, 4, 0, 0), (8, 4, 1, 0), (5, 3, 1, 0), (7, 2, 1, 0), (11, 2, 1, 0), (6, 5, 0, 0), (4, 3, 0, 1), (4, 3, 1, 1),
+    (12, 1, 0, 0), (1, 3, 0, 0), (3, 1, 1, 1),
+])
+def test_matvec_random_sizes_vs_oracle(M, Nz, per, va):
+    """Odd/mixed-radix FFT lengths, one layer, one column, VA kernels."""
+    rng = np.random.default_rng(M * 100 + Nz)
+    g = SlabGeometry(M, Nz, 1.0)
+    mat = random_slab_material(g, REF, CONTRAST, 0.5, seed=M + Nz)
+    t4 = O.t0_scalars(OMEGA, 1.0, REF.alpha, REF.beta, REF.rho, mat.Dlambda, mat.Dmu, mat.Drho)
+    kh = O.build_slab_kernels(M, Nz, 1.0, OMEGA, REF.alpha, REF.beta, REF.rho, periodic=bool(per),
+                              volume_averaged=bool(va))
+    x = rng.standard_normal(Nz * M * M * 9) + 1j * rng.standard_normal(Nz * M * M * 9)
+    want = O.slab_matvec(x, t4, kh, M, Nz, periodic=bool(per))
+    plan = SlabPlan(g, REF, periodic=bool(per))
+    plan.build_t0(mat, OMEGA)
+    plan.build_g0(OMEGA, volume_averaged=bool(va))
+    got = plan.matvec(torch.from_numpy(x.reshape(Nz, M, M, 9))).cpu().numpy().ravel()
+    assert _rel(got, want) < 1e-12
+    assert_allclose(got, want, rtol=1e-10, atol=1e-12 * np.abs(want).max())
+
+
+def test_matvec_identity_when_T_zero():
+    g = SlabGeometry(5, 3, 1.0)
+    zero = MaterialContrast(0.0, 0.0, 0.0)
+    plan = SlabPlan(g, REF)
+    plan.build_t0(uniform_slab_material(g, REF, zero), OMEGA)
+    plan.build_g0(OMEGA)
+    x = torch.randn(3, 5, 5, 9, dtype=torch.complex128)
+    assert_allclose(plan.matvec(x).cpu().numpy(), x.numpy(), atol=1e-14)
+
+
+def test_bloch_fold_is_reference_fold_at_normal_incidence():
+    g = SlabGeometry(6, 2, 1.0)
+    mat = random_slab_material(g, REF, CONTRAST, 0.5, seed=2)
+    x = torch.randn(2, 6, 6, 9, dtype=torch.complex128)
+    ys = []
+    for kp in (None, (0.0, 0.0)):
+        plan = SlabPlan(g, REF, periodic=True)
+        plan.build_t0(mat, OMEGA)
+        plan.build_g0(OMEGA, kpar=kp)
+        ys.append(plan.matvec(x).cpu().numpy())
+    assert_allclose(ys[1], ys[0], rtol=1e-13, atol=1e-16)
+
+
+def test_bloch_matvec_vs_oracle():
+    M, Nz = 6, 2
+    g = SlabGeometry(M, Nz, 1.0)
+    mat = random_slab_material(g, REF, CONTRAST, 0.5, seed=4)
+    kpar = (0.013, -0.007)
+    t4 = O.t0_scalars(OMEGA, 1.0, REF.alpha, REF.beta, REF.rho, mat.Dlambda, mat.Dmu, mat.Drho)
+    kh = O.build_slab_kernels(M, Nz, 1.0, OMEGA, REF.alpha, REF.beta, REF.rho, periodic=True,
+                              phase_xy=(kpar[0] * 2.0, kpar[1] * 2.0))
+    rng = np.random.default_rng(0)
+    x = rng.standard_normal(Nz * M * M * 9) + 1j * rng.standard_normal(Nz * M * M * 9)
+    want = O.slab_matvec(x, t4, kh, M, Nz, periodic=True)
+    plan = SlabPlan(g, REF, periodic=True)
+    plan.build_t0(mat, OMEGA)
+    plan.build_g0(OMEGA, kpar=kpar)
+    got = plan.matvec(torch.from_numpy(x.reshape(Nz, M, M, 9))).cpu().numpy().ravel()
+    assert _rel(got, want) < 1e-12
+
+
+# ---- solves ---------------------------------------------------------------------------
+
+
+@pytest.mark.parametrize("precision", ["mixed", "fp64"])
+@pytest.mark.parametrize("name,M,Nz,opt", [
+    ("ap_P", 4, 2, {}), ("per_P", 4, 2, {"periodic": True}), ("va_P", 3, 2, {"volume_averaged": True}),
+    ("ap_S", 3, 3, {}),
+])
+def test_small_solves_match_reference(golden, precision, name, M, Nz, opt):
+    z = golden("solve_small.npz")
+    ref = _medium(z)
+    g = SlabGeometry(M, Nz, float(z["a"]))
+    mat = SlabMaterial(z[f"{name}_dlam"], z[f"{name}_dmu"], z[f"{name}_drho"], ref)
+    wt = "S" if name.endswith("S") else "P"
+    res = compute_slab_scattering_gpu(g, mat, float(z["omega"]), z[f"{name}_khat"], wt, gmres_tol=1e-12,
+                                      precision=precision, **opt)
+    assert res.gmres_residual < 1e-12
+    assert _rel(res.psi, z[f"{name}_psi"]) < 1e-10
+    T = compute_slab_tmatrices(g, mat, float(z["omega"]))
+    rpp = slab_rpp_periodic(res, T)
+    assert abs(rpp - complex(z[f"{name}_rpp"])) <= 1e-9 * abs(complex(z[f"{name}_rpp"]))
+    refl = np.array(slab_reflected_field(res, T))
+    # R_PS can be orders below R_PP; its error is bounded relative to the largest amplitude
+    want = z[f"{name}_refl"]
+    assert_allclose(refl, want, rtol=1e-9, atol=1e-9 * np.abs(want).max())
+
+
+@pytest.mark.parametrize("precision", ["mixed", "fp64"])
+def test_headline_16x16x4_matches_reference(golden, precision):
+    """16x16x4, ka 0.2, i.i.d. +-10 %, periodic, normal P, GMRES(30) to 1e-10:
+    R_PP within 1e-7 of the reference's FP64 solve."""
+    z = golden("slab_16x16x4.npz")
+    ref = _medium(z)
+    g = SlabGeometry(16, 4, float(z["a"]))
+    mat = SlabMaterial(z["dlam"], z["dmu"], z["drho"], ref)
+    res = compute_slab_scattering_gpu(g, mat, float(z["omega"]), KZ, "P", gmres_tol=1e-10, periodic=True,
+                                      precision=precision, restart=30)
+    assert res.gmres_residual < 1e-10
+    assert _rel(res.psi0, z["psi0"]) < 1e-14
+    assert _rel(res.psi, z["psi"]) < 1e-9
+    rpp = slab_rpp_periodic(res, res.t0)
+    assert abs(rpp - complex(z["rpp"])) <= 1e-7 * abs(complex(z["rpp"]))
+
+
+def test_dense_direct_solution(golden):
+    """GMRES on the FFT operator equals LU on the dense pairwise operator."""
+    z = golden("dense_m3_nz2.npz")
+    ref = _medium(z)
+    g = SlabGeometry(3, 2, float(z["a"]))
+    mat = SlabMaterial(z["dlam"], z["dmu"], z["drho"], ref)
+    res = compute_slab_scattering_gpu(g, mat, float(z["omega"]), KZ, "P", gmres_tol=1e-13)
+    assert _rel(res.psi, z["psi"]) < 1e-11
+
+
+def test_zero_contrast_gives_incident_field():
+    g = SlabGeometry(4, 2, 1.0)
+    mat = uniform_slab_material(g, REF, MaterialContrast(0.0, 0.0, 0.0))
+    for per in (False, True):
+        res = compute_slab_scattering_gpu(g, mat, OMEGA, KZ, periodic=per)
+        assert_allclose(res.psi, res.psi0, atol=1e-12)
+        assert abs(slab_rpp_periodic(res, res.t0)) < 1e-20
+
+
+def test_single_scatterer_centre_unchanged():
+    g = SlabGeometry(3, 1, 1.0)
+    z = np.zeros((1, 3, 3))
+    dl, dm, dr = z.copy(), z.copy(), z.copy()
+    dl[0, 1, 1], dm[0, 1, 1], dr[0, 1, 1] = CONTRAST.Dlambda, CONTRAST.Dmu, CONTRAST.Drho
+    res = compute_slab_scattering_gpu(g, SlabMaterial(dl, dm, dr, REF), OMEGA, KZ, gmres_tol=1e-10)
+    assert_allclose(res.psi[0, 1, 1], res.psi0[0, 1, 1], atol=1e-10)
+    assert np.any(np.abs(res.psi[0, 0, 0] - res.psi0[0, 0, 0]) > 1e-15)
+
+
+def test_born_scaling():
+    g = SlabGeometry(4, 2, 1.0)
+    w = MaterialContrast(2e5, 1e5, 0.01)
+    w2 = MaterialContrast(4e5, 2e5, 0.02)
+    r1 = compute_slab_scattering_gpu(g, uniform_slab_material(g, REF, w), OMEGA, KZ, gmres_tol=1e-12)
+    r2 = compute_slab_scattering_gpu(g, uniform_slab_material(g, REF, w2), OMEGA, KZ, gmres_tol=1e-12)
+    s1, s2 = r1.psi - r1.psi0, r2.psi - r2.psi0
+    m = np.abs(s1) > 1e-15
+    assert_allclose(np.abs(s2[m] / s1[m]), 2.0, rtol=0.02)
+
+
+def test_oblique_random_solve_vs_oracle():
+    """Aperiodic oblique SV at ka 0.5 with +-20 % i.i.d. contrast: both precisions."""
+    ref = ReferenceMedium(3000.0, 1732.0, 2500.0)
+    g = SlabGeometry(10, 3, 1.0)
+    om = 0.5 * ref.beta
+    mat = uniform_random_material(g, ref, 0.2, seed=3)
+    kh = np.array([np.cos(0.4), np.sin(0.4), 0.0])
+    ora = O.solve(10, 3, 1.0, ref.alpha, ref.beta, ref.rho, mat.Dlambda, mat.Dmu, mat.Drho, om, kh, "S", 1e-13,
+                  restart=30)
+    for prec in ("mixed", "fp64"):
+        res = compute_slab_scattering_gpu(g, mat, om, kh, "S", gmres_tol=1e-11, precision=prec, restart=30)
+        assert res.gmres_residual < 1e-11
+        assert _rel(res.psi, ora["psi"]) < 1e-9
+
+
+def test_nonconvergence_warns_and_reports():
+    g = SlabGeometry(6, 3, 1.0)
+    mat = random_slab_material(g, REF, CONTRAST, 0.5, seed=1)
+    with pytest.warns(UserWarning, match="did not converge"):
+        res = compute_slab_scattering_gpu(g, mat, OMEGA, KZ, gmres_tol=1e-14, max_iter=3)
+    assert res.stats["n_matvec"] - res.stats["n_matvec64"] <= 3
+    assert res.gmres_residual > 1e-14
+
+
+def test_input_validation():
+    g = SlabGeometry(2, 1, 1.0)
+    mat = uniform_slab_material(g, REF, CONTRAST)
+    with pytest.raises(ValueError, match="wave_type"):
+        compute_slab_scattering_gpu(g, mat, OMEGA, KZ, "X")
+    with pytest.raises(ValueError, match="bloch"):
+        compute_slab_scattering_gpu(g, mat, OMEGA, KZ, bloch=True)
+    with pytest.raises(ValueError, match="omega"):
+        compute_slab_scattering_gpu(g, mat, -1.0, KZ)
+    with pytest.raises(ValueError):
+        compute_slab_scattering_gpu(g, mat, OMEGA, KZ, device="cpu")
