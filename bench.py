@@ -1,0 +1,372 @@
+"""Benchmark of the slab Foldy-Lax solve on B200 (one JSON line on rank 0).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload cfg2|cfg1|cfg5]
+
+Workload (default ``cfg2``): one 64 x 64 x 16 slab (589,824 unknowns), ka = 0.5
+(omega = 0.5 beta / a, a = 1 m half-width), P plane wave at 20 deg, contrasts from a
+seeded Gaussian random field (correlation length 3 cells, std 15 %), aperiodic
+(padded 32 x 128 x 128), solved to an FP64 true relative residual of 1e-10 by
+complex64 GMRES(30) inside FP64 iterative refinement. A step is one complete
+slab solve with the material already in HBM: T0 build, G0 spectrum build,
+incident field, GMRES solve and R_PP. ``value`` is solves/s over all ranks; with
+N ranks each rank solves its own slab (different seed): weak scaling, no
+collective on the data path.
+
+Extra keys: ``roofline`` (the complex64 matvec, timed live with CUDA events),
+``cpu_baseline`` (the oracle port of the reference's numpy/scipy solver on the
+host, one solve of the same workload), ``e2e`` (the public
+``compute_slab_scattering_gpu`` call from pinned host arrays to numpy result),
+``fp64`` (the plain complex128 GMRES solve on the same slab), ``clocks``.
+
+``--impl reference`` times the reference's CPU algorithm (the oracle port, with
+all host threads) on the same workload; under torchrun only rank 0 runs it.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "time to 1e-8 residual per slab solve, learned-PC+mixed vs plain GMRES; matvec GB/s"
+
+WORKLOADS = {
+    # name: M, N_z, ka, angle_deg, wave, material, tol, periodic
+    "cfg2": dict(M=64, N_z=16, ka=0.5, angle=20.0, wave="P", mat=("grf", 3.0, 0.15), tol=1e-10, periodic=False),
+    "cfg1": dict(M=16, N_z=4, ka=0.2, angle=0.0, wave="P", mat=("iid", 0.10), tol=1e-10, periodic=True),
+    "cfg5": dict(M=256, N_z=32, ka=1.0, angle=30.0, wave="S", mat=("grf", 3.0, 0.40), tol=1e-8, periodic=True),
+}
+ALPHA, BETA, RHO, A = 3000.0, 1732.0, 2500.0, 1.0
+
+
+def _peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def make_problem(wl: dict, seed: int):
+    from multiplescatteringcalculations_b200 import (
+        ReferenceMedium,
+        SlabGeometry,
+        gaussian_random_field_material,
+        uniform_random_material,
+    )
+
+    ref = ReferenceMedium(ALPHA, BETA, RHO)
+    geom = SlabGeometry(wl["M"], wl["N_z"], A)
+    if wl["mat"][0] == "grf":
+        mat = gaussian_random_field_material(geom, ref, correlation_length=wl["mat"][1], std=wl["mat"][2], seed=seed)
+    else:
+        mat = uniform_random_material(geom, ref, wl["mat"][1], seed=seed)
+    th = np.deg2rad(wl["angle"])
+    k_hat = np.array([np.cos(th), np.sin(th), 0.0])
+    omega = wl["ka"] * BETA / A
+    return ref, geom, mat, k_hat, omega
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.path or not os.path.exists(self.path):
+            return None
+        rows = [r.split(",") for r in open(self.path).read().strip().splitlines() if r.strip()]
+        os.unlink(self.path)
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].strip().replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].strip().replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if len(r) > 5 + i and "Active" == r[5 + i].strip()})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def cpu_baseline(wl: dict, threads: int, seed: int = 0):
+    """One solve of the workload by the oracle port of the reference's CPU path."""
+    from oracle import slab_oracle as O
+
+    ref, geom, mat, k_hat, omega = make_problem(wl, seed)
+    tm = {}
+    t0 = time.perf_counter()
+    r = O.solve(geom.M, geom.N_z, geom.a, ref.alpha, ref.beta, ref.rho, mat.Dlambda, mat.Dmu, mat.Drho, omega,
+                k_hat, wl["wave"], wl["tol"], 500, periodic=wl["periodic"], restart=30, threads=threads, timings=tm)
+    dt = time.perf_counter() - t0
+    return dt, r, tm
+
+
+def run_reference(args, wl, rank, world):
+    if rank != 0:
+        return 0
+    threads = os.cpu_count() or 1
+    times = []
+    last = None
+    for i in range(args.warmup + args.steps):
+        dt, r, tm = cpu_baseline(wl, threads, seed=0)
+        if i >= args.warmup:
+            times.append(dt)
+            last = (r, tm)
+    ms = float(np.mean(times)) * 1e3
+    value = 1e3 / ms
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "c128", "data": "synthetic",
+        "config": {"workload": args.workload, **_cfg_desc(wl)},
+        "cpu_baseline": {"value": value, "unit": "solves/s", "cores": threads, "kind": "port",
+                         "sample": f"one full {args.workload} solve per step (T0 + kernel build + scipy GMRES(30) "
+                                   f"to {wl['tol']:g}); split s: t0 {last[1]['t0']:.2f}, kernel "
+                                   f"{last[1]['kernel']:.2f}, solve {last[1]['solve']:.2f}; {last[0]['n_matvec']} "
+                                   "matvecs"},
+        "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def _cfg_desc(wl):
+    return {"lattice": f"{wl['M']}x{wl['M']}x{wl['N_z']}", "ka": wl["ka"], "incidence_deg": wl["angle"],
+            "wave": wl["wave"], "material": list(wl["mat"]), "tol": wl["tol"], "periodic": wl["periodic"],
+            "restart": 30, "l2": "inputs larger than L2 (G0 spectrum build and matvec stream > 126 MB per step)"}
+
+
+def run_ours(args, wl, rank, world, local_rank):
+    import torch
+    import torch.distributed as dist
+
+    from multiplescatteringcalculations_b200 import SlabPlan, compute_slab_scattering_gpu, _native
+
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    lib = _native.load()
+    ref, geom, mat, k_hat, omega = make_problem(wl, seed=1000 + rank)
+    plan = SlabPlan(geom, ref, periodic=wl["periodic"], device=dev)
+    mat_dev = type(mat)(torch.from_numpy(mat.Dlambda).to(dev), torch.from_numpy(mat.Dmu).to(dev),
+                        torch.from_numpy(mat.Drho).to(dev), ref)
+    stream = torch.cuda.current_stream(dev)
+    stats = {}
+
+    def step():
+        plan.build_t0(mat_dev, omega)
+        plan.build_g0(omega)
+        psi0 = plan.incident(omega, k_hat, wl["wave"])
+        x, st = plan.solve(psi0, tol=wl["tol"], max_iter=1000, restart=30, precision="mixed")
+        stats.update(st)
+        stats["rpp"] = plan.rpp_periodic(x, omega)
+        return x
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    n0 = lib.msc_launch_count()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local_rank) as clk:
+        ev0.record(stream)
+        for _ in range(args.steps):
+            step()
+        ev1.record(stream)
+        torch.cuda.synchronize()
+    launches = lib.msc_launch_count() - n0
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    ms = ev0.elapsed_time(ev1)
+    t = torch.tensor([ms], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_max = float(t.item())
+    value = world * args.steps / (ms_max / 1e3)
+    if stats.get("residual", 1.0) > wl["tol"]:
+        raise RuntimeError(f"solve did not reach tol: {stats}")
+
+    if args.solve_only:
+        if rank == 0:
+            print(json.dumps({"metric": METRIC, "value": value, "unit": "solves/s", "ms_per_step": ms_max / args.steps,
+                              "solve": {k: (v if not isinstance(v, complex) else [v.real, v.imag])
+                                        for k, v in stats.items()}, "gpu_launches": int(launches)}), flush=True)
+        plan.close()
+        return 0
+
+    # ---- the plain FP64 GMRES solve of the same slab (the comparator) ----
+    def step64():
+        plan.build_t0(mat_dev, omega)
+        plan.build_g0(omega)
+        psi0 = plan.incident(omega, k_hat, wl["wave"])
+        return plan.solve(psi0, tol=wl["tol"], max_iter=1000, restart=30, precision="fp64")[1]
+
+    step64()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    nrep64 = max(1, min(args.steps, 3))
+    for _ in range(nrep64):
+        st64 = step64()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms64 = e0.elapsed_time(e1) / nrep64
+
+    # ---- roofline of the complex64 matvec, timed live ----
+    x32 = torch.randn(geom.N_z, geom.M, geom.M, 9, dtype=torch.complex64, device=dev)
+    Lz, Lx, Ly = plan.fft_sizes()
+    import ctypes as C
+
+    ns = geom.N_z * geom.M * geom.M
+    hy = Ly // 2 + 1
+    E = 45
+    b_alg = E * hy * Lx * Lz * 8 + 4 * ns * 8 + 2 * 9 * ns * 8
+    b_alg_ref = 81 * Lz * Lx * Ly * 8 + 4 * ns * 8 + 2 * 9 * ns * 8
+    # the SoA matvec (no layout conversion): measured through the internal launcher
+    y32 = torch.empty_like(x32)
+    nrep = 50
+    for _ in range(5):
+        lib.msc_matvec(plan.handle, C.c_void_p(x32.data_ptr()), C.c_void_p(y32.data_ptr()), 0)
+    torch.cuda.synchronize()
+    m0, m1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    m0.record(stream)
+    for _ in range(nrep):
+        lib.msc_matvec(plan.handle, C.c_void_p(x32.data_ptr()), C.c_void_p(y32.data_ptr()), 0)
+    m1.record(stream)
+    torch.cuda.synchronize()
+    t_mv = m0.elapsed_time(m1) / nrep / 1e3
+    # the layout conversions of msc_matvec (2 transposes of the field) are part of this time
+    peak, peak_kind = _peaks()
+    achieved = b_alg / t_mv / 1e9
+    traffic = None
+    tf = ROOT / "profiles" / f"matvec_{args.workload}_traffic.txt"
+    if tf.exists():
+        for ln in tf.read_text().splitlines():
+            if ln.startswith("dram_bytes_per_matvec:"):
+                traffic = float(ln.split(":")[1])
+
+    line = {
+        "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "c64+c128", "data": "synthetic",
+        "config": {"workload": args.workload, **_cfg_desc(wl), "fft": [Lz, Lx, Ly]},
+        "gpu_launches": int(launches),
+        "solve": {"n_matvec": stats["n_matvec"], "n_matvec64": stats["n_matvec64"], "n_outer": stats["n_outer"],
+                  "residual": stats["residual"], "rpp": [stats["rpp"].real, stats["rpp"].imag]},
+        "fp64": {"ms_per_solve": ms64, "n_matvec": st64["n_matvec"], "residual": st64["residual"],
+                 "speedup_mixed_vs_fp64": ms64 / (ms_max / args.steps)},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": traffic, "kernel": "complex64 matvec (5 launches + 2 layout transposes)",
+                     "us_per_matvec": t_mv * 1e6, "alg_bytes": b_alg,
+                     "peak_kind": peak_kind,
+                     "effective_gbs_reference_layout": b_alg_ref / t_mv / 1e9},
+    }
+    if rank == 0 and not args.no_e2e:
+        # public API from pinned host arrays; the plan cache keeps allocations out of the loop
+        import torch as _t
+
+        from multiplescatteringcalculations_b200 import SlabMaterial
+
+        pin = [_t.from_numpy(a).pin_memory() for a in (mat.Dlambda, mat.Dmu, mat.Drho)]
+        hmat = SlabMaterial(pin[0], pin[1], pin[2], ref)
+        for _ in range(max(1, args.warmup)):
+            compute_slab_scattering_gpu(geom, hmat, omega, k_hat, wl["wave"], gmres_tol=wl["tol"], max_iter=1000,
+                                        device=dev, periodic=wl["periodic"])
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            r = compute_slab_scattering_gpu(geom, hmat, omega, k_hat, wl["wave"], gmres_tol=wl["tol"], max_iter=1000,
+                                            device=dev, periodic=wl["periodic"])
+        dt = time.perf_counter() - t0
+        line["e2e"] = {"value": args.steps / dt, "unit": "solves/s", "h2d_bytes_per_step": 3 * ns * 8,
+                       "d2h_bytes_per_step": 2 * 9 * ns * 16 + 4 * ns * 16,
+                       "ms_per_solve": dt / args.steps * 1e3, "residual": r.gmres_residual}
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        threads = os.cpu_count() or 1
+        dt, rr, tm = cpu_baseline(wl, threads, seed=1000)
+        line["cpu_baseline"] = {"value": 1.0 / dt, "unit": "solves/s", "cores": threads, "kind": "port",
+                                "sample": f"one {args.workload} solve by the oracle port (numpy/scipy FP64, scipy "
+                                          f"GMRES(30) to {wl['tol']:g}; t0 {tm['t0']:.2f} s, kernel "
+                                          f"{tm['kernel']:.2f} s, solve {tm['solve']:.2f} s, "
+                                          f"{rr['n_matvec']} matvecs)"}
+    line["clocks"] = clk.summary()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    plan.close()
+    return 0
+
+
+def main(argv=None) -> int:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="cfg2", choices=sorted(WORKLOADS))
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--solve-only", action="store_true", help="timed solves only (for profiler launch lists)")
+    args = ap.parse_args(argv)
+    wl = WORKLOADS[args.workload]
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        return run_reference(args, wl, rank, world)
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    try:
+        return run_ours(args, wl, rank, world, local_rank)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -59,6 +59,7 @@ typedef struct msc_solve_opts {
   int32_t precision;      /* msc_solver_precision */
   int32_t initial_guess;  /* 0 = Born (x0 = psi0), 1 = zero */
   double inner_tol;       /* mixed precision: relative tolerance of each complex64 inner solve (0 = default) */
+  int32_t ortho;          /* Arnoldi: 0 = default (mixed: CGS1, fp64: CGS2), 1 = CGS1, 2 = CGS2 */
 } msc_solve_opts;
 
 typedef struct msc_solve_stats {
@@ -130,6 +131,8 @@ int msc_reflected_field(msc_plan* plan, const void* psi, double omega, const dou
 const char* msc_status_string(int status);
 /* Message of the last error on this thread. */
 const char* msc_last_error(void);
+/* Kernel launches issued by this library since it was loaded (all plans, all threads). */
+int64_t msc_launch_count(void);
 /* Library version string. */
 const char* msc_version(void);
 

@@ -13,6 +13,7 @@ from .slab import (  # noqa: F401
     SlabMaterial,
     SlabPlan,
     SlabResult,
+    clear_plan_cache,
     compute_slab_scattering_gpu,
     compute_slab_tmatrices,
     gaussian_random_field_material,

@@ -52,6 +52,7 @@ class SolveOpts(C.Structure):
         ("precision", C.c_int32),
         ("initial_guess", C.c_int32),
         ("inner_tol", C.c_double),
+        ("ortho", C.c_int32),
     ]
 
 
@@ -84,6 +85,7 @@ SIGNATURES = {
     "msc_status_string": (C.c_char_p, [C.c_int]),
     "msc_last_error": (C.c_char_p, []),
     "msc_version": (C.c_char_p, []),
+    "msc_launch_count": (C.c_int64, []),
 }
 
 _lib = None

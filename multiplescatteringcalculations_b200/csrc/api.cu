@@ -1,4 +1,5 @@
 // C-ABI entry points of libmsc_b200.so (declared in include/msc.h).
+#include <atomic>
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
@@ -8,6 +9,9 @@
 namespace msc {
 
 static thread_local char g_err[512] = "";
+static std::atomic<long long> g_launches{0};
+
+void note_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
 
 void set_error(const char* fmt, ...) {
   va_list ap;
@@ -61,7 +65,7 @@ __global__ void k_narrow(const double2* __restrict__ a, float2* __restrict__ b, 
 }
 
 int launch_narrow(msc_plan* pl, const double2* a, float2* b, size_t n) {
-  k_narrow<<<ceil_div((long long)n, 256), 256, 0, pl->stream>>>(a, b, n);
+  k_narrow<<<ceil_div((long long)n, 256), 256, 0, pl->stream>>>(a, b, n); ::msc::note_launch();
   MSC_CUDA(cudaGetLastError());
   return MSC_OK;
 }
@@ -69,7 +73,7 @@ int launch_narrow(msc_plan* pl, const double2* a, float2* b, size_t n) {
 int bloch_modulate(msc_plan* pl, double2* v, int sign) {
   const Geo& g = pl->g;
   k_bloch<<<ceil_div(9LL * g.nsite, 256), 256, 0, pl->stream>>>(v, g.M, g.nsite, pl->desc.a, pl->kpar[0], pl->kpar[1],
-                                                                sign);
+                                                                sign); ::msc::note_launch();
   MSC_CUDA(cudaGetLastError());
   return MSC_OK;
 }
@@ -106,6 +110,7 @@ const char* msc_status_string(int s) {
 }
 
 const char* msc_last_error(void) { return g_err; }
+int64_t msc_launch_count(void) { return g_launches.load(); }
 const char* msc_version(void) { return "msc_b200 0.1.0 (sm_100a)"; }
 
 int msc_plan_create(const msc_slab_desc* d, void* stream, msc_plan** out) {
@@ -170,6 +175,8 @@ int msc_plan_create(const msc_slab_desc* d, void* stream, msc_plan** out) {
     return MSC_ERR_UNSUPPORTED;
   }
   int s = build_twiddles(pl);
+  if (s == MSC_OK) s = dalloc(pl, pl->status, 64);
+  if (s == MSC_OK && cudaMemsetAsync(pl->status.p, 0, 64, pl->stream) != cudaSuccess) s = MSC_ERR_CUDA;
   if (s == MSC_OK) s = dalloc(pl, pl->W64, sizeof(double2) * ws_elems(g));
   if (s == MSC_OK) s = dalloc(pl, pl->W32, sizeof(float2) * ws_elems(g));
   if (s != MSC_OK) {
@@ -186,8 +193,8 @@ int msc_plan_destroy(msc_plan* pl) {
   else cudaDeviceSynchronize();
   gmres_free(pl);
   DBuf* bufs[] = {&pl->tw64_z, &pl->tw64_xy, &pl->tw32_z, &pl->tw32_xy, &pl->t4_64, &pl->t4_32, &pl->khat64,
-                  &pl->khat32, &pl->va_blocks, &pl->W64, &pl->W32, &pl->f64a, &pl->f64b, &pl->f32a, &pl->f32b,
-                  &pl->red};
+                  &pl->khat32, &pl->va_blocks, &pl->g0_scratch, &pl->W64, &pl->W32, &pl->f64a, &pl->f64b, &pl->f32a, &pl->f32b,
+                  &pl->red, &pl->status};
   for (DBuf* b : bufs) dfree(pl, *b);
   delete pl;
   return MSC_OK;

@@ -10,8 +10,8 @@
 // transforms into (Ns*R)-point ones (self-sorting Stockham, decimation in time):
 //   j in [0, L/R): k = j mod Ns, v_r = x[j + r L/R] * w_{Ns R}^{r k},
 //   v <- DFT_R(v), out[(j / Ns) Ns R + k + r Ns] = v_r.
-// Each stage runs in place: every thread loads its butterfly inputs into
-// registers, the block synchronises, then all threads store.
+// Stages alternate between two tiles (ping-pong), so a thread streams one
+// butterfly at a time through registers and a stage costs one barrier.
 #pragma once
 #include "msc_common.cuh"
 #include "radix_constants.cuh"
@@ -23,7 +23,7 @@ constexpr int FFT_MAX_STAGES = 12;
 struct FftPlan1D {
   int L;
   int nstages;
-  int min_radix;
+  int pow2;  // 1 if L is a power of two (radices 2, 4, 8 only)
   int radix[FFT_MAX_STAGES];
   int ns[FFT_MAX_STAGES];
 };
@@ -34,15 +34,11 @@ inline bool make_fft_plan(int L, FftPlan1D* p) {
   int rad[FFT_MAX_STAGES];
   int n = 0, rest = L, e2 = 0;
   while (rest % 2 == 0) { rest /= 2; ++e2; }
-  // powers of two: prefer radix 8, then 4 (no radix-2 stage unless L = 2^1)
-  if (e2 == 1) rad[n++] = 2;
-  else if (e2 > 0) {
-    int r3 = e2 % 3;
-    int n8 = e2 / 3;
-    if (r3 == 1) { n8 -= 1; rad[n++] = 4; rad[n++] = 4; }
-    else if (r3 == 2) rad[n++] = 4;
-    for (int i = 0; i < n8; ++i) rad[n++] = 8;
-  }
+  // powers of two: radix 8 stages, completed by one radix 4 or 2 stage
+  int n8 = e2 / 3, r3 = e2 % 3;
+  for (int i = 0; i < n8; ++i) rad[n++] = 8;
+  if (r3 == 2) rad[n++] = 4;
+  if (r3 == 1) rad[n++] = 2;
   const int odd[] = {3, 5, 7, 11};
   for (int r : odd) {
     while (rest % r == 0) {
@@ -52,19 +48,15 @@ inline bool make_fft_plan(int L, FftPlan1D* p) {
     }
   }
   if (rest != 1) return false;
-  // order: largest radix first (fewest butterflies in the early stages does not
-  // matter for Stockham; any order is exact)
   p->L = L;
   p->nstages = n;
-  int ns = 1, mr = 64;
+  p->pow2 = (rest == 1 && (L & (L - 1)) == 0) ? 1 : 0;
+  int ns = 1;
   for (int s = 0; s < n; ++s) {
     p->radix[s] = rad[s];
     p->ns[s] = ns;
     ns *= rad[s];
-    if (rad[s] < mr) mr = rad[s];
   }
-  p->min_radix = (n == 0) ? 1 : mr;
-  if (L == 1) { p->nstages = 0; p->min_radix = 1; }
   return true;
 }
 
@@ -129,11 +121,11 @@ template <int R, int DIR, typename C> struct Dft {
     C y0 = v[0];
 #pragma unroll
     for (int q = 0; q < H; ++q) y0 += s[q];
-    C out[R];
-    out[0] = y0;
+    const C v0 = v[0];
+    v[0] = y0;
 #pragma unroll
     for (int k = 1; k <= H; ++k) {
-      C A = v[0], B;
+      C A = v0, B;
       B.x = 0;
       B.y = 0;
 #pragma unroll
@@ -146,87 +138,73 @@ template <int R, int DIR, typename C> struct Dft {
         B.y += sn * d[q - 1].y;
       }
       C iB = mul_i<DIR>(B);  // DIR * i * B
-      out[k] = A + iB;
-      out[R - k] = A - iB;
+      v[k] = A + iB;
+      v[R - k] = A - iB;
     }
-#pragma unroll
-    for (int k = 0; k < R; ++k) v[k] = out[k];
   }
 };
 
-// One Stockham stage over the tile. Thread `tid` owns line l = tid % nlines and
-// butterflies j = tid / nlines + k * jstride, k < KMAX.
-template <int R, int DIR, int KMAX, typename C>
-__device__ __forceinline__ void fft_stage(C* buf, int pitch, int L, int Ns, const C* tw, int l, int j0, int jstride,
-                                          bool active) {
+// One Stockham stage src -> dst. Thread owns line l and butterflies j0, j0 + jstride, ...
+template <int R, int DIR, bool POW2, typename C>
+__device__ __forceinline__ void fft_stage(const C* __restrict__ src, C* __restrict__ dst, int pitch, int L, int Ns,
+                                          const C* __restrict__ tw, int l, int j0, int jstride) {
   const int nb = L / R;
-  C v[KMAX][R];
-  if (active) {
+  const int tstep = L / (Ns * R);
+  for (int j = j0; j < nb; j += jstride) {
+    C v[R];
 #pragma unroll
-    for (int k = 0; k < KMAX; ++k) {
-      const int j = j0 + k * jstride;
-      if (j < nb) {
+    for (int r = 0; r < R; ++r) v[r] = src[(j + r * nb) * pitch + l];
+    const int kk = POW2 ? (j & (Ns - 1)) : (j % Ns);
+    if (Ns > 1) {
 #pragma unroll
-        for (int r = 0; r < R; ++r) v[k][r] = buf[(j + r * nb) * pitch + l];
+      for (int r = 1; r < R; ++r) {
+        C w = tw[r * kk * tstep];
+        if (DIR > 0) w.y = -w.y;
+        v[r] = v[r] * w;
       }
     }
+    Dft<R, DIR, C>::run(v);
+    const int idxD = (j - kk) * R + kk;
+#pragma unroll
+    for (int r = 0; r < R; ++r) dst[(idxD + r * Ns) * pitch + l] = v[r];
   }
-  __syncthreads();
-  if (active) {
-    const int tstep = L / (Ns * R);
-#pragma unroll
-    for (int k = 0; k < KMAX; ++k) {
-      const int j = j0 + k * jstride;
-      if (j < nb) {
-        const int kk = j % Ns;
-        if (Ns > 1) {
-#pragma unroll
-          for (int r = 1; r < R; ++r) {
-            C w = tw[r * kk * tstep];
-            if (DIR > 0) w.y = -w.y;
-            v[k][r] = v[k][r] * w;
-          }
-        }
-        Dft<R, DIR, C>::run(v[k]);
-        const int idxD = (j - kk) * R + kk;
-#pragma unroll
-        for (int r = 0; r < R; ++r) buf[(idxD + r * Ns) * pitch + l] = v[k][r];
-      }
-    }
-  }
-  __syncthreads();
 }
 
-// Full transform of every line in the tile. Requirements (checked by the host):
-// nlines <= nthr and ceil((L / min_radix) / (nthr / nlines)) <= KMAX.
-template <int DIR, int KMAX, typename C>
-__device__ void fft_tile(C* buf, int pitch, int nlines, const FftPlan1D& pl, const C* tw, int tid, int nthr) {
+// Full transform of every line of the tile in `a`, using `b` as the second tile.
+// Returns the tile holding the result (a or b). Needs nthr >= nlines; threads
+// tid >= (nthr / nlines) * nlines idle during the stages. Ends with a barrier.
+template <int DIR, bool POW2, typename C>
+__device__ C* fft_tile(C* a, C* b, int pitch, int nlines, const FftPlan1D& pl, const C* tw, int tid, int nthr) {
   const int jstride = nthr / nlines;
   const bool active = tid < jstride * nlines;
   const int l = tid % nlines;
-  const int j0 = tid / nlines;
+  const int j0 = active ? tid / nlines : (1 << 30);
+  C* src = a;
+  C* dst = b;
   for (int s = 0; s < pl.nstages; ++s) {
     const int Ns = pl.ns[s];
     switch (pl.radix[s]) {
-      case 8: fft_stage<8, DIR, KMAX>(buf, pitch, pl.L, Ns, tw, l, j0, jstride, active); break;
-      case 4: fft_stage<4, DIR, KMAX>(buf, pitch, pl.L, Ns, tw, l, j0, jstride, active); break;
-      case 2: fft_stage<2, DIR, KMAX>(buf, pitch, pl.L, Ns, tw, l, j0, jstride, active); break;
-      case 3: fft_stage<3, DIR, KMAX>(buf, pitch, pl.L, Ns, tw, l, j0, jstride, active); break;
-      case 5: fft_stage<5, DIR, KMAX>(buf, pitch, pl.L, Ns, tw, l, j0, jstride, active); break;
-      case 7: fft_stage<7, DIR, KMAX>(buf, pitch, pl.L, Ns, tw, l, j0, jstride, active); break;
-      case 11: fft_stage<11, DIR, KMAX>(buf, pitch, pl.L, Ns, tw, l, j0, jstride, active); break;
-      default: break;
+      case 8: fft_stage<8, DIR, POW2>(src, dst, pitch, pl.L, Ns, tw, l, j0, jstride); break;
+      case 4: fft_stage<4, DIR, POW2>(src, dst, pitch, pl.L, Ns, tw, l, j0, jstride); break;
+      case 2: fft_stage<2, DIR, POW2>(src, dst, pitch, pl.L, Ns, tw, l, j0, jstride); break;
+      default:
+        if (!POW2) {
+          switch (pl.radix[s]) {
+            case 3: fft_stage<3, DIR, false>(src, dst, pitch, pl.L, Ns, tw, l, j0, jstride); break;
+            case 5: fft_stage<5, DIR, false>(src, dst, pitch, pl.L, Ns, tw, l, j0, jstride); break;
+            case 7: fft_stage<7, DIR, false>(src, dst, pitch, pl.L, Ns, tw, l, j0, jstride); break;
+            case 11: fft_stage<11, DIR, false>(src, dst, pitch, pl.L, Ns, tw, l, j0, jstride); break;
+            default: break;
+          }
+        }
+        break;
     }
+    __syncthreads();
+    C* t = src;
+    src = dst;
+    dst = t;
   }
-}
-
-// Host helper: the KMAX a tile transform needs for the given thread count.
-inline int fft_kmax_needed(const FftPlan1D& pl, int nlines, int nthr) {
-  if (pl.nstages == 0) return 1;
-  const int jstride = nthr / nlines;
-  if (jstride < 1) return 1 << 30;
-  const int nb = pl.L / pl.min_radix;
-  return (nb + jstride - 1) / jstride;
+  return src;
 }
 
 }  // namespace msc

@@ -22,8 +22,8 @@
 namespace msc {
 
 template <typename T>
-int launch_fft_contig(msc_plan* pl, const cx<T>* in, cx<T>* out, long long nlines, long long in_stride,
-                      long long out_stride, int n_in, int n_out, const FftPlan1D& f, const cx<T>* tw, int dir,
+int launch_fft_contig(msc_plan* pl, const cx<T>* in, cx<T>* out, long long nlines, long long G, long long GS,
+                      long long stride, int n_in, int n_out, const FftPlan1D& f, const cx<T>* tw, int dir,
                       const int* done);
 
 struct GState {
@@ -127,68 +127,136 @@ __device__ void reduce_to(double2* sums, int nv, double2* __restrict__ part, int
   if (threadIdx.x == 0) *counter = 0;
 }
 
-// out[i] = sum_k conj(s_i V_i[k]) w[k], i < nv
-template <typename T, int NV>
+// Chunked multi-vector kernels. A block of NTH threads covers chunks of NTH*EPT
+// consecutive elements (thread t holds elements t, t + NTH, ..., so each warp
+// access is coalesced); blocks stride over the chunks.
+constexpr int EPT = 8;
+
+// Thread i < nv of every block holds the block's total of row i; the last block
+// to finish sums the rows over blocks in a fixed order into out[i].
+__device__ void reduce_rows(double2 mine, int nv, double2* __restrict__ part, int* counter, double2* out) {
+  __shared__ bool last;
+  if (threadIdx.x < nv) part[(size_t)blockIdx.x * PLD + threadIdx.x] = mine;
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) last = (atomicAdd(counter, 1) == (int)gridDim.x - 1);
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  for (int i = w; i < nv; i += NTH / 32) {
+    double2 v = make_double2(0, 0);
+    for (int b = l; b < (int)gridDim.x; b += 32) v += ((volatile double2*)part)[(size_t)b * PLD + i];
+    for (int o = 16; o > 0; o >>= 1) {
+      v.x += __shfl_xor_sync(0xffffffffu, v.x, o);
+      v.y += __shfl_xor_sync(0xffffffffu, v.y, o);
+    }
+    if (l == 0) out[i] = v;
+  }
+  if (threadIdx.x == 0) *counter = 0;
+}
+
+// out[i] = sum_k conj(s_i V_i[k]) w[k], i < nv. Per chunk and vector the
+// products of a warp are summed (FP32 within a thread's 8 elements, warp
+// shuffles), and lane 0 accumulates into the block's FP64 shared totals.
+template <typename T>
 __global__ void __launch_bounds__(NTH) k_mdot(const cx<T>* __restrict__ V, size_t n, int nv, const double* scale,
                                               const cx<T>* __restrict__ w, double2* part, int* counter, double2* out,
                                               const int* done) {
   if (done && *done) return;
-  double2 acc[NV];
+  __shared__ double2 sh[NTH / 32][33];
+  const int lane = threadIdx.x & 31, wp = threadIdx.x >> 5;
+  for (int i = lane; i < nv; i += 32) sh[wp][i] = make_double2(0, 0);
+  __syncwarp();
+  const size_t chunk = (size_t)NTH * EPT;
+  for (size_t base = (size_t)blockIdx.x * chunk; base < n; base += (size_t)gridDim.x * chunk) {
+    cx<T> wr[EPT];
 #pragma unroll
-  for (int i = 0; i < NV; ++i) acc[i] = make_double2(0, 0);
-  for (size_t k = (size_t)blockIdx.x * NTH + threadIdx.x; k < n; k += (size_t)gridDim.x * NTH) {
-    const double2 wk = to_d(w[k]);
-#pragma unroll
-    for (int i = 0; i < NV; ++i)
-      if (i < nv) {
-        const double2 v = to_d(V[(size_t)i * n + k]);
-        acc[i].x += v.x * wk.x + v.y * wk.y;
-        acc[i].y += v.x * wk.y - v.y * wk.x;
-      }
-  }
-#pragma unroll
-  for (int i = 0; i < NV; ++i)
-    if (i < nv) {
-      const double s = scale ? scale[i] : 1.0;
-      acc[i].x *= s;
-      acc[i].y *= s;
+    for (int u = 0; u < EPT; ++u) {
+      const size_t k = base + (size_t)u * NTH + threadIdx.x;
+      wr[u] = k < n ? w[k] : czero<cx<T>>();
     }
-  reduce_to<NV>(acc, nv, part, counter, out);
+    for (int i = 0; i < nv; ++i) {
+      const cx<T>* Vi = V + (size_t)i * n;
+      cx<T> a = czero<cx<T>>();
+#pragma unroll
+      for (int u = 0; u < EPT; ++u) {
+        const size_t k = base + (size_t)u * NTH + threadIdx.x;
+        if (k < n) {
+          const cx<T> v = Vi[k];
+          a.x += v.x * wr[u].x + v.y * wr[u].y;
+          a.y += v.x * wr[u].y - v.y * wr[u].x;
+        }
+      }
+      double ax = a.x, ay = a.y;
+      for (int o = 16; o > 0; o >>= 1) {
+        ax += __shfl_xor_sync(0xffffffffu, ax, o);
+        ay += __shfl_xor_sync(0xffffffffu, ay, o);
+      }
+      if (lane == 0) {
+        sh[wp][i].x += ax;
+        sh[wp][i].y += ay;
+      }
+    }
+  }
+  __syncthreads();
+  double2 mine[1] = {make_double2(0, 0)};
+  // thread i < nv owns vector i's block total
+  if (threadIdx.x < nv) {
+    double2 v = make_double2(0, 0);
+    for (int q = 0; q < NTH / 32; ++q) v += sh[q][threadIdx.x];
+    const double sc = scale ? scale[threadIdx.x] : 1.0;
+    mine[0] = make_double2(sc * v.x, sc * v.y);
+  }
+  reduce_rows(mine[0], nv, part, counter, out);
 }
 
-// w -= sum_i coef_i s_i V_i (i < nv); optionally out_norm = ||w||^2 (in .x)
-template <typename T, int NV, bool NORM>
+// w -= sum_i coef_i s_i V_i (i < nv); optionally out_norm.x = ||w||^2
+template <typename T, bool NORM>
 __global__ void __launch_bounds__(NTH) k_maxpy(const cx<T>* __restrict__ V, size_t n, int nv, const double* scale,
                                                const double2* coef, cx<T>* __restrict__ w, double2* part, int* counter,
                                                double2* out_norm, const int* done) {
   if (done && *done) return;
-  __shared__ double2 cf[NV];
-  if (threadIdx.x < NV) {
-    const double s = (scale && threadIdx.x < nv) ? scale[threadIdx.x] : 1.0;
-    cf[threadIdx.x] = threadIdx.x < nv ? make_double2(s * coef[threadIdx.x].x, s * coef[threadIdx.x].y)
-                                       : make_double2(0, 0);
+  __shared__ cx<T> cf[32];
+  if (threadIdx.x < 32) {
+    const int i = threadIdx.x;
+    const double s = (scale && i < nv) ? scale[i] : 1.0;
+    cf[i] = i < nv ? mk<T>((T)(s * coef[i].x), (T)(s * coef[i].y)) : czero<cx<T>>();
   }
   __syncthreads();
-  double2 nrm = make_double2(0, 0);
-  for (size_t k = (size_t)blockIdx.x * NTH + threadIdx.x; k < n; k += (size_t)gridDim.x * NTH) {
-    double2 wk = to_d(w[k]);
+  const size_t chunk = (size_t)NTH * EPT;
+  double nrm = 0.0;
+  for (size_t base = (size_t)blockIdx.x * chunk; base < n; base += (size_t)gridDim.x * chunk) {
+    cx<T> wr[EPT];
 #pragma unroll
-    for (int i = 0; i < NV; ++i)
-      if (i < nv) {
-        const double2 v = to_d(V[(size_t)i * n + k]);
-        const double2 c = cf[i];
-        wk.x -= c.x * v.x - c.y * v.y;
-        wk.y -= c.x * v.y + c.y * v.x;
+    for (int u = 0; u < EPT; ++u) {
+      const size_t k = base + (size_t)u * NTH + threadIdx.x;
+      wr[u] = k < n ? w[k] : czero<cx<T>>();
+    }
+    for (int i = 0; i < nv; ++i) {
+      const cx<T>* Vi = V + (size_t)i * n;
+      const cx<T> c = cf[i];
+#pragma unroll
+      for (int u = 0; u < EPT; ++u) {
+        const size_t k = base + (size_t)u * NTH + threadIdx.x;
+        if (k < n) {
+          const cx<T> v = Vi[k];
+          wr[u].x -= c.x * v.x - c.y * v.y;
+          wr[u].y -= c.x * v.y + c.y * v.x;
+        }
       }
-    const cx<T> o = from_d<cx<T>>(wk);
-    w[k] = o;
-    if (NORM) {
-      const double2 od = to_d(o);
-      nrm.x += od.x * od.x + od.y * od.y;
+    }
+#pragma unroll
+    for (int u = 0; u < EPT; ++u) {
+      const size_t k = base + (size_t)u * NTH + threadIdx.x;
+      if (k < n) {
+        w[k] = wr[u];
+        if (NORM) nrm += (double)wr[u].x * wr[u].x + (double)wr[u].y * wr[u].y;
+      }
     }
   }
   if (NORM) {
-    double2 a[1] = {nrm};
+    double2 a[1] = {make_double2(nrm, 0.0)};
     reduce_to<1>(a, 1, part, counter, out_norm);
   }
 }
@@ -240,72 +308,94 @@ __global__ void k_cycle_init(GState* st, HessPtr h, int m, double tol_abs) {
 __device__ __forceinline__ double cabs_(double2 a) { return hypot(a.x, a.y); }
 
 // Column j of H from the two CGS passes, rotations, residual estimate, and (when the
-// cycle ends) the back substitution.
+// cycle ends) the back substitution. One warp stages the data in shared memory;
+// lane 0 runs the sequential FP64 recurrences.
 __global__ void k_givens(GState* st, HessPtr h, int m, int j) {
-  if (threadIdx.x != 0 || st->done) return;
+  __shared__ double2 col[33], sn[32];
+  __shared__ double cs[32];
+  __shared__ int stop;
+  const int l = threadIdx.x;
+  if (l == 0) stop = st->done;
+  __syncthreads();
+  if (stop) return;
   double2* Hc = h.H + (size_t)j * (m + 1);
-  for (int i = 0; i <= j; ++i) Hc[i] = h.h1[i] + h.h2[i];
-  const double hn = sqrt(h.nrm[0].x);
-  Hc[j + 1] = make_double2(hn, 0);
-  h.scale[j + 1] = hn > 0 ? 1.0 / hn : 0.0;
-  for (int i = 0; i < j; ++i) {
-    const double c = h.cs[i];
-    const double2 s = h.sn[i];
-    const double2 a = Hc[i], b = Hc[i + 1];
-    Hc[i] = c * a + s * b;
-    Hc[i + 1] = c * b - conj_(s) * a;
+  for (int i = l; i <= j; i += 32) col[i] = h.h1[i] + h.h2[i];
+  for (int i = l; i < j; i += 32) {
+    cs[i] = h.cs[i];
+    sn[i] = h.sn[i];
   }
-  const double2 a = Hc[j];
-  const double bb = hn;
-  const double aa = cabs_(a);
-  double c;
-  double2 s;
-  if (bb == 0.0) {
-    c = 1.0;
-    s = make_double2(0, 0);
-  } else if (aa == 0.0) {
-    c = 0.0;
-    s = make_double2(1, 0);
-    Hc[j] = make_double2(bb, 0);
-  } else {
-    const double r = hypot(aa, bb);
-    c = aa / r;
-    const double2 ph = make_double2(a.x / aa, a.y / aa);
-    s = make_double2(ph.x * bb / r, ph.y * bb / r);  // (a/|a|) conj(b)/r with b real
-    Hc[j] = make_double2(ph.x * r, ph.y * r);
-  }
-  Hc[j + 1] = make_double2(0, 0);
-  h.cs[j] = c;
-  h.sn[j] = s;
-  const double2 gj = h.g[j];
-  h.g[j] = c * gj;
-  h.g[j + 1] = make_double2(0, 0) - conj_(s) * gj;
-  const double res = cabs_(h.g[j + 1]);
-  st->res = res;
-  bool end = false;
-  if (!(res == res) || isinf(res)) {
-    st->status = MSC_ERR_NONFINITE;
-    end = true;
-  } else if (res <= st->tol_abs) {
-    st->converged = 1;
-    end = true;
-  } else if (hn <= 1e-300 * (st->beta > 0 ? st->beta : 1.0)) {
-    st->status = MSC_BREAKDOWN;  // invariant subspace: the solution is exact in it
-    end = true;
-  } else if (j + 1 == m) {
-    end = true;
-  }
-  if (end) {
-    const int k = j + 1;
-    st->k = k;
-    for (int i = k - 1; i >= 0; --i) {
-      double2 v = h.g[i];
-      for (int q = i + 1; q < k; ++q) v -= h.H[(size_t)q * (m + 1) + i] * h.y[q];
-      const double2 d = h.H[(size_t)i * (m + 1) + i];
-      const double dd = d.x * d.x + d.y * d.y;
-      h.y[i] = dd > 0 ? make_double2((v.x * d.x + v.y * d.y) / dd, (v.y * d.x - v.x * d.y) / dd) : make_double2(0, 0);
+  __syncthreads();
+  if (l == 0) {
+    const double hn = sqrt(h.nrm[0].x);
+    col[j + 1] = make_double2(hn, 0);
+    h.scale[j + 1] = hn > 0 ? 1.0 / hn : 0.0;
+    for (int i = 0; i < j; ++i) {
+      const double c = cs[i];
+      const double2 s = sn[i];
+      const double2 a = col[i], b = col[i + 1];
+      col[i] = c * a + s * b;
+      col[i + 1] = c * b - conj_(s) * a;
     }
-    st->done = 1;
+    const double2 a = col[j];
+    const double bb = hn;
+    const double aa = cabs_(a);
+    double c;
+    double2 s;
+    if (bb == 0.0) {
+      c = 1.0;
+      s = make_double2(0, 0);
+    } else if (aa == 0.0) {
+      c = 0.0;
+      s = make_double2(1, 0);
+      col[j] = make_double2(bb, 0);
+    } else {
+      const double r = hypot(aa, bb);
+      c = aa / r;
+      const double2 ph = make_double2(a.x / aa, a.y / aa);
+      s = make_double2(ph.x * bb / r, ph.y * bb / r);  // (a/|a|) conj(b)/r with b real
+      col[j] = make_double2(ph.x * r, ph.y * r);
+    }
+    col[j + 1] = make_double2(0, 0);
+    h.cs[j] = c;
+    h.sn[j] = s;
+    const double2 gj = h.g[j];
+    h.g[j] = c * gj;
+    h.g[j + 1] = make_double2(0, 0) - conj_(s) * gj;
+    const double res = cabs_(h.g[j + 1]);
+    st->res = res;
+    bool end = false;
+    if (!(res == res) || isinf(res)) {
+      st->status = MSC_ERR_NONFINITE;
+      end = true;
+    } else if (res <= st->tol_abs) {
+      st->converged = 1;
+      end = true;
+    } else if (hn <= 1e-300 * (st->beta > 0 ? st->beta : 1.0)) {
+      st->status = MSC_BREAKDOWN;  // invariant subspace: the solution is exact in it
+      end = true;
+    } else if (j + 1 == m) {
+      end = true;
+    }
+    stop = end ? 1 : 0;
+  }
+  __syncthreads();
+  for (int i = l; i <= j + 1; i += 32) Hc[i] = col[i];
+  if (stop) {
+    __syncthreads();
+    if (l == 0) {
+      const int k = j + 1;
+      st->k = k;
+      for (int i = k - 1; i >= 0; --i) {
+        double2 v = h.g[i];
+        for (int q = i + 1; q < k; ++q) v -= h.H[(size_t)q * (m + 1) + i] * h.y[q];
+        const double2 d = h.H[(size_t)i * (m + 1) + i];
+        const double dd = d.x * d.x + d.y * d.y;
+        h.y[i] = dd > 0 ? make_double2((v.x * d.x + v.y * d.y) / dd, (v.y * d.x - v.x * d.y) / dd)
+                        : make_double2(0, 0);
+      }
+      __threadfence();
+      st->done = 1;
+    }
   }
 }
 
@@ -350,22 +440,13 @@ __global__ void k_sqrt(const double* a, double* b) {
 }
 
 // ---- host side ---------------------------------------------------------------------------
-static int nv_bucket(int nv) { return nv <= 4 ? 4 : nv <= 8 ? 8 : nv <= 16 ? 16 : 32; }
-
 template <typename T>
 static int mdot(msc_plan* pl, GmresWork* gw, const cx<T>* V, int nv, const double* scale, const cx<T>* w, double2* out,
                 const int* done) {
   GState* st = (GState*)gw->state.p;
   double2* part = (double2*)gw->part.p;
-  const int nb = std::min<long long>(NB, ceil_div((long long)gw->n, NTH));
-#define L_(NV) k_mdot<T, NV><<<nb, NTH, 0, pl->stream>>>(V, gw->n, nv, scale, w, part, &st->counter[0], out, done)
-  switch (nv_bucket(nv)) {
-    case 4: L_(4); break;
-    case 8: L_(8); break;
-    case 16: L_(16); break;
-    default: L_(32); break;
-  }
-#undef L_
+  const int nb = std::min<long long>(NB, ceil_div((long long)gw->n, (long long)NTH * EPT));
+  k_mdot<T><<<nb, NTH, 0, pl->stream>>>(V, gw->n, nv, scale, w, part, &st->counter[0], out, done); ::msc::note_launch();
   MSC_CUDA(cudaGetLastError());
   return MSC_OK;
 }
@@ -375,16 +456,8 @@ static int maxpy(msc_plan* pl, GmresWork* gw, const cx<T>* V, int nv, const doub
                  cx<T>* w, double2* out_norm, const int* done) {
   GState* st = (GState*)gw->state.p;
   double2* part = (double2*)gw->part.p;
-  const int nb = std::min<long long>(NB, ceil_div((long long)gw->n, NTH));
-#define L_(NV) \
-  k_maxpy<T, NV, NORM><<<nb, NTH, 0, pl->stream>>>(V, gw->n, nv, scale, coef, w, part, &st->counter[1], out_norm, done)
-  switch (nv_bucket(nv)) {
-    case 4: L_(4); break;
-    case 8: L_(8); break;
-    case 16: L_(16); break;
-    default: L_(32); break;
-  }
-#undef L_
+  const int nb = std::min<long long>(NB, ceil_div((long long)gw->n, (long long)NTH * EPT));
+  k_maxpy<T, NORM><<<nb, NTH, 0, pl->stream>>>(V, gw->n, nv, scale, coef, w, part, &st->counter[1], out_norm, done); ::msc::note_launch();
   MSC_CUDA(cudaGetLastError());
   return MSC_OK;
 }
@@ -394,7 +467,7 @@ static int resid_norm(msc_plan* pl, GmresWork* gw, const cx<T>* b, const cx<T>* 
   GState* st = (GState*)gw->state.p;
   const int nb = std::min<long long>(NB, ceil_div((long long)gw->n, NTH));
   k_resid_norm<T><<<nb, NTH, 0, pl->stream>>>(b, ax, r, gw->n, (double2*)gw->part.p, &st->counter[2],
-                                             (double2*)out_nrm2);
+                                             (double2*)out_nrm2); ::msc::note_launch();
   MSC_CUDA(cudaGetLastError());
   return MSC_OK;
 }
@@ -443,7 +516,7 @@ void gmres_free(msc_plan* pl) {
 // Returns the number of matvecs used in *n_mv and the final estimate in *res.
 template <typename T>
 static int gmres_core(msc_plan* pl, int m, const cx<T>* rhs, cx<T>* x, bool x_zero, double tol_abs, int max_mv,
-                      int* n_mv, double* res, int* status) {
+                      int* n_mv, double* res, int* status, bool cgs2) {
   GmresWork* gw = pl->gw;
   GState* st = (GState*)gw->state.p;
   HessPtr h = hess_ptrs(gw);
@@ -465,7 +538,7 @@ static int gmres_core(msc_plan* pl, int m, const cx<T>* rhs, cx<T>* x, bool x_ze
       MSC_TRY(resid_norm<T>(pl, gw, rhs, V + n, V, &h.nrm[0].x));
     }
     first = false;
-    k_cycle_init<<<1, 32, 0, pl->stream>>>(st, h, m, tol_abs);
+    k_cycle_init<<<1, 32, 0, pl->stream>>>(st, h, m, tol_abs); ::msc::note_launch();
     MSC_CUDA(cudaGetLastError());
     int enq = 0;  // steps enqueued in this cycle
     bool cycle_over = false;
@@ -481,10 +554,16 @@ static int gmres_core(msc_plan* pl, int m, const cx<T>* rhs, cx<T>* x, bool x_ze
       ++enq;
       cx<T>* w = V + (size_t)(j + 1) * n;
       MSC_TRY(mdot<T>(pl, gw, V, j + 1, h.scale, w, h.h1, done));
-      MSC_TRY((maxpy<T, false>(pl, gw, V, j + 1, h.scale, h.h1, w, nullptr, done)));
-      MSC_TRY(mdot<T>(pl, gw, V, j + 1, h.scale, w, h.h2, done));
-      MSC_TRY((maxpy<T, true>(pl, gw, V, j + 1, h.scale, h.h2, w, &h.nrm[0], done)));
-      k_givens<<<1, 32, 0, pl->stream>>>(st, h, m, j);
+      if (cgs2) {
+        MSC_TRY((maxpy<T, false>(pl, gw, V, j + 1, h.scale, h.h1, w, nullptr, done)));
+        MSC_TRY(mdot<T>(pl, gw, V, j + 1, h.scale, w, h.h2, done));
+        MSC_TRY((maxpy<T, true>(pl, gw, V, j + 1, h.scale, h.h2, w, &h.nrm[0], done)));
+      } else {
+        // one projection; h2 = 0 so the Hessenberg column is h1
+        MSC_CUDA(cudaMemsetAsync(h.h2, 0, sizeof(double2) * (j + 1), pl->stream));
+        MSC_TRY((maxpy<T, true>(pl, gw, V, j + 1, h.scale, h.h1, w, &h.nrm[0], done)));
+      }
+      k_givens<<<1, 32, 0, pl->stream>>>(st, h, m, j); ::msc::note_launch();
       MSC_CUDA(cudaGetLastError());
       const int slot = (pending + 1) & 1;
       MSC_CUDA(cudaMemcpyAsync(&gw->hstate[slot], st, sizeof(GState), cudaMemcpyDeviceToHost, pl->stream));
@@ -507,7 +586,7 @@ static int gmres_core(msc_plan* pl, int m, const cx<T>* rhs, cx<T>* x, bool x_ze
     // x += V y (k columns)
     if (cur.k > 0) {
       const int nb = std::min<long long>(NB, ceil_div((long long)n, NTH));
-      k_update_x<T, T, 32><<<nb, NTH, 0, pl->stream>>>(x, V, n, h.scale, h.y, st);
+      k_update_x<T, T, 32><<<nb, NTH, 0, pl->stream>>>(x, V, n, h.scale, h.y, st); ::msc::note_launch();
       MSC_CUDA(cudaGetLastError());
     }
     *res = cur.res;
@@ -573,7 +652,8 @@ int solve(msc_plan* pl, const double2* b_ref, double2* x_ref, const msc_solve_op
   } else if (o->precision == MSC_SOLVE_FP64) {
     int used = 0, st = 0;
     double est = 0;
-    MSC_TRY(gmres_core<double>(pl, m, b, x, o->initial_guess != 0, tol * bnorm, max_mv, &used, &est, &st));
+    MSC_TRY(gmres_core<double>(pl, m, b, x, o->initial_guess != 0, tol * bnorm, max_mv, &used, &est, &st,
+                               o->ortho != 1));
     s.n_matvec = used;
     s.n_matvec64 = used;
     s.status = st;
@@ -613,12 +693,12 @@ int solve(msc_plan* pl, const double2* b_ref, double2* x_ref, const msc_solve_op
       }
       if (used >= max_mv) break;
       // inner: A d = r / ||r|| in complex64, relative target `inner` (or what is left to reach tol)
-      k_to32_scaled<<<std::min<long long>(NB, ceil_div((long long)n, NTH)), NTH, 0, pl->stream>>>(r, r32, n, dn);
+      k_to32_scaled<<<std::min<long long>(NB, ceil_div((long long)n, NTH)), NTH, 0, pl->stream>>>(r, r32, n, dn); ::msc::note_launch();
       MSC_CUDA(cudaMemsetAsync(d, 0, sizeof(float2) * n, pl->stream));
       const double target = std::max(inner, 0.5 * tol / res);
       int iu = 0, ist = 0;
       double est = 0;
-      MSC_TRY(gmres_core<float>(pl, m, r32, d, true, target, max_mv - used, &iu, &est, &ist));
+      MSC_TRY(gmres_core<float>(pl, m, r32, d, true, target, max_mv - used, &iu, &est, &ist, o->ortho == 2));
       used += iu;
       ++outer;
       if (ist == MSC_ERR_NONFINITE) {
@@ -626,8 +706,8 @@ int solve(msc_plan* pl, const double2* b_ref, double2* x_ref, const msc_solve_op
         break;
       }
       // x += ||r|| d
-      k_sqrt<<<1, 32, 0, pl->stream>>>(dn, dn);
-      k_axpy_mixed<<<std::min<long long>(NB, ceil_div((long long)n, NTH)), NTH, 0, pl->stream>>>(x, d, n, dn);
+      k_sqrt<<<1, 32, 0, pl->stream>>>(dn, dn); ::msc::note_launch();
+      k_axpy_mixed<<<std::min<long long>(NB, ceil_div((long long)n, NTH)), NTH, 0, pl->stream>>>(x, d, n, dn); ::msc::note_launch();
       MSC_CUDA(cudaGetLastError());
       if (iu == 0) break;
     }
@@ -640,7 +720,13 @@ int solve(msc_plan* pl, const double2* b_ref, double2* x_ref, const msc_solve_op
     MSC_TRY(bloch_modulate(pl, x, +1));
   }
   MSC_TRY(launch_soa_to_ref<double, double>(pl, x, x_ref));
+  int kerr = 0;
+  MSC_CUDA(cudaMemcpyAsync(&kerr, pl->status.p, sizeof(int), cudaMemcpyDeviceToHost, pl->stream));
   MSC_CUDA(cudaStreamSynchronize(pl->stream));
+  if (kerr) {
+    set_error("a kernel's bounded wait for its asynchronous copies timed out");
+    return MSC_ERR_CUDA;
+  }
   if (stats) *stats = s;
   return s.status;
 }

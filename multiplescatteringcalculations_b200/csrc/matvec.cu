@@ -2,17 +2,17 @@
 // (Lz, Lx, Ly) grid, the B200 replacement of _slab_matvec_gpu
 // (tmnestor/MultipleScatteringCalculations cubic_scattering/slab_scattering_gpu.py:95-155).
 //
-// Five launches, every one a shared-memory line-FFT pass:
-//   A  tau = T0 x (4 scalars per site), zero padded, FFT along y  -> W[c][n][ky][x]
-//   X  FFT along x (only x < M nonzero)                           -> W[c][n][ky][kx]
-//   B  per (kx, ky) column pair {k, -k}: zero pad z, FFT along z, 9x9 block multiply
-//      by the stored half-space spectrum (K(-k) = S K(k) S, S = diag(1,1,1,-1 x6)),
-//      inverse FFT along z, keep the N_z output planes                 -> W
-//   X' inverse FFT along kx, keep x < M                            -> W[c][m][ky][x]
-//   C  inverse FFT along ky, y = scale*x - acc on the M x M window  -> y
-// The kernel spectrum carries the 1/(Lz Lx Ly) normalisation. W is 9*N_z*Ly*Lx
-// complex and stays L2-resident at the benchmark sizes; the spectrum is streamed
-// once per matvec with evict-first loads.
+// Seven launches over the spectrum workspace W[c][kz][ky][kx] (9 x Lz x Ly x Lx):
+//   A   tau = T0 (s x) (4 scalars per site), zero padded, FFT along y (planes n < N_z)
+//   X   FFT along x (only x < M nonzero)
+//   Z   FFT along z (only n < N_z nonzero)
+//   B   9x9 block multiply by the half-space kernel spectrum, in place
+//   Z'  inverse FFT along z, keep the N_z output planes
+//   X'  inverse FFT along kx, keep x < M
+//   C   inverse FFT along ky, y = s x - acc on the M x M window
+// The FFT passes are shared-memory line FFTs on data that stays in L2 at the
+// benchmark sizes; B streams the kernel spectrum once (evict-first loads). The
+// spectrum carries the 1/(Lz Lx Ly) normalisation.
 #include "mv_common.cuh"
 
 namespace msc {
@@ -27,11 +27,17 @@ int launch_matvec(msc_plan* pl, const cx<T>* x, const double* scale, cx<T>* y, c
   cx<T>* W = (cx<T>*)(sizeof(T) == 8 ? pl->W64.p : pl->W32.p);
   const cx<T>* twz = (const cx<T>*)(sizeof(T) == 8 ? pl->tw64_z.p : pl->tw32_z.p);
   const cx<T>* twxy = (const cx<T>*)(sizeof(T) == 8 ? pl->tw64_xy.p : pl->tw32_xy.p);
-  MSC_TRY(launch_t0_fft_y<T>(pl, x, scale, W, twxy, done));                                                  // A
-  MSC_TRY(launch_fft_contig<T>(pl, W, W, (long long)9 * g.Nz * g.Ly, g.Lx, g.Lx, g.M, g.Lx, pl->fxy, twxy, -1, done));  // X
-  MSC_TRY(launch_zfft_block<T>(pl, W, twz, done));                                                           // B
-  MSC_TRY(launch_fft_contig<T>(pl, W, W, (long long)9 * g.Nz * g.Ly, g.Lx, g.Lx, g.Lx, g.M, pl->fxy, twxy, +1, done));  // X'
-  MSC_TRY(launch_fft_y_out<T>(pl, W, x, scale, y, twxy, done));                                              // C
+  const long long plane = (long long)g.Ly * g.Lx, vol = (long long)g.Lz * plane;
+  MSC_TRY(launch_t0_fft_y<T>(pl, x, scale, W, twxy, done));  // A
+  const long long G = (long long)g.Nz * g.Ly;  // live lines per component: planes n < N_z
+  MSC_TRY(launch_fft_contig<T>(pl, W, W, 9 * G, G, vol, g.Lx, g.M, g.Lx, pl->fxy, twxy, -1, done));  // X
+  MSC_TRY(launch_fft_strided<T>(pl, W, plane, g.Lx, vol, W, plane, g.Lx, vol, nullptr, g.Lx, g.Ly, 9, g.Nz, g.Lz,
+                                pl->fz, twz, -1, done));  // Z
+  MSC_TRY(launch_block_mul<T>(pl, W, done));               // B
+  MSC_TRY(launch_fft_strided<T>(pl, W, plane, g.Lx, vol, W, plane, g.Lx, vol, nullptr, g.Lx, g.Ly, 9, g.Lz, g.Nz,
+                                pl->fz, twz, +1, done));  // Z'
+  MSC_TRY(launch_fft_contig<T>(pl, W, W, 9 * G, G, vol, g.Lx, g.Lx, g.M, pl->fxy, twxy, +1, done));  // X'
+  MSC_TRY(launch_fft_y_out<T>(pl, W, x, scale, y, twxy, done));  // C
   return MSC_OK;
 }
 

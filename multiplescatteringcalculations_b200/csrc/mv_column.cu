@@ -1,6 +1,6 @@
-// Matvec kernel B, complex64 instantiation.
+// Matvec kernel B (block multiply), complex64 instantiation.
 #include "mv_column.cuh"
 
 namespace msc {
-template int launch_zfft_block<float>(msc_plan*, float2*, const float2*, const int*);
+template int launch_block_mul<float>(msc_plan*, float2*, const int*);
 }  // namespace msc

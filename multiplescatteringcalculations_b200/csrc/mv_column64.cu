@@ -1,6 +1,6 @@
-// Matvec kernel B, complex128 instantiation.
+// Matvec kernel B (block multiply), complex128 instantiation.
 #include "mv_column.cuh"
 
 namespace msc {
-template int launch_zfft_block<double>(msc_plan*, double2*, const double2*, const int*);
+template int launch_block_mul<double>(msc_plan*, double2*, const int*);
 }  // namespace msc

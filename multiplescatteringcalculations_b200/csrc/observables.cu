@@ -118,8 +118,8 @@ int rpp_periodic(msc_plan* pl, const double2* psi, double omega, double p, int b
   double2* means = (double2*)pl->red.p;
   double2* res = means + (size_t)9 * g.Nz;
   k_layer_means<256><<<g.Nz, 256, 0, pl->stream>>>(psi, (const double2*)pl->t4_64.p, g.M, g.nsite, pl->desc.a,
-                                                   bloch ? 1 : 0, pl->kpar[0], pl->kpar[1], means);
-  k_rpp_combine<<<1, 32, 0, pl->stream>>>(means, g.Nz, pl->desc.a, omega, pl->desc.alpha, pl->desc.rho, p, res);
+                                                   bloch ? 1 : 0, pl->kpar[0], pl->kpar[1], means); ::msc::note_launch();
+  k_rpp_combine<<<1, 32, 0, pl->stream>>>(means, g.Nz, pl->desc.a, omega, pl->desc.alpha, pl->desc.rho, p, res); ::msc::note_launch();
   MSC_CUDA(cudaGetLastError());
   double2 h;
   MSC_CUDA(cudaMemcpyAsync(&h, res, sizeof(double2), cudaMemcpyDeviceToHost, pl->stream));
@@ -198,7 +198,7 @@ int reflected_field(msc_plan* pl, const double2* psi, double omega, const double
   r.a = pl->desc.a;
   r.M = g.M;
   r.nsite = g.nsite;
-  k_refl_partial<256><<<nb, 256, 0, pl->stream>>>(psi, (const double2*)pl->t4_64.p, r, part);
+  k_refl_partial<256><<<nb, 256, 0, pl->stream>>>(psi, (const double2*)pl->t4_64.p, r, part); ::msc::note_launch();
   MSC_CUDA(cudaGetLastError());
   std::vector<double2> h((size_t)nb * 4);
   MSC_CUDA(cudaMemcpyAsync(h.data(), part, sizeof(double2) * nb * 4, cudaMemcpyDeviceToHost, pl->stream));

@@ -20,6 +20,8 @@ struct Geo {
 };
 
 void set_error(const char* fmt, ...);
+// counts kernel launches of this library (msc_launch_count)
+void note_launch();
 
 #define MSC_CUDA(...)                                                                           \
   do {                                                                                          \
@@ -67,12 +69,15 @@ struct msc_plan {
   double kpar[2] = {0, 0};
   msc::DBuf khat64, khat32;
   msc::DBuf va_blocks;     // [26][81] double
+  msc::DBuf g0_scratch;    // [E][Lz][Ly][Lx] complex128, the spectrum build's work array
   // matvec workspace [9][Nz][Ly][Lx]
   msc::DBuf W64, W32;
   // boundary scratch: SoA copies of in/out fields
   msc::DBuf f64a, f64b, f32a, f32b;
   // reduction scratch (partials, results)
   msc::DBuf red;
+  // device status words: [0] = a bounded wait of a kernel timed out
+  msc::DBuf status;
   // GMRES workspace (lazily grown)
   msc::GmresWork* gw = nullptr;
   int64_t bytes = 0;
@@ -106,7 +111,7 @@ void gmres_free(msc_plan* pl);
 int bloch_modulate(msc_plan* pl, double2* v, int sign);
 
 inline size_t field_elems(const Geo& g) { return (size_t)9 * g.nsite; }
-inline size_t ws_elems(const Geo& g) { return (size_t)9 * g.Nz * g.Ly * g.Lx; }
+inline size_t ws_elems(const Geo& g) { return (size_t)9 * g.Lz * g.Ly * g.Lx; }
 inline size_t khat_elems(const Geo& g, int E) { return (size_t)E * g.Hy * g.Lx * g.Lz; }
 
 }  // namespace msc

@@ -3,13 +3,14 @@
 #include <algorithm>
 
 #include "physics.cuh"
+#include "mv_common.cuh"
 #include "plan.cuh"
 
 namespace msc {
 
 template <typename T>
-int launch_fft_contig(msc_plan* pl, const cx<T>* in, cx<T>* out, long long nlines, long long in_stride,
-                      long long out_stride, int n_in, int n_out, const FftPlan1D& f, const cx<T>* tw, int dir,
+int launch_fft_contig(msc_plan* pl, const cx<T>* in, cx<T>* out, long long nlines, long long G, long long GS,
+                      long long stride, int n_in, int n_out, const FftPlan1D& f, const cx<T>* tw, int dir,
                       const int* done);
 
 // ---- twiddles ------------------------------------------------------------------------
@@ -28,8 +29,8 @@ int build_twiddles(msc_plan* pl) {
   MSC_TRY(dalloc(pl, pl->tw32_z, sizeof(float2) * Lz));
   MSC_TRY(dalloc(pl, pl->tw64_xy, sizeof(double2) * Lxy));
   MSC_TRY(dalloc(pl, pl->tw32_xy, sizeof(float2) * Lxy));
-  k_twiddles<<<ceil_div(Lz, 128), 128, 0, pl->stream>>>((double2*)pl->tw64_z.p, (float2*)pl->tw32_z.p, Lz);
-  k_twiddles<<<ceil_div(Lxy, 128), 128, 0, pl->stream>>>((double2*)pl->tw64_xy.p, (float2*)pl->tw32_xy.p, Lxy);
+  k_twiddles<<<ceil_div(Lz, 128), 128, 0, pl->stream>>>((double2*)pl->tw64_z.p, (float2*)pl->tw32_z.p, Lz); ::msc::note_launch();
+  k_twiddles<<<ceil_div(Lxy, 128), 128, 0, pl->stream>>>((double2*)pl->tw64_xy.p, (float2*)pl->tw32_xy.p, Lxy); ::msc::note_launch();
   MSC_CUDA(cudaGetLastError());
   return MSC_OK;
 }
@@ -58,7 +59,7 @@ int launch_t0(msc_plan* pl, const double* dlam, const double* dmu, const double*
   MSC_TRY(dalloc(pl, pl->t4_32, sizeof(float2) * 4 * g.nsite));
   k_t0<<<ceil_div(g.nsite, 256), 256, 0, pl->stream>>>(dlam, dmu, drho, (double2*)pl->t4_64.p, (float2*)pl->t4_32.p,
                                                        g.nsite, omega, pl->desc.a, pl->desc.alpha, pl->desc.beta,
-                                                       pl->desc.rho);
+                                                       pl->desc.rho); ::msc::note_launch();
   MSC_CUDA(cudaGetLastError());
   return MSC_OK;
 }
@@ -130,7 +131,7 @@ int launch_incident(msc_plan* pl, double omega, const double* k_hat, int wave, d
   }
   const Geo& g = pl->g;
   k_incident<<<ceil_div(g.nsite, 256), 256, 0, pl->stream>>>(ref_out, soa_out, g.M, g.Nz, pl->desc.a, iv, demod ? 1 : 0,
-                                                            pl->kpar[0], pl->kpar[1]);
+                                                            pl->kpar[0], pl->kpar[1]); ::msc::note_launch();
   MSC_CUDA(cudaGetLastError());
   return MSC_OK;
 }
@@ -155,14 +156,14 @@ __global__ void k_soa_to_ref(const cx<Tin>* __restrict__ in, cx<Tout>* __restric
 template <typename Tin, typename Tout>
 int launch_ref_to_soa(msc_plan* pl, const cx<Tin>* in, cx<Tout>* out) {
   const long long n = 9LL * pl->g.nsite;
-  k_ref_to_soa<Tin, Tout><<<ceil_div(n, 256), 256, 0, pl->stream>>>(in, out, pl->g.nsite);
+  k_ref_to_soa<Tin, Tout><<<ceil_div(n, 256), 256, 0, pl->stream>>>(in, out, pl->g.nsite); ::msc::note_launch();
   MSC_CUDA(cudaGetLastError());
   return MSC_OK;
 }
 template <typename Tin, typename Tout>
 int launch_soa_to_ref(msc_plan* pl, const cx<Tin>* in, cx<Tout>* out) {
   const long long n = 9LL * pl->g.nsite;
-  k_soa_to_ref<Tin, Tout><<<ceil_div(n, 256), 256, 0, pl->stream>>>(in, out, pl->g.nsite);
+  k_soa_to_ref<Tin, Tout><<<ceil_div(n, 256), 256, 0, pl->stream>>>(in, out, pl->g.nsite); ::msc::note_launch();
   MSC_CUDA(cudaGetLastError());
   return MSC_OK;
 }
@@ -209,121 +210,59 @@ struct G0Params {
   double scale;    // 1/(Lz Lx Ly)
 };
 
-// Spatial kernel entry e at padded point (z, y, x): sum over the images of the
-// point (or volume-averaged) propagator; SYM stores (K D)_ij for i <= j.
-__global__ void k_g0_spatial(double2* __restrict__ Ks, const double* __restrict__ vab, G0Params p) {
+// Spatial kernel at padded point (z, y, x), all E entries: the sum over the images
+// of the point (or volume-averaged) propagator; SYM stores (K D)_ij for i <= j.
+// One thread per point; Ks[e][point].
+__global__ void __launch_bounds__(128) k_g0_spatial(double2* __restrict__ Ks, const double* __restrict__ vab,
+                                                    G0Params p) {
   const Geo& g = p.g;
   const long long npts = (long long)g.Lz * g.Ly * g.Lx;
   const long long gid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  const int e = blockIdx.y;
   if (gid >= npts) return;
   const int x = (int)(gid % g.Lx);
   const int y = (int)((gid / g.Lx) % g.Ly);
   const int z = (int)(gid / ((long long)g.Lx * g.Ly));
-  int a, b;
-  if (p.E == 45) {
-    int ee = e, i = 0;
-    while (ee >= 9 - i) { ee -= 9 - i; ++i; }
-    a = i;
-    b = i + ee;
-  } else {
-    a = e / 9;
-    b = e % 9;
-  }
   int oz[2], ox[2], oy[2];
   const int nz = axis_offsets(z, g.Lz, g.Nz, false, oz);
   const int nx = axis_offsets(x, g.Lx, g.M, p.periodic, ox);
   const int ny = axis_offsets(y, g.Ly, g.M, p.periodic, oy);
-  double2 acc = make_double2(0, 0);
+  bool first = true;
   for (int iz = 0; iz < nz; ++iz)
     for (int ix = 0; ix < nx; ++ix)
       for (int iy = 0; iy < ny; ++iy) {
         const int dz = oz[iz], dx = ox[ix], dy = oy[iy];
         if (dz == 0 && dx == 0 && dy == 0) continue;  // self term
-        double2 v;
-        if (p.va && abs(dz) <= 1 && abs(dx) <= 1 && abs(dy) <= 1) {
-          v = make_double2(vab[va_slot(dz, dx, dy) * 81 + a * 9 + b], 0.0);
-        } else {
-          PointProp pp;
-          pp.init(dz * p.d, dx * p.d, dy * p.d, p.omega, p.alpha, p.beta, p.rho);
-          v = pp.entry(a, b);
-        }
+        double2 ph = make_double2(p.scale, 0.0);
         if (p.bloch) {
           double s, c;
           sincos(-(p.kx * dx + p.ky * dy) * p.d, &s, &c);
-          v = v * make_double2(c, s);
+          ph = make_double2(p.scale * c, p.scale * s);
         }
-        acc += v;
+        const bool va = p.va && abs(dz) <= 1 && abs(dx) <= 1 && abs(dy) <= 1;
+        const double* vb = va ? vab + va_slot(dz, dx, dy) * 81 : nullptr;
+        PointProp pp;
+        if (!va) pp.init(dz * p.d, dx * p.d, dy * p.d, p.omega, p.alpha, p.beta, p.rho);
+        int e = 0;
+        for (int a = 0; a < 9; ++a)
+          for (int b = (p.E == 45 ? a : 0); b < 9; ++b, ++e) {
+            double2 v = va ? make_double2(vb[a * 9 + b], 0.0) : pp.entry(a, b);
+            if (p.E == 45 && b >= 6) v = 2.0 * v;  // (K D)_ij = K_ij D_j
+            v = v * ph;
+            double2* dst = Ks + (size_t)e * npts + gid;
+            if (first) *dst = v;
+            else *dst = *dst + v;
+          }
+        first = false;
       }
-  double f = p.scale;
-  if (p.E == 45 && b >= 6) f *= 2.0;  // (K D)_ij = K_ij D_j
-  Ks[(size_t)e * npts + gid] = make_double2(f * acc.x, f * acc.y);
-}
-
-// Strided line FFT: element idx of column col in slab (s1, s2) is at
-// base + s1*S1 + s2*S2 + idx*es + col. Output either in place (idx < n_out) or,
-// when TRANS, to out[(s2*O2 + s1*O1 + col) * L + idx] (and a complex64 copy).
-template <typename T, int DIR, int KMAX, bool TRANS>
-__global__ void __launch_bounds__(256) k_fft_strided(cx<T>* data, long long es, int ncol, long long S1, long long S2,
-                                                     int n_in, int n_out, FftPlan1D pl, const cx<T>* __restrict__ twg,
-                                                     cx<T>* out, float2* out32, long long O1, long long O2) {
-  constexpr int TC = 128 / (int)sizeof(cx<T>);
-  constexpr int P = TC + 1;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  cx<T>* tw = reinterpret_cast<cx<T>*>(smem_raw);
-  cx<T>* tile = tw + pl.L;
-  const int tid = threadIdx.x, nthr = blockDim.x;
-  const int col0 = blockIdx.x * TC;
-  const int nc = min(TC, ncol - col0);
-  const long long base = (long long)blockIdx.y * S1 + (long long)blockIdx.z * S2 + col0;
-  for (int t = tid; t < pl.L; t += nthr) tw[t] = twg[t];
-  for (int it = tid; it < TC * pl.L; it += nthr) {
-    const int t = it % TC, idx = it / TC;
-    tile[idx * P + t] = (t < nc && idx < n_in) ? data[base + idx * es + t] : czero<cx<T>>();
-  }
-  __syncthreads();
-  fft_tile<DIR, KMAX>(tile, P, TC, pl, tw, tid, nthr);
-  if (!TRANS) {
-    for (int it = tid; it < TC * n_out; it += nthr) {
-      const int t = it % TC, idx = it / TC;
-      if (t < nc) data[base + idx * es + t] = tile[idx * P + t];
-    }
-  } else {
-    const long long ob = (long long)blockIdx.z * O2 + (long long)blockIdx.y * O1 + col0;
-    for (int it = tid; it < TC * pl.L; it += nthr) {
-      const int idx = it % pl.L, t = it / pl.L;
-      if (t < nc) {
-        const cx<T> v = tile[idx * P + t];
-        out[(ob + t) * pl.L + idx] = v;
-        if (out32) out32[(ob + t) * pl.L + idx] = make_float2((float)v.x, (float)v.y);
-      }
-    }
+  if (first) {  // no offset maps here: zero
+    for (int e = 0; e < p.E; ++e) Ks[(size_t)e * npts + gid] = make_double2(0, 0);
   }
 }
 
-template <bool TRANS>
-static int launch_fft_strided64(msc_plan* pl, double2* data, long long es, int ncol, long long S1, int n1, long long S2,
-                                int n2, int n_in, int n_out, const FftPlan1D& f, const double2* tw, double2* out,
-                                float2* out32, long long O1, long long O2) {
-  constexpr int TC = 8;
-  const int nthr = 256;
-  const size_t sm = sizeof(double2) * ((size_t)f.L + (size_t)f.L * (TC + 1));
-  const int kmax = fft_kmax_needed(f, TC, nthr);
-  dim3 grid((unsigned)((ncol + TC - 1) / TC), (unsigned)n1, (unsigned)n2);
-#define CALL(K)                                                                                               \
-  {                                                                                                           \
-    auto kern = k_fft_strided<double, -1, K, TRANS>;                                                          \
-    MSC_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));               \
-    kern<<<grid, nthr, sm, pl->stream>>>(data, es, ncol, S1, S2, n_in, n_out, f, tw, out, out32, O1, O2);     \
-  }
-  if (kmax <= 1) CALL(1) else if (kmax <= 2) CALL(2) else if (kmax <= 4) CALL(4) else if (kmax <= 8) CALL(8) else {
-    set_error("strided FFT needs KMAX=%d", kmax);
-    return MSC_ERR_UNSUPPORTED;
-  }
-#undef CALL
-  MSC_CUDA(cudaGetLastError());
-  return MSC_OK;
-}
+template <typename T>
+int launch_fft_strided(msc_plan* pl, const cx<T>* in, long long es, long long S1, long long S2, cx<T>* out,
+                       long long eo, long long O1, long long O2, float2* out32, int ncol, int n1, int n2, int n_in,
+                       int n_out, const FftPlan1D& f, const cx<T>* tw, int dir, const int* done);
 
 int launch_g0(msc_plan* pl, double omega, const double* kpar, int va, int n_orders) {
   // The Bloch-phased kernel loses the parity K(-r) = S K(r) S, so its spectrum is
@@ -341,11 +280,12 @@ int launch_g0(msc_plan* pl, double omega, const double* kpar, int va, int n_orde
   MSC_TRY(dalloc(pl, pl->khat32, sizeof(float2) * khat_elems(g, E)));
   MSC_TRY(dalloc(pl, pl->va_blocks, sizeof(double) * 26 * 81));
   const long long npts = (long long)g.Lz * g.Ly * g.Lx;
-  DBuf ks;
-  MSC_TRY(dalloc(pl, ks, sizeof(double2) * (size_t)E * npts));
+  // FP64 spatial kernel and its partial transforms; kept by the plan for the next frequency
+  MSC_TRY(dalloc(pl, pl->g0_scratch, sizeof(double2) * (size_t)E * npts));
+  DBuf& ks = pl->g0_scratch;
   if (va) {
     k_va_blocks<<<1, 32, 0, pl->stream>>>((double*)pl->va_blocks.p, pl->desc.alpha, pl->desc.beta, pl->desc.rho, omega,
-                                          n_orders);
+                                          n_orders); ::msc::note_launch();
     MSC_CUDA(cudaGetLastError());
   }
   G0Params p;
@@ -362,30 +302,26 @@ int launch_g0(msc_plan* pl, double omega, const double* kpar, int va, int n_orde
   p.kx = kpar ? kpar[0] : 0.0;
   p.ky = kpar ? kpar[1] : 0.0;
   p.scale = 1.0 / ((double)g.Lz * g.Lx * g.Ly);
-  dim3 grid((unsigned)ceil_div(npts, 128), (unsigned)E);
-  k_g0_spatial<<<grid, 128, 0, pl->stream>>>((double2*)ks.p, (const double*)pl->va_blocks.p, p);
+  k_g0_spatial<<<(unsigned)ceil_div(npts, 128), 128, 0, pl->stream>>>((double2*)ks.p, (const double*)pl->va_blocks.p, p); ::msc::note_launch();
   MSC_CUDA(cudaGetLastError());
   double2* K = (double2*)ks.p;
   const double2* twxy = (const double2*)pl->tw64_xy.p;
   const double2* twz = (const double2*)pl->tw64_z.p;
+  const long long plane = (long long)g.Ly * g.Lx, vol = (long long)g.Lz * plane;
   // x pass (contiguous lines), in place
-  int s = launch_fft_contig<double>(pl, K, K, (long long)E * g.Lz * g.Ly, g.Lx, g.Lx, g.Lx, g.Lx, pl->fxy, twxy, -1,
-                                    nullptr);
+  int s = launch_fft_contig<double>(pl, K, K, (long long)E * g.Lz * g.Ly, (long long)E * g.Lz * g.Ly, 0, g.Lx, g.Lx,
+                                    g.Lx, pl->fxy, twxy, -1, nullptr);
   // y pass: axis stride Lx, columns x, slabs (z, e); keep ky < Hy
   if (s == MSC_OK)
-    s = launch_fft_strided64<false>(pl, K, g.Lx, g.Lx, (long long)g.Ly * g.Lx, g.Lz, (long long)g.Lz * g.Ly * g.Lx, E,
-                                    g.Ly, g.Hy, pl->fxy, twxy, nullptr, nullptr, 0, 0);
-  // z pass: axis stride Ly*Lx, columns kx, slabs (ky < Hy, e); transposed store to khat[e][ky][kx][kz]
+    s = launch_fft_strided<double>(pl, K, g.Lx, plane, vol, K, g.Lx, plane, vol, nullptr, g.Lx, g.Lz, E, g.Ly, g.Hy,
+                                   pl->fxy, twxy, -1, nullptr);
+  // z pass: axis stride Ly*Lx, columns kx, slabs (ky < Hy, e); written to khat[e][kz][ky][kx]
+  // in complex128 and complex64
+  const long long hplane = (long long)g.Hy * g.Lx;
   if (s == MSC_OK)
-    s = launch_fft_strided64<true>(pl, K, (long long)g.Ly * g.Lx, g.Lx, g.Lx, g.Hy, (long long)g.Lz * g.Ly * g.Lx, E,
-                                   g.Lz, g.Lz, pl->fz, twz, (double2*)pl->khat64.p, (float2*)pl->khat32.p, g.Lx,
-                                   (long long)g.Hy * g.Lx);
-  // the scratch is released after the stream drains (cudaFreeAsync keeps stream order)
-  if (ks.p) {
-    cudaFreeAsync(ks.p, pl->stream);
-    pl->bytes -= (int64_t)ks.bytes;
-    ks.p = nullptr;
-  }
+    s = launch_fft_strided<double>(pl, K, plane, g.Lx, vol, (double2*)pl->khat64.p, hplane, g.Lx,
+                                   (long long)g.Lz * hplane, (float2*)pl->khat32.p, g.Lx, g.Hy, E, g.Lz, g.Lz, pl->fz,
+                                   twz, -1, nullptr);
   return s;
 }
 

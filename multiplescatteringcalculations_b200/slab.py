@@ -33,6 +33,7 @@ __all__ = [
     "SlabPlan",
     "SlabResult",
     "compute_slab_scattering_gpu",
+    "clear_plan_cache",
     "compute_slab_tmatrices",
     "gaussian_random_field_material",
     "random_slab_material",
@@ -274,15 +275,19 @@ class SlabPlan:
         return y
 
     def solve(self, b: torch.Tensor, *, tol: float, max_iter: int, restart: int = 30, precision: str = "mixed",
-              initial_guess: str = "born", inner_tol: float = 0.0, x: torch.Tensor | None = None):
+              initial_guess: str = "born", inner_tol: float = 0.0, x: torch.Tensor | None = None,
+              ortho: str = "auto"):
         """Solve (I - G0 T0) x = b; returns (x, stats dict)."""
         if precision not in ("mixed", "fp64"):
             raise ValueError(f"precision must be 'mixed' or 'fp64', got {precision!r}")
         bb = b.to(device=self.device, dtype=torch.complex128).contiguous()
         xx = torch.empty_like(bb) if x is None else x
+        if ortho not in ("auto", "cgs1", "cgs2"):
+            raise ValueError(f"ortho must be 'auto', 'cgs1' or 'cgs2', got {ortho!r}")
         opts = N.SolveOpts(float(tol), int(max_iter), int(restart),
                            N.MSC_SOLVE_MIXED if precision == "mixed" else N.MSC_SOLVE_FP64,
-                           0 if initial_guess == "born" else 1, float(inner_tol))
+                           0 if initial_guess == "born" else 1, float(inner_tol),
+                           {"auto": 0, "cgs1": 1, "cgs2": 2}[ortho])
         st = N.SolveStats()
         status = N.check(self.lib.msc_solve(self.handle, _ptr(bb), _ptr(xx), C.byref(opts), C.byref(st)), "msc_solve")
         stats = {"n_matvec": st.n_matvec, "n_matvec64": st.n_matvec64, "n_outer": st.n_outer, "status": status,
@@ -345,6 +350,32 @@ def compute_slab_tmatrices(geometry: SlabGeometry, material: SlabMaterial, omega
 # ---------------------------------------------------------------------------
 
 
+_PLAN_CACHE: dict = {}
+_PLAN_CACHE_SIZE = 2
+
+
+def _cached_plan(geometry: SlabGeometry, ref: ReferenceMedium, periodic: bool, device) -> SlabPlan:
+    """Plans are reused across calls with the same geometry, medium, periodicity
+    and device (allocations and FFT set-up happen once); the two most recent
+    plans are kept."""
+    dev = _device(device)
+    key = (geometry.M, geometry.N_z, float(geometry.a), float(ref.alpha), float(ref.beta), float(ref.rho),
+           bool(periodic), dev.index)
+    plan = _PLAN_CACHE.pop(key, None)
+    if plan is None:
+        plan = SlabPlan(geometry, ref, periodic=periodic, device=dev)
+        while len(_PLAN_CACHE) >= _PLAN_CACHE_SIZE:
+            _PLAN_CACHE.pop(next(iter(_PLAN_CACHE))).close()
+    _PLAN_CACHE[key] = plan
+    return plan
+
+
+def clear_plan_cache() -> None:
+    """Release the cached plans (their device memory)."""
+    while _PLAN_CACHE:
+        _PLAN_CACHE.popitem()[1].close()
+
+
 def _bloch_kpar(omega: float, ref: ReferenceMedium, k_hat, wave_type: str) -> tuple[float, float]:
     kh = np.asarray(k_hat, dtype=float)
     kh = kh / np.linalg.norm(kh)
@@ -372,6 +403,7 @@ def compute_slab_scattering_gpu(
     preconditioner=None,
     bloch: bool = False,
     inner_tol: float = 0.0,
+    ortho: str = "auto",
     plan: SlabPlan | None = None,
 ) -> SlabResult:
     """Solve (I - G0 T0) psi = psi0 on the GPU.
@@ -380,8 +412,10 @@ def compute_slab_scattering_gpu(
     additions: ``restart`` (GMRES(m)), ``precision`` ("mixed": complex64 inner
     GMRES inside FP64 iterative refinement, "fp64": plain complex128 GMRES),
     ``bloch`` (periodic only: Bloch-phased lateral fold for oblique incidence;
-    False is the reference's phase-free fold), ``inner_tol`` and ``plan`` (reuse
-    a plan of the same geometry). ``dtype`` is accepted for compatibility
+    False is the reference's phase-free fold), ``inner_tol``, ``ortho`` (Arnoldi
+    orthogonalisation: "auto" = one classical Gram-Schmidt pass in the complex64
+    inner solves and two in FP64 solves; "cgs1"; "cgs2") and ``plan`` (reuse a
+    plan of the same geometry). ``dtype`` is accepted for compatibility
     (complex64 or complex128); the arithmetic is set by ``precision`` and the
     returned field is always complex128 with its FP64 true residual.
     ``preconditioner`` must be None.
@@ -394,44 +428,39 @@ def compute_slab_scattering_gpu(
         raise ValueError("preconditioner must be None in this version")
     if bloch and not periodic:
         raise ValueError("bloch=True needs periodic=True")
-    own = plan is None
-    if own:
-        plan = SlabPlan(geometry, material.ref, periodic=periodic, device=device)
+    if plan is None:
+        plan = _cached_plan(geometry, material.ref, periodic, device)
     elif plan.periodic != bool(periodic) or plan.geometry != geometry:
         raise ValueError("plan geometry/periodicity does not match the problem")
-    try:
-        kp = _bloch_kpar(omega, material.ref, k_hat, wave_type) if bloch else None
-        plan.build_t0(material, omega)
-        plan.build_g0(omega, kpar=kp, volume_averaged=volume_averaged, n_orders=n_orders)
-        psi0 = plan.incident(omega, k_hat, wave_type)
-        x, st = plan.solve(psi0, tol=gmres_tol, max_iter=max_iter, restart=restart, precision=precision,
-                           initial_guess=initial_guess, inner_tol=inner_tol)
-        if st["residual"] > gmres_tol:
-            warnings.warn(
-                f"GPU GMRES did not converge: rel_res={st['residual']:.2e} after {st['n_matvec']} matvecs",
-                stacklevel=2,
-            )
-        t4 = plan.t0_scalars()
-        psi = x.cpu().numpy()
-        res = SlabResult(
-            psi=psi,
-            psi0=psi0.cpu().numpy(),
-            geometry=geometry,
-            material=material,
-            omega=float(omega),
-            k_hat=np.asarray(k_hat, dtype=float),
-            wave_type=wave_type,
-            n_gmres_iter=int(st["n_matvec"]),
-            gmres_residual=float(st["residual"]),
-            periodic=bool(periodic),
-            t0=t4.cpu().numpy(),
-            bloch=bool(bloch),
-            stats=st,
+    kp = _bloch_kpar(omega, material.ref, k_hat, wave_type) if bloch else None
+    plan.build_t0(material, omega)
+    plan.build_g0(omega, kpar=kp, volume_averaged=volume_averaged, n_orders=n_orders)
+    psi0 = plan.incident(omega, k_hat, wave_type)
+    x, st = plan.solve(psi0, tol=gmres_tol, max_iter=max_iter, restart=restart, precision=precision,
+                       initial_guess=initial_guess, inner_tol=inner_tol, ortho=ortho)
+    if st["residual"] > gmres_tol:
+        warnings.warn(
+            f"GPU GMRES did not converge: rel_res={st['residual']:.2e} after {st['n_matvec']} matvecs",
+            stacklevel=2,
         )
-        return res
-    finally:
-        if own:
-            plan.close()
+    t4 = plan.t0_scalars()
+    psi = x.cpu().numpy()
+    res = SlabResult(
+        psi=psi,
+        psi0=psi0.cpu().numpy(),
+        geometry=geometry,
+        material=material,
+        omega=float(omega),
+        k_hat=np.asarray(k_hat, dtype=float),
+        wave_type=wave_type,
+        n_gmres_iter=int(st["n_matvec"]),
+        gmres_residual=float(st["residual"]),
+        periodic=bool(periodic),
+        t0=t4.cpu().numpy(),
+        bloch=bool(bloch),
+        stats=st,
+    )
+    return res
 
 
 # ---------------------------------------------------------------------------

@@ -438,27 +438,52 @@ def slab_kernel_spatial(M, N_z, a, omega, alpha, beta, rho, *, volume_averaged=F
     propagator is evaluated on the fundamental domain 0 <= dy <= dx < M and
     expanded by the D4h orbit R P R^T; nearest neighbours (max |offset| <= 1)
     use the volume-averaged propagator at each signed offset when enabled.
-    Index [k, ix, iy] holds offset (k-(N_z-1), ix-(M-1), iy-(M-1)).
+    Index [k, ix, iy] holds offset (k-(N_z-1), ix-(M-1), iy-(M-1)). The orbit
+    operations are applied in the reference's order (slab_scattering.py:241-259),
+    vectorised over the fundamental points, so where two images of one point
+    coincide the later operation wins, as in the reference loop.
     """
     d = 2.0 * a
     S = 2 * M - 1
     n_dz = 2 * N_z - 1
     ker = np.zeros((n_dz, S, S, 9, 9), dtype=complex)
-    fd = [(dx, dy) for dx in range(M) for dy in range(dx + 1)]
+    fd = np.array([(dx, dy) for dx in range(M) for dy in range(dx + 1)], dtype=int)
+    I9 = np.eye(9)
+    # (target offset as a function of (dx, dy), 9x9 transform, which points take part)
+    ops = [
+        (lambda x, y: (x, y), I9, "all"),
+        (lambda x, y: (-x, y), _RX, "nz"),
+        (lambda x, y: (x, -y), _RY, "nz"),
+        (lambda x, y: (-x, -y), _RX @ _RY, "nz"),
+        (lambda x, y: (y, x), _P90, "off"),
+        (lambda x, y: (-y, x), _RX @ _P90, "off"),
+        (lambda x, y: (y, -x), _RY @ _P90, "off"),
+        (lambda x, y: (-y, -x), _RX @ _RY @ _P90, "off"),
+    ]
     for k in range(n_dz):
         dz = k - (N_z - 1)
-        pts = [(dx, dy) for dx, dy in fd if not (dx == 0 and dy == 0 and dz == 0)]
-        if not pts:
+        keep = ~((fd[:, 0] == 0) & (fd[:, 1] == 0) & (dz == 0))
+        pts = fd[keep]
+        if pts.size == 0:
             continue
-        r = np.array([[dz * d, dx * d, dy * d] for dx, dy in pts])
+        r = np.stack([np.full(len(pts), dz * d), pts[:, 0] * d, pts[:, 1] * d], axis=1)
         blocks = point_propagator(r, omega, alpha, beta, rho)
-        for (dx, dy), G in zip(pts, blocks):
-            nn = max(abs(dz), dx, dy) <= 1
-            for sdx, sdy, R9 in _orbit(dx, dy):
-                if volume_averaged and nn:
-                    ker[k, sdx + M - 1, sdy + M - 1] = va_propagator((dz, sdx, sdy), alpha, beta, rho, omega, n_orders)
-                else:
-                    ker[k, sdx + M - 1, sdy + M - 1] = R9 @ G @ R9.T
+        nn = np.maximum(abs(dz), np.maximum(pts[:, 0], pts[:, 1])) <= 1
+        zero = (pts[:, 0] == 0) & (pts[:, 1] == 0)
+        diag = pts[:, 0] == pts[:, 1]
+        for tgt, R9, which in ops:
+            sel = np.ones(len(pts), bool) if which == "all" else (~zero if which == "nz" else ~diag)
+            if volume_averaged:
+                sel = sel & ~nn
+            if not np.any(sel):
+                continue
+            tx, ty = tgt(pts[sel, 0], pts[sel, 1])
+            ker[k, tx + M - 1, ty + M - 1] = np.einsum("ab,nbc,dc->nad", R9, blocks[sel], R9)
+        if volume_averaged:
+            for dx, dy in pts[nn]:
+                for sdx, sdy, _ in _orbit(int(dx), int(dy)):
+                    ker[k, sdx + M - 1, sdy + M - 1] = va_propagator((dz, sdx, sdy), alpha, beta, rho, omega,
+                                                                     n_orders)
     return ker
 
 
@@ -495,29 +520,47 @@ def build_slab_kernels(M, N_z, a, omega, alpha, beta, rho, *, volume_averaged=Fa
 # ---------------------------------------------------------------------------
 
 
-def slab_matvec(psi_flat, T_local, kernel_hat, M, N_z, *, periodic=False):
+def slab_matvec(psi_flat, T_local, kernel_hat, M, N_z, *, periodic=False, threads=1):
     """(I - G T) psi by 2D FFT per layer and the O(N_z^2) layer-pair sum.
 
     ``T_local`` is either the (N_z,M,M,9,9) matrices or the (4,N_z,M,M) scalars.
+    ``threads`` > 1 runs the FFTs with scipy.fft workers and the output layers of
+    the layer-pair sum in a thread pool (the same arithmetic, for CPU timing).
     """
     psi = psi_flat.reshape(N_z, M, M, 9)
     if T_local.ndim == 4 and T_local.shape[0] == 4:
         tau = apply_t0(T_local, psi)
     else:
         tau = np.einsum("lmnab,lmnb->lmna", T_local, psi)
+    fft2, ifft2 = np.fft.fft2, np.fft.ifft2
+    if threads > 1:
+        import scipy.fft as sfft
+
+        fft2 = lambda x, axes: sfft.fft2(x, axes=axes, workers=threads)  # noqa: E731
+        ifft2 = lambda x, axes: sfft.ifft2(x, axes=axes, workers=threads)  # noqa: E731
     if periodic:
         H = M
-        tau_hat = np.fft.fft2(tau, axes=(1, 2))
+        tau_hat = fft2(tau, axes=(1, 2))
     else:
         H = 2 * M - 1
         pad = np.zeros((N_z, H, H, 9), dtype=complex)
         pad[:, :M, :M] = tau
-        tau_hat = np.fft.fft2(pad, axes=(1, 2))
+        tau_hat = fft2(pad, axes=(1, 2))
     acc = np.zeros((N_z, H, H, 9), dtype=complex)
-    for m in range(N_z):
+
+    def layer(m):
         for n in range(N_z):
             acc[m] += np.einsum("xyij,xyj->xyi", kernel_hat[m - n + N_z - 1], tau_hat[n])
-    acc = np.fft.ifft2(acc, axes=(1, 2))
+
+    if threads > 1:
+        from concurrent.futures import ThreadPoolExecutor
+
+        with ThreadPoolExecutor(threads) as ex:
+            list(ex.map(layer, range(N_z)))
+    else:
+        for m in range(N_z):
+            layer(m)
+    acc = ifft2(acc, axes=(1, 2))
     if not periodic:
         acc = acc[:, M - 1 :, M - 1 :]
     return (psi - acc).ravel()
@@ -593,7 +636,7 @@ def incident_field(M, N_z, a, omega, alpha, beta, k_hat, wave_type):
 
 
 def solve(M, N_z, a, alpha, beta, rho, dlam, dmu, drho, omega, k_hat, wave_type="P", gmres_tol=1e-6, max_iter=500,
-          *, volume_averaged=False, n_orders=2, periodic=False, restart=20, phase_xy=None):
+          *, volume_averaged=False, n_orders=2, periodic=False, restart=20, phase_xy=None, threads=1, timings=None):
     """scipy GMRES on the FFT operator with x0 = psi0, as ``compute_slab_scattering``.
 
     ``restart=20`` is scipy's default that the reference call uses
@@ -601,9 +644,14 @@ def solve(M, N_z, a, alpha, beta, rho, dlam, dmu, drho, omega, k_hat, wave_type=
     (including the final residual matvec, as the reference counts it) and the
     true relative residual.
     """
+    import time
+
+    t_0 = time.perf_counter()
     t4 = t0_scalars(omega, a, alpha, beta, rho, dlam, dmu, drho)
+    t_1 = time.perf_counter()
     kh = build_slab_kernels(M, N_z, a, omega, alpha, beta, rho, volume_averaged=volume_averaged, n_orders=n_orders,
                             periodic=periodic, phase_xy=phase_xy)
+    t_2 = time.perf_counter()
     psi0 = incident_field(M, N_z, a, omega, alpha, beta, k_hat, wave_type)
     b = psi0.ravel()
     if phase_xy is not None:
@@ -613,11 +661,14 @@ def solve(M, N_z, a, alpha, beta, rho, dlam, dmu, drho, omega, k_hat, wave_type=
 
     def mv(x):
         cnt[0] += 1
-        return slab_matvec(x, t4, kh, M, N_z, periodic=periodic)
+        return slab_matvec(x, t4, kh, M, N_z, periodic=periodic, threads=threads)
 
     A = LinearOperator((n, n), matvec=mv, dtype=complex)
+    t_3 = time.perf_counter()
     x, info = gmres(A, b, x0=b.copy(), rtol=gmres_tol, maxiter=max_iter, restart=restart)
     res = np.linalg.norm(mv(x) - b) / np.linalg.norm(b)
+    if timings is not None:
+        timings.update(t0=t_1 - t_0, kernel=t_2 - t_1, solve=time.perf_counter() - t_3)
     psi = x.reshape(N_z, M, M, 9)
     if phase_xy is not None:
         psi = psi / bloch_demodulation(M, N_z, a, phase_xy)[..., None]

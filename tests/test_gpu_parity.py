@@ -246,9 +246,11 @@ def test_oblique_random_solve_vs_oracle():
     ora = O.solve(10, 3, 1.0, ref.alpha, ref.beta, ref.rho, mat.Dlambda, mat.Dmu, mat.Drho, om, kh, "S", 1e-13,
                   restart=30)
     for prec in ("mixed", "fp64"):
-        res = compute_slab_scattering_gpu(g, mat, om, kh, "S", gmres_tol=1e-11, precision=prec, restart=30)
-        assert res.gmres_residual < 1e-11
-        assert _rel(res.psi, ora["psi"]) < 1e-9
+        for ortho in ("auto", "cgs1", "cgs2"):
+            res = compute_slab_scattering_gpu(g, mat, om, kh, "S", gmres_tol=1e-11, precision=prec, restart=30,
+                                              ortho=ortho)
+            assert res.gmres_residual < 1e-11, (prec, ortho)
+            assert _rel(res.psi, ora["psi"]) < 1e-9, (prec, ortho)
 
 
 def test_nonconvergence_warns_and_reports():
