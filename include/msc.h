@@ -112,6 +112,19 @@ int msc_incident(msc_plan* plan, double omega, const double* k_hat, int wave_typ
  * _slab_matvec (slab_scattering.py:359-418). x and y may not alias. */
 int msc_matvec(msc_plan* plan, const void* x, void* y, int precision);
 
+/* The same operator as msc_matvec, for callers that cannot allocate device memory
+ * when they apply it: a host framework whose allocator owns the device memory and
+ * forbids other allocations, or a real-time loop that must not risk an allocation's
+ * latency or failure mid-run. msc_matvec allocates two field copies on first use;
+ * this call allocates nothing. Its scratch is one static device array of this
+ * library, at most 64 MiB, resident on every GPU that loads the library until the
+ * process exits. A plan needing more (9*Lz*Ly*Lx + 18*N_z*M*M complex elements,
+ * each aligned up to 256 bytes) is rejected with MSC_ERR_INVALID. The first call on a
+ * device looks the array up with cudaGetSymbolAddress (make it with that device
+ * current, before any stream capture). All calls share the array: calls whose GPU
+ * work overlaps race on it. No counterpart in the reference. */
+int msc_matvec_noalloc(msc_plan* plan, const void* x, void* y, int precision);
+
 /* Solve (I - G0 T0) x = b; b, x complex128 (N_z, M, M, 9). Restarted GMRES with
  * CGS2 Arnoldi and FP64 Givens/least squares; precision MIXED runs complex64
  * inner solves inside FP64 iterative refinement. Replaces torch_gmres

@@ -79,6 +79,7 @@ SIGNATURES = {
     "msc_build_g0": (C.c_int, [C.c_void_p, C.c_double, C.c_void_p, C.c_int, C.c_int]),
     "msc_incident": (C.c_int, [C.c_void_p, C.c_double, C.c_void_p, C.c_int, C.c_void_p]),
     "msc_matvec": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int]),
+    "msc_matvec_noalloc": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int]),
     "msc_solve": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(SolveOpts), C.POINTER(SolveStats)]),
     "msc_rpp_periodic": (C.c_int, [C.c_void_p, C.c_void_p, C.c_double, C.c_double, C.c_int, C.c_void_p]),
     "msc_reflected_field": (C.c_int, [C.c_void_p, C.c_void_p, C.c_double, C.c_void_p, C.c_void_p]),
