@@ -334,6 +334,35 @@ def run_ours(args, wl, rank, world, local_rank):
     return 0
 
 
+def run_matvecs(wl: dict, n: int) -> int:
+    """Plan + T0 + G0 of the workload, then n complex64 operator applications
+    (each: 2 layout transposes and the 7 matvec launches). Prints the mean time."""
+    import ctypes as C
+
+    import torch
+
+    from multiplescatteringcalculations_b200 import SlabPlan, _native
+
+    dev = torch.device("cuda", 0)
+    ref, geom, mat, k_hat, omega = make_problem(wl, seed=1000)
+    plan = SlabPlan(geom, ref, periodic=wl["periodic"], device=dev)
+    plan.build_t0(mat, omega)
+    plan.build_g0(omega)
+    lib = _native.load()
+    x = torch.randn(geom.N_z, geom.M, geom.M, 9, dtype=torch.complex64, device=dev)
+    y = torch.empty_like(x)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(n):
+        _native.check(lib.msc_matvec(plan.handle, C.c_void_p(x.data_ptr()), C.c_void_p(y.data_ptr()), 0), "matvec")
+    e1.record()
+    torch.cuda.synchronize()
+    print(json.dumps({"matvecs": n, "us_per_matvec": e0.elapsed_time(e1) * 1e3 / n, "fft": plan.fft_sizes()}))
+    plan.close()
+    return 0
+
+
 def main(argv=None) -> int:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -344,6 +373,8 @@ def main(argv=None) -> int:
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--solve-only", action="store_true", help="timed solves only (for profiler launch lists)")
+    ap.add_argument("--matvec-only", type=int, default=0, metavar="N",
+                    help="build the plan and run N complex64 matvecs through msc_matvec (for kernel profiles)")
     args = ap.parse_args(argv)
     wl = WORKLOADS[args.workload]
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -351,6 +382,8 @@ def main(argv=None) -> int:
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
         return run_reference(args, wl, rank, world)
+    if args.matvec_only:
+        return run_matvecs(wl, args.matvec_only)
     if world > 1:
         import datetime
 

@@ -273,3 +273,17 @@ def test_input_validation():
         compute_slab_scattering_gpu(g, mat, -1.0, KZ)
     with pytest.raises(ValueError):
         compute_slab_scattering_gpu(g, mat, OMEGA, KZ, device="cpu")
+
+
+def test_run_from_config_matches_oracle():
+    """The YAML entry (reference schema) solves the same slab as the oracle."""
+    from pathlib import Path
+
+    from multiplescatteringcalculations_b200.solver_config import build_material, load_config, run_from_config
+
+    cfg = load_config(Path(__file__).resolve().parent / "configs" / "slab_small.yml")
+    res = run_from_config(cfg)
+    mat = build_material(cfg)
+    ora = O.solve(6, 3, 1.0, 5000.0, 3000.0, 2500.0, mat.Dlambda, mat.Dmu, mat.Drho, 150.0, KZ, "P", 1e-13)
+    assert res.gmres_residual < 1e-10
+    assert _rel(res.psi, ora["psi"]) < 1e-9
