@@ -277,7 +277,7 @@ def run_ours(args, wl, rank, world, local_rank):
     peak, peak_kind = _peaks()
     achieved = b_alg / t_mv / 1e9
     traffic = None
-    tf = ROOT / "profiles" / f"matvec_{args.workload}_traffic.txt"
+    tf = ROOT / "profiles" / f"matvec_{args.workload}_traffic.txt"  # warm-cache ncu capture, per matvec
     if tf.exists():
         for ln in tf.read_text().splitlines():
             if ln.startswith("dram_bytes_per_matvec:"):
