@@ -4,7 +4,7 @@
 #include <cstdio>
 #include <cstring>
 
-#include "plan.cuh"
+#include "mv_common.cuh"
 
 namespace msc {
 
@@ -161,17 +161,16 @@ int msc_plan_create(const msc_slab_desc* d, void* stream, msc_plan** out) {
   }
   g.Lz = Lz;
   g.Lx = g.Ly = Lxy;
-  g.Hy = Lxy / 2 + 1;
-  g.half = 1;
+  set_spectrum_box(g, true);
   if (!make_fft_plan(Lz, &pl->fz) || !make_fft_plan(Lxy, &pl->fxy)) {
     delete pl;
     set_error("FFT lengths (Lz=%d, Lxy=%d) need prime factors <= 11 and length <= 4096", Lz, Lxy);
     return MSC_ERR_UNSUPPORTED;
   }
-  // shared memory of the column kernel: (Lz + Lz*(2*9*8+1)) complex128
-  if ((size_t)(Lz + (size_t)Lz * 145) * 16 > 227 * 1024) {
+  // the fused z-pass kernel holds at least 36 lines of Lz complex128 twice
+  if (zbz_min_smem64(Lz) > (size_t)ZBZ_SMEM_LIMIT) {
     delete pl;
-    set_error("Lz=%d exceeds the column kernel's shared memory (N_z <= 48)", Lz);
+    set_error("Lz=%d exceeds the shared memory of the fused z pass (Lz <= 192, N_z <= 96)", Lz);
     return MSC_ERR_UNSUPPORTED;
   }
   int s = build_twiddles(pl);

@@ -144,16 +144,18 @@ template <int R, int DIR, typename C> struct Dft {
   }
 };
 
-// One Stockham stage src -> dst. Thread owns line l and butterflies j0, j0 + jstride, ...
+// One Stockham stage src -> dst. Element idx of line l sits at idx*is + l*ls.
+// Thread owns line l and butterflies j0, j0 + jstride, ...
 template <int R, int DIR, bool POW2, typename C>
-__device__ __forceinline__ void fft_stage(const C* __restrict__ src, C* __restrict__ dst, int pitch, int L, int Ns,
-                                          const C* __restrict__ tw, int l, int j0, int jstride) {
+__device__ __forceinline__ void fft_stage(const C* __restrict__ src, C* __restrict__ dst, int is, int ls, int L,
+                                          int Ns, const C* __restrict__ tw, int l, int j0, int jstride) {
   const int nb = L / R;
   const int tstep = L / (Ns * R);
+  const int lo = l * ls;
   for (int j = j0; j < nb; j += jstride) {
     C v[R];
 #pragma unroll
-    for (int r = 0; r < R; ++r) v[r] = src[(j + r * nb) * pitch + l];
+    for (int r = 0; r < R; ++r) v[r] = src[(j + r * nb) * is + lo];
     const int kk = POW2 ? (j & (Ns - 1)) : (j % Ns);
     if (Ns > 1) {
 #pragma unroll
@@ -166,15 +168,17 @@ __device__ __forceinline__ void fft_stage(const C* __restrict__ src, C* __restri
     Dft<R, DIR, C>::run(v);
     const int idxD = (j - kk) * R + kk;
 #pragma unroll
-    for (int r = 0; r < R; ++r) dst[(idxD + r * Ns) * pitch + l] = v[r];
+    for (int r = 0; r < R; ++r) dst[(idxD + r * Ns) * is + lo] = v[r];
   }
 }
 
-// Full transform of every line of the tile in `a`, using `b` as the second tile.
-// Returns the tile holding the result (a or b). Needs nthr >= nlines; threads
-// tid >= (nthr / nlines) * nlines idle during the stages. Ends with a barrier.
+// Full transform of every line of the tile in `a`, using `b` as the second tile;
+// element idx of line l at idx*is + l*ls. Returns the tile holding the result (a
+// or b). Needs nthr >= nlines; threads tid >= (nthr / nlines) * nlines idle during
+// the stages. Ends with a barrier.
 template <int DIR, bool POW2, typename C>
-__device__ C* fft_tile(C* a, C* b, int pitch, int nlines, const FftPlan1D& pl, const C* tw, int tid, int nthr) {
+__device__ __forceinline__ C* fft_tile2(C* a, C* b, int is, int ls, int nlines, const FftPlan1D& pl, const C* tw,
+                                        int tid, int nthr) {
   const int jstride = nthr / nlines;
   const bool active = tid < jstride * nlines;
   const int l = tid % nlines;
@@ -184,16 +188,16 @@ __device__ C* fft_tile(C* a, C* b, int pitch, int nlines, const FftPlan1D& pl, c
   for (int s = 0; s < pl.nstages; ++s) {
     const int Ns = pl.ns[s];
     switch (pl.radix[s]) {
-      case 8: fft_stage<8, DIR, POW2>(src, dst, pitch, pl.L, Ns, tw, l, j0, jstride); break;
-      case 4: fft_stage<4, DIR, POW2>(src, dst, pitch, pl.L, Ns, tw, l, j0, jstride); break;
-      case 2: fft_stage<2, DIR, POW2>(src, dst, pitch, pl.L, Ns, tw, l, j0, jstride); break;
+      case 8: fft_stage<8, DIR, POW2>(src, dst, is, ls, pl.L, Ns, tw, l, j0, jstride); break;
+      case 4: fft_stage<4, DIR, POW2>(src, dst, is, ls, pl.L, Ns, tw, l, j0, jstride); break;
+      case 2: fft_stage<2, DIR, POW2>(src, dst, is, ls, pl.L, Ns, tw, l, j0, jstride); break;
       default:
         if (!POW2) {
           switch (pl.radix[s]) {
-            case 3: fft_stage<3, DIR, false>(src, dst, pitch, pl.L, Ns, tw, l, j0, jstride); break;
-            case 5: fft_stage<5, DIR, false>(src, dst, pitch, pl.L, Ns, tw, l, j0, jstride); break;
-            case 7: fft_stage<7, DIR, false>(src, dst, pitch, pl.L, Ns, tw, l, j0, jstride); break;
-            case 11: fft_stage<11, DIR, false>(src, dst, pitch, pl.L, Ns, tw, l, j0, jstride); break;
+            case 3: fft_stage<3, DIR, false>(src, dst, is, ls, pl.L, Ns, tw, l, j0, jstride); break;
+            case 5: fft_stage<5, DIR, false>(src, dst, is, ls, pl.L, Ns, tw, l, j0, jstride); break;
+            case 7: fft_stage<7, DIR, false>(src, dst, is, ls, pl.L, Ns, tw, l, j0, jstride); break;
+            case 11: fft_stage<11, DIR, false>(src, dst, is, ls, pl.L, Ns, tw, l, j0, jstride); break;
             default: break;
           }
         }
@@ -205,6 +209,82 @@ __device__ C* fft_tile(C* a, C* b, int pitch, int nlines, const FftPlan1D& pl, c
     dst = t;
   }
   return src;
+}
+
+// Lines interleaved: element idx of line l at idx*pitch + l.
+template <int DIR, bool POW2, typename C>
+__device__ C* fft_tile(C* a, C* b, int pitch, int nlines, const FftPlan1D& pl, const C* tw, int tid, int nthr) {
+  return fft_tile2<DIR, POW2>(a, b, pitch, 1, nlines, pl, tw, tid, nthr);
+}
+
+// ---- compile-time engine for power-of-two lengths ---------------------------
+// The same Stockham stages with the length, the radix sequence, the tile pitch,
+// the line count and the block size known at compile time: every stride and
+// loop bound is a constant, the loops unroll and the address arithmetic folds
+// into the shared-memory offsets.
+constexpr int ilog2(int n) { return n <= 1 ? 0 : 1 + ilog2(n / 2); }
+
+template <int L> struct Pow2Plan {
+  static_assert(L >= 2 && (L & (L - 1)) == 0, "power-of-two length");
+  static constexpr int LG = ilog2(L);
+  static constexpr int N8 = LG / 3;
+  static constexpr int NSTAGES = N8 + (LG % 3 != 0 ? 1 : 0);
+  static constexpr int radix(int s) { return s < N8 ? 8 : (LG % 3 == 2 ? 4 : 2); }
+  static constexpr int ns(int s) { return s == 0 ? 1 : ns(s - 1) * radix(s - 1); }
+};
+
+// Stage (R, NS) for line l, butterflies j0, j0 + JS, ...; element idx of line l at
+// idx * P + l.
+template <int R, int NS, int L, int DIR, int P, int JS, typename C>
+__device__ __forceinline__ void fft_stage_ct(const C* __restrict__ src, C* __restrict__ dst, const C* __restrict__ tw,
+                                             int l, int j0) {
+  constexpr int NB = L / R;
+  constexpr int TSTEP = L / (NS * R);
+  constexpr int ITER = (NB + JS - 1) / JS;
+#pragma unroll
+  for (int it = 0; it < ITER; ++it) {
+    const int j = j0 + it * JS;
+    if (NB % JS != 0 && j >= NB) break;
+    C v[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) v[r] = src[(j + r * NB) * P + l];
+    const int kk = j & (NS - 1);
+    if (NS > 1) {
+#pragma unroll
+      for (int r = 1; r < R; ++r) {
+        C w = tw[r * kk * TSTEP];
+        if (DIR > 0) w.y = -w.y;
+        v[r] = v[r] * w;
+      }
+    }
+    Dft<R, DIR, C>::run(v);
+    const int idxD = (j - kk) * R + kk;
+#pragma unroll
+    for (int r = 0; r < R; ++r) dst[(idxD + r * NS) * P + l] = v[r];
+  }
+}
+
+template <int S, int L, int DIR, int P, int JS, typename C>
+__device__ __forceinline__ void fft_stages_ct(C* src, C* dst, const C* tw, int l, int j0, bool active) {
+  using PL = Pow2Plan<L>;
+  if constexpr (S < PL::NSTAGES) {
+    if (active) fft_stage_ct<PL::radix(S), PL::ns(S), L, DIR, P, JS>(src, dst, tw, l, j0);
+    __syncthreads();
+    fft_stages_ct<S + 1, L, DIR, P, JS>(dst, src, tw, l, j0, active);
+  }
+}
+
+// Full transform of the NLINES lines of tile a (pitch P), b the second tile; the
+// block has NTHR threads. Returns the tile holding the result. Ends with a barrier.
+template <int L, int DIR, int P, int NLINES, int NTHR, typename C>
+__device__ __forceinline__ C* fft_tile_ct(C* a, C* b, const C* tw, int tid) {
+  constexpr int JS = NTHR / NLINES;
+  static_assert(JS >= 1, "at least one thread per line");
+  const bool active = tid < JS * NLINES;
+  const int l = tid % NLINES;
+  const int j0 = tid / NLINES;
+  fft_stages_ct<0, L, DIR, P, JS>(a, b, tw, l, j0, active);
+  return (Pow2Plan<L>::NSTAGES % 2 == 0) ? a : b;
 }
 
 }  // namespace msc

@@ -2,45 +2,45 @@
 // (Lz, Lx, Ly) grid, the B200 replacement of _slab_matvec_gpu
 // (tmnestor/MultipleScatteringCalculations cubic_scattering/slab_scattering_gpu.py:95-155).
 //
-// Seven launches over the spectrum workspace W[c][kz][ky][kx] (9 x Lz x Ly x Lx):
-//   A   tau = T0 (s x) (4 scalars per site), zero padded, FFT along y (planes n < N_z)
-//   X   FFT along x (only x < M nonzero)
-//   Z   FFT along z (only n < N_z nonzero)
-//   B   9x9 block multiply by the half-space kernel spectrum, in place
-//   Z'  inverse FFT along z, keep the N_z output planes
-//   X'  inverse FFT along kx, keep x < M
-//   C   inverse FFT along ky, y = s x - acc on the M x M window
-// The FFT passes are shared-memory line FFTs on data that stays in L2 at the
-// benchmark sizes; B streams the kernel spectrum once (evict-first loads). The
+// Five launches over the workspace W[c][n][ky][kx] (9 x N_z x Ly x Lx):
+//   A    tau = T0 (s x) (4 scalars per site), zero padded, FFT along y
+//   X    FFT along x (only x < M nonzero)
+//   ZBZ' per column (ky, kx), all 9 components in shared memory: FFT along z
+//        (zero padded to Lz), 9x9 block multiply by the kernel spectrum, inverse
+//        FFT along z, keep the N_z layers
+//   X'   inverse FFT along kx, keep x < M
+//   C    inverse FFT along ky, y = s x - acc on the M x M window
+// The x and y passes are shared-memory line FFTs on data that stays in L2 at the
+// benchmark sizes; the z-padded spectrum exists only inside ZBZ'. The kernel
 // spectrum carries the 1/(Lz Lx Ly) normalisation.
 #include "mv_common.cuh"
 
 namespace msc {
 
 template <typename T>
-int launch_matvec(msc_plan* pl, const cx<T>* x, const double* scale, cx<T>* y, const int* done) {
+int launch_matvec_ws(msc_plan* pl, const cx<T>* x, const double* scale, cx<T>* y, cx<T>* W, const int* done) {
   const Geo& g = pl->g;
   if (!pl->has_t0 || !pl->has_g0) {
     set_error("matvec needs build_t0 and build_g0 first");
     return MSC_ERR_STATE;
   }
-  cx<T>* W = (cx<T>*)(sizeof(T) == 8 ? pl->W64.p : pl->W32.p);
-  const cx<T>* twz = (const cx<T>*)(sizeof(T) == 8 ? pl->tw64_z.p : pl->tw32_z.p);
   const cx<T>* twxy = (const cx<T>*)(sizeof(T) == 8 ? pl->tw64_xy.p : pl->tw32_xy.p);
-  const long long plane = (long long)g.Ly * g.Lx, vol = (long long)g.Lz * plane;
-  MSC_TRY(launch_t0_fft_y<T>(pl, x, scale, W, twxy, done));  // A
-  const long long G = (long long)g.Nz * g.Ly;  // live lines per component: planes n < N_z
-  MSC_TRY(launch_fft_contig<T>(pl, W, W, 9 * G, G, vol, g.Lx, g.M, g.Lx, pl->fxy, twxy, -1, done));  // X
-  MSC_TRY(launch_fft_strided<T>(pl, W, plane, g.Lx, vol, W, plane, g.Lx, vol, nullptr, g.Lx, g.Ly, 9, g.Nz, g.Lz,
-                                pl->fz, twz, -1, done));  // Z
-  MSC_TRY(launch_block_mul<T>(pl, W, done));               // B
-  MSC_TRY(launch_fft_strided<T>(pl, W, plane, g.Lx, vol, W, plane, g.Lx, vol, nullptr, g.Lx, g.Ly, 9, g.Lz, g.Nz,
-                                pl->fz, twz, +1, done));  // Z'
-  MSC_TRY(launch_fft_contig<T>(pl, W, W, 9 * G, G, vol, g.Lx, g.Lx, g.M, pl->fxy, twxy, +1, done));  // X'
-  MSC_TRY(launch_fft_y_out<T>(pl, W, x, scale, y, twxy, done));  // C
+  const long long G = (long long)9 * g.Nz * g.Ly;  // x lines, contiguous rows of W
+  MSC_TRY(launch_t0_fft_y<T>(pl, x, scale, W, twxy, done));                                       // A
+  MSC_TRY(launch_fft_contig<T>(pl, W, W, G, G, 0, g.Lx, g.M, g.Lx, pl->fxy, twxy, -1, done));      // X
+  MSC_TRY(launch_zbz<T>(pl, W, done));                                                            // ZBZ'
+  MSC_TRY(launch_fft_contig<T>(pl, W, W, G, G, 0, g.Lx, g.Lx, g.M, pl->fxy, twxy, +1, done));      // X'
+  MSC_TRY(launch_fft_y_out<T>(pl, W, x, scale, y, twxy, done));                                   // C
   return MSC_OK;
 }
 
+template <typename T>
+int launch_matvec(msc_plan* pl, const cx<T>* x, const double* scale, cx<T>* y, const int* done) {
+  return launch_matvec_ws<T>(pl, x, scale, y, (cx<T>*)(sizeof(T) == 8 ? pl->W64.p : pl->W32.p), done);
+}
+
+template int launch_matvec_ws<float>(msc_plan*, const float2*, const double*, float2*, float2*, const int*);
+template int launch_matvec_ws<double>(msc_plan*, const double2*, const double*, double2*, double2*, const int*);
 template int launch_matvec<float>(msc_plan*, const float2*, const double*, float2*, const int*);
 template int launch_matvec<double>(msc_plan*, const double2*, const double*, double2*, const int*);
 

@@ -70,6 +70,25 @@ template <typename C> __device__ __forceinline__ C from_d(double2 a) { return to
 __device__ __forceinline__ float2 ld_stream(const float2* p) { return __ldcs(p); }
 __device__ __forceinline__ double2 ld_stream(const double2* p) { return __ldcs(p); }
 
+// Asynchronous global -> shared copies (cp.async): one complex element per call,
+// zero-filled without a read when ok is false (src must still be a valid address).
+// Many copies stay in flight per thread; cp_async_wait_all() then a barrier
+// makes them visible to the block.
+__device__ __forceinline__ void cp_async_elem(float2* dst, const float2* src, bool ok) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(d), "l"(src), "r"(ok ? 8 : 0) : "memory");
+}
+__device__ __forceinline__ void cp_async_elem(double2* dst, const double2* src, bool ok) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(d), "l"(src), "r"(ok ? 16 : 0) : "memory");
+}
+// 16 bytes, both addresses 16-byte aligned
+__device__ __forceinline__ void cp_async16(void* dst, const void* src) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
 inline int ceil_div(long long a, long long b) { return (int)((a + b - 1) / b); }
 
 }  // namespace msc

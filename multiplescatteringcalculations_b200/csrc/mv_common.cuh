@@ -52,6 +52,60 @@ inline cudaError_t prep_kernel(const void* fn) {
   return e;
 }
 
+// Fused z pass (mv_zbz.cuh). A block holds 9 components x 4 KX column slots
+// (lines) of Lz points twice (ping-pong) plus the twiddles and, for an octant
+// spectrum, the block's contiguous slice of the kernel spectrum.
+constexpr int ZBZ_THREADS = 288;
+constexpr int ZBZ_MAX_LINES = 144;
+constexpr int ZBZ_SMEM_LIMIT = 227 * 1024 - 2048;  // opt-in maximum less the static tables
+
+struct ZbzLayout {
+  int KX;       // kx per quadrant; 4 KX column slots per block, KX in {4, 2, 1}
+  int NXC;      // kx chunks of the octant, ceil(Hx / KX)
+  int CS;       // elements of one block's spectrum slice [e][kz][j], a 16-byte multiple
+  int ksm;      // 1: the slice is staged in shared memory
+  size_t smem;  // dynamic shared memory of a block
+};
+
+// Layout for element type T. Preference: two blocks per SM with the slice in
+// shared memory, then two blocks per SM reading the slice from global memory,
+// then one block per SM. The octant spectrum of type T is stored blocked with
+// this layout: slice (ky_o, xc) at ((ky_o * NXC + xc) * CS), entry (e, kz, j) at
+// (e * Hz + kz) * KX + j, kx = xc * KX + j (zero beyond Hx).
+template <typename T> constexpr ZbzLayout zbz_layout(int Lz, int Hz, int Hx, int E, bool oct) {
+  const size_t es = sizeof(cx<T>);
+  const int al = (int)(16 / es);
+  auto tiles = [&](int kx) { return es * ((size_t)Lz + 2 * (size_t)Lz * (36 * kx + 1)); };
+  auto make = [&](int kx, int ksm) {
+    ZbzLayout L{};
+    L.KX = kx;
+    L.NXC = oct ? (Hx + kx - 1) / kx : 0;
+    L.CS = oct ? (E * Hz * kx + al - 1) / al * al : 0;
+    L.ksm = ksm;
+    L.smem = tiles(kx) + (ksm ? es * (size_t)L.CS : 0);
+    return L;
+  };
+  const size_t two = (size_t)(ZBZ_SMEM_LIMIT / 2);
+  if (oct)
+    for (int kx = 4; kx >= 1; kx /= 2)
+      if (make(kx, 1).smem <= two) return make(kx, 1);
+  for (int kx = 4; kx >= 1; kx /= 2)
+    if (make(kx, 0).smem <= two) return make(kx, 0);
+  if (oct && make(1, 1).smem <= (size_t)ZBZ_SMEM_LIMIT) return make(1, 1);
+  return make(1, 0);
+}
+template <typename T> inline ZbzLayout zbz_layout(const Geo& g, int E) {
+  return zbz_layout<T>(g.Lz, g.Hz, g.Hx, E, g.oct != 0);
+}
+// elements of the stored kernel spectrum of type T
+template <typename T> inline size_t khat_elems_t(const Geo& g, int E) {
+  if (!g.oct) return (size_t)E * g.Hz * g.Hy * g.Hx;
+  const ZbzLayout L = zbz_layout<T>(g, E);
+  return (size_t)g.Hy * L.NXC * L.CS;
+}
+// smallest shared memory of the fused z pass for complex128 (one block per SM)
+inline size_t zbz_min_smem64(int Lz) { return sizeof(double2) * ((size_t)Lz + 2 * (size_t)Lz * 37); }
+
 #define MSC_POW2_DISPATCH(pow2, CALL) \
   do {                                \
     if (pow2) { CALL(true); }         \
@@ -70,7 +124,7 @@ int launch_fft_strided(msc_plan* pl, const cx<T>* in, long long es, long long S1
                        long long eo, long long O1, long long O2, float2* out32, int ncol, int n1, int n2, int n_in,
                        int n_out, const FftPlan1D& f, const cx<T>* tw, int dir, const int* done);
 template <typename T>
-int launch_block_mul(msc_plan* pl, cx<T>* W, const int* done);
+int launch_zbz(msc_plan* pl, cx<T>* W, const int* done);
 template <typename T>
 int launch_fft_y_out(msc_plan* pl, const cx<T>* W, const cx<T>* x, const double* scale, cx<T>* y, const cx<T>* tw,
                      const int* done);

@@ -45,7 +45,7 @@ __global__ void __launch_bounds__(256, 4) k_t0_fft_y(const cx<T>* __restrict__ x
   }
   __syncthreads();
   const C* res = fft_tile<-1, POW2>(ta, tb, P, TR, pl, tw, tid, nthr);
-  C* Wl = W + ((size_t)(c * g.Lz + n) * g.Ly) * g.Lx + i0;
+  C* Wl = W + ((size_t)(c * g.Nz + n) * g.Ly) * g.Lx + i0;
   for (int it = tid; it < TR * g.Ly; it += nthr) {
     const int r = it & (TR - 1), ky = it / TR;  // TR is a power of two
     if (r < nr) Wl[(size_t)ky * g.Lx + r] = res[ky * P + r];

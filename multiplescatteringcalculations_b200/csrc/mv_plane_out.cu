@@ -19,7 +19,7 @@ __global__ void __launch_bounds__(256, 4) k_fft_y_out(const cx<T>* __restrict__ 
   const int c = blockIdx.z, m = blockIdx.y, x0 = blockIdx.x * TR;
   const int nr = min(TR, g.M - x0);
   for (int t = tid; t < g.Ly; t += nthr) tw[t] = twg[t];
-  const C* Wl = W + ((size_t)(c * g.Lz + m) * g.Ly) * g.Lx + x0;
+  const C* Wl = W + ((size_t)(c * g.Nz + m) * g.Ly) * g.Lx + x0;
   for (int it = tid; it < TR * g.Ly; it += nthr) {
     const int r = it & (TR - 1), ky = it / TR;  // TR is a power of two
     ta[ky * P + r] = (r < nr) ? Wl[(size_t)ky * g.Lx + r] : czero<C>();

@@ -59,20 +59,8 @@ static int matvec_static(msc_plan* pl, const cx<T>* x_ref, cx<T>* y_ref, unsigne
   cx<T>* W = reinterpret_cast<cx<T>*>(scratch);
   cx<T>* xs = reinterpret_cast<cx<T>*>(scratch + align256(sizeof(cx<T>) * ws_elems(g)));
   cx<T>* ys = reinterpret_cast<cx<T>*>(reinterpret_cast<unsigned char*>(xs) + align256(sizeof(cx<T>) * nf));
-  const cx<T>* twz = (const cx<T>*)(sizeof(T) == 8 ? pl->tw64_z.p : pl->tw32_z.p);
-  const cx<T>* twxy = (const cx<T>*)(sizeof(T) == 8 ? pl->tw64_xy.p : pl->tw32_xy.p);
-  const long long plane = (long long)g.Ly * g.Lx, vol = (long long)g.Lz * plane;
-  const long long G = (long long)g.Nz * g.Ly;
   MSC_TRY((launch_ref_to_soa<T, T>(pl, x_ref, xs)));
-  MSC_TRY(launch_t0_fft_y<T>(pl, xs, nullptr, W, twxy, nullptr));
-  MSC_TRY(launch_fft_contig<T>(pl, W, W, 9 * G, G, vol, g.Lx, g.M, g.Lx, pl->fxy, twxy, -1, nullptr));
-  MSC_TRY(launch_fft_strided<T>(pl, W, plane, g.Lx, vol, W, plane, g.Lx, vol, nullptr, g.Lx, g.Ly, 9, g.Nz, g.Lz,
-                                pl->fz, twz, -1, nullptr));
-  MSC_TRY(launch_block_mul<T>(pl, W, nullptr));
-  MSC_TRY(launch_fft_strided<T>(pl, W, plane, g.Lx, vol, W, plane, g.Lx, vol, nullptr, g.Lx, g.Ly, 9, g.Lz, g.Nz,
-                                pl->fz, twz, +1, nullptr));
-  MSC_TRY(launch_fft_contig<T>(pl, W, W, 9 * G, G, vol, g.Lx, g.Lx, g.M, pl->fxy, twxy, +1, nullptr));
-  MSC_TRY(launch_fft_y_out<T>(pl, W, xs, nullptr, ys, twxy, nullptr));
+  MSC_TRY(launch_matvec_ws<T>(pl, xs, nullptr, ys, W, nullptr));
   MSC_TRY((launch_soa_to_ref<T, T>(pl, ys, y_ref)));
   return MSC_OK;
 }

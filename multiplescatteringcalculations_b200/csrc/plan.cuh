@@ -14,8 +14,12 @@ namespace msc {
 struct Geo {
   int M, Nz;
   int Lz, Lx, Ly;  // padded FFT lengths (Lx = Ly)
-  int Hy;          // stored spectrum lines ky in [0, Hy): Ly/2 + 1 (half), Ly (full)
-  int half;        // 1: half-space spectrum, columns k and -k share K(-k) = S K(k) S
+  // Stored spectrum box kz < Hz, ky < Hy, kx < Hx. Octant (oct = 1): H = L/2 + 1 on
+  // each axis; the kernel is mirror symmetric, K(R_a k) = S_a K(k) S_a for the
+  // reflection of each axis a, and every wavevector reads its mirror image in the
+  // box. Full (oct = 0, Bloch-phased kernels, which lose the symmetry): H = L.
+  int Hz, Hy, Hx;
+  int oct;
   int nsite;       // Nz*M*M
 };
 
@@ -60,7 +64,7 @@ struct msc_plan {
   bool has_t0 = false;
   double omega_t0 = 0;
   msc::DBuf t4_64, t4_32;  // [4][nsite]
-  // G0 spectrum [E][Hy][Lx][Lz]
+  // G0 spectrum: octant, blocked per the fused z pass layout; full: [E][Hz][Hy][Hx]
   bool has_g0 = false;
   int E = 0;               // 45 (symmetric form) or 81 (full, volume averaged)
   int va = 0, n_orders = 2;
@@ -70,7 +74,7 @@ struct msc_plan {
   msc::DBuf khat64, khat32;
   msc::DBuf va_blocks;     // [26][81] double
   msc::DBuf g0_scratch;    // [E][Lz][Ly][Lx] complex128, the spectrum build's work array
-  // matvec workspace [9][Nz][Ly][Lx]
+  // matvec workspace [9][Nz][Ly][Lx] (y and x transformed, z in space)
   msc::DBuf W64, W32;
   // boundary scratch: SoA copies of in/out fields
   msc::DBuf f64a, f64b, f32a, f32b;
@@ -102,6 +106,9 @@ int launch_soa_to_ref(msc_plan* pl, const cx<Tin>* in, cx<Tout>* out);
 // y = x - G0 T0 (scale * x), SoA; scale may be null (1). done may be null.
 template <typename T>
 int launch_matvec(msc_plan* pl, const cx<T>* x, const double* scale, cx<T>* y, const int* done);
+// the same on a caller-provided workspace of ws_elems(g) elements
+template <typename T>
+int launch_matvec_ws(msc_plan* pl, const cx<T>* x, const double* scale, cx<T>* y, cx<T>* W, const int* done);
 
 int rpp_periodic(msc_plan* pl, const double2* psi_ref, double omega, double p, int bloch, double* out);
 int reflected_field(msc_plan* pl, const double2* psi_ref, double omega, const double* k_hat, double* out);
@@ -111,7 +118,13 @@ void gmres_free(msc_plan* pl);
 int bloch_modulate(msc_plan* pl, double2* v, int sign);
 
 inline size_t field_elems(const Geo& g) { return (size_t)9 * g.nsite; }
-inline size_t ws_elems(const Geo& g) { return (size_t)9 * g.Lz * g.Ly * g.Lx; }
-inline size_t khat_elems(const Geo& g, int E) { return (size_t)E * g.Hy * g.Lx * g.Lz; }
+inline size_t ws_elems(const Geo& g) { return (size_t)9 * g.Nz * g.Ly * g.Lx; }
+// Set the stored spectrum box: octant (mirror-symmetric kernel) or full.
+inline void set_spectrum_box(Geo& g, bool octant) {
+  g.oct = octant ? 1 : 0;
+  g.Hz = octant ? g.Lz / 2 + 1 : g.Lz;
+  g.Hy = octant ? g.Ly / 2 + 1 : g.Ly;
+  g.Hx = octant ? g.Lx / 2 + 1 : g.Lx;
+}
 
 }  // namespace msc

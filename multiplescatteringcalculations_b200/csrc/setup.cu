@@ -264,11 +264,54 @@ int launch_fft_strided(msc_plan* pl, const cx<T>* in, long long es, long long S1
                        long long eo, long long O1, long long O2, float2* out32, int ncol, int n1, int n2, int n_in,
                        int n_out, const FftPlan1D& f, const cx<T>* tw, int dir, const int* done);
 
+// Copy the spectrum box kz < Hz, ky < Hy, kx < Hx of the transformed work array
+// K[e][z][y][x] into the stored layout of element type T: blocked slices of the
+// fused z pass for an octant spectrum (zero in the padding and beyond Hx), plain
+// [e][kz][ky][kx] for a full one.
+template <typename T>
+__global__ void k_khat_pack(const double2* __restrict__ K, cx<T>* __restrict__ out, Geo g, int E, ZbzLayout lay,
+                            long long n) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  int e, kz, ky, kx;
+  bool ok = true;
+  if (g.oct) {
+    const long long blk = i / lay.CS;
+    const int r = (int)(i - blk * lay.CS);
+    const int xc = (int)(blk % lay.NXC);
+    ky = (int)(blk / lay.NXC);
+    const int j = r % lay.KX, ekz = r / lay.KX;
+    e = ekz / g.Hz;
+    kz = ekz % g.Hz;
+    kx = xc * lay.KX + j;
+    ok = e < E && kx < g.Hx;
+  } else {
+    long long t = i;
+    kx = (int)(t % g.Hx);
+    t /= g.Hx;
+    ky = (int)(t % g.Hy);
+    t /= g.Hy;
+    kz = (int)(t % g.Hz);
+    e = (int)(t / g.Hz);
+  }
+  const double2 v = ok ? K[(((long long)e * g.Lz + kz) * g.Ly + ky) * g.Lx + kx] : make_double2(0.0, 0.0);
+  out[i] = from_d<cx<T>>(v);
+}
+
+template <typename T> static int launch_khat_pack(msc_plan* pl, const double2* K, cx<T>* out, int E) {
+  const Geo& g = pl->g;
+  const long long n = (long long)khat_elems_t<T>(g, E);
+  k_khat_pack<T><<<ceil_div(n, 256), 256, 0, pl->stream>>>(K, out, g, E, zbz_layout<T>(g, E), n);
+  ::msc::note_launch();
+  MSC_CUDA(cudaGetLastError());
+  return MSC_OK;
+}
+
 int launch_g0(msc_plan* pl, double omega, const double* kpar, int va, int n_orders) {
-  // The Bloch-phased kernel loses the parity K(-r) = S K(r) S, so its spectrum is
-  // stored on the full (kx, ky) plane; otherwise on the half plane ky <= Ly/2.
-  pl->g.half = kpar ? 0 : 1;
-  pl->g.Hy = pl->g.half ? pl->g.Ly / 2 + 1 : pl->g.Ly;
+  // The kernel is mirror symmetric in each axis, K(R_a r) = S_a K(r) S_a, and its
+  // spectrum is stored on the octant kz <= Lz/2, ky <= Ly/2, kx <= Lx/2. The
+  // Bloch-phased kernel loses the symmetry in x and y and is stored in full.
+  set_spectrum_box(pl->g, kpar == nullptr);
   const Geo& g = pl->g;
   const int E = va ? 81 : 45;
   if (pl->khat64.p && pl->E != E) {
@@ -276,8 +319,8 @@ int launch_g0(msc_plan* pl, double omega, const double* kpar, int va, int n_orde
     dfree(pl, pl->khat32);
   }
   pl->E = E;
-  MSC_TRY(dalloc(pl, pl->khat64, sizeof(double2) * khat_elems(g, E)));
-  MSC_TRY(dalloc(pl, pl->khat32, sizeof(float2) * khat_elems(g, E)));
+  MSC_TRY(dalloc(pl, pl->khat64, sizeof(double2) * khat_elems_t<double>(g, E)));
+  MSC_TRY(dalloc(pl, pl->khat32, sizeof(float2) * khat_elems_t<float>(g, E)));
   MSC_TRY(dalloc(pl, pl->va_blocks, sizeof(double) * 26 * 81));
   const long long npts = (long long)g.Lz * g.Ly * g.Lx;
   // FP64 spatial kernel and its partial transforms; kept by the plan for the next frequency
@@ -308,20 +351,20 @@ int launch_g0(msc_plan* pl, double omega, const double* kpar, int va, int n_orde
   const double2* twxy = (const double2*)pl->tw64_xy.p;
   const double2* twz = (const double2*)pl->tw64_z.p;
   const long long plane = (long long)g.Ly * g.Lx, vol = (long long)g.Lz * plane;
-  // x pass (contiguous lines), in place
+  // x pass (contiguous lines), in place; keep kx < Hx
   int s = launch_fft_contig<double>(pl, K, K, (long long)E * g.Lz * g.Ly, (long long)E * g.Lz * g.Ly, 0, g.Lx, g.Lx,
-                                    g.Lx, pl->fxy, twxy, -1, nullptr);
-  // y pass: axis stride Lx, columns x, slabs (z, e); keep ky < Hy
+                                    g.Hx, pl->fxy, twxy, -1, nullptr);
+  // y pass: axis stride Lx, columns kx < Hx, slabs (z, e); keep ky < Hy
   if (s == MSC_OK)
-    s = launch_fft_strided<double>(pl, K, g.Lx, plane, vol, K, g.Lx, plane, vol, nullptr, g.Lx, g.Lz, E, g.Ly, g.Hy,
+    s = launch_fft_strided<double>(pl, K, g.Lx, plane, vol, K, g.Lx, plane, vol, nullptr, g.Hx, g.Lz, E, g.Ly, g.Hy,
                                    pl->fxy, twxy, -1, nullptr);
-  // z pass: axis stride Ly*Lx, columns kx, slabs (ky < Hy, e); written to khat[e][kz][ky][kx]
-  // in complex128 and complex64
-  const long long hplane = (long long)g.Hy * g.Lx;
+  // z pass: axis stride Ly*Lx, columns kx < Hx, slabs (ky < Hy, e); keep kz < Hz, in place
   if (s == MSC_OK)
-    s = launch_fft_strided<double>(pl, K, plane, g.Lx, vol, (double2*)pl->khat64.p, hplane, g.Lx,
-                                   (long long)g.Lz * hplane, (float2*)pl->khat32.p, g.Lx, g.Hy, E, g.Lz, g.Lz, pl->fz,
-                                   twz, -1, nullptr);
+    s = launch_fft_strided<double>(pl, K, plane, g.Lx, vol, K, plane, g.Lx, vol, nullptr, g.Hx, g.Hy, E, g.Lz, g.Hz,
+                                   pl->fz, twz, -1, nullptr);
+  // stored layouts of the fused z pass, complex128 and complex64
+  if (s == MSC_OK) s = launch_khat_pack<double>(pl, K, (double2*)pl->khat64.p, E);
+  if (s == MSC_OK) s = launch_khat_pack<float>(pl, K, (float2*)pl->khat32.p, E);
   return s;
 }
 

@@ -48,7 +48,7 @@ def _call(lib, name, plan, x, precision):
     return st, y
 
 
-@pytest.mark.parametrize("M,Nz,periodic", [(12, 3, False), (10, 4, True), (64, 16, False)])
+@pytest.mark.parametrize("M,Nz,periodic", [(12, 3, False), (10, 4, True), (64, 16, False), (96, 16, False)])
 @pytest.mark.parametrize("precision", [_native.MSC_COMPLEX64, _native.MSC_COMPLEX128])
 def test_noalloc_matches_matvec_twice(M, Nz, periodic, precision):
     lib = _native.load()
@@ -56,7 +56,8 @@ def test_noalloc_matches_matvec_twice(M, Nz, periodic, precision):
     dt = torch.complex128 if precision == _native.MSC_COMPLEX128 else torch.complex64
     rtol = 1e-10 if precision == _native.MSC_COMPLEX128 else 1e-5
     torch.manual_seed(M + Nz)
-    need = (16 if precision else 8) * (9 * np.prod(plan.fft_sizes()) + 18 * g.n_cubes)
+    Lz, Lx, Ly = plan.fft_sizes()
+    need = (16 if precision else 8) * (9 * Nz * Ly * Lx + 18 * g.n_cubes)  # workspace + two fields
     for _ in range(2):
         x = torch.randn(Nz, M, M, 9, dtype=dt, device=plan.device)
         st_ref, y_ref = _call(lib, "msc_matvec", plan, x, precision)
