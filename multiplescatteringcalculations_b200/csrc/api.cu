@@ -78,6 +78,13 @@ int bloch_modulate(msc_plan* pl, double2* v, int sign) {
   return MSC_OK;
 }
 
+// Smallest power of two >= n.
+static int pow2_at_least(int n) {
+  int L = 1;
+  while (L < n) L *= 2;
+  return L;
+}
+
 // Smallest FFT length >= n whose factors are 2, 3, 5, 7.
 static int nice_length(int n) {
   for (int L = std::max(n, 1);; ++L) {
@@ -143,7 +150,9 @@ int msc_plan_create(const msc_slab_desc* d, void* stream, msc_plan** out) {
   g.M = d->M;
   g.Nz = d->N_z;
   g.nsite = (int)nsite;
-  int Lz = d->Lz > 0 ? d->Lz : nice_length(2 * d->N_z - 1);
+  // z padding: a power of two (the z spectrum exists only in shared memory; power-of-two
+  // lengths use the compile-time FFT kernels and their pruned first and last stages)
+  int Lz = d->Lz > 0 ? d->Lz : pow2_at_least(2 * d->N_z - 1);
   if (Lz < 2 * d->N_z - 1) {
     delete pl;
     set_error("Lz=%d is below 2*N_z-1=%d", Lz, 2 * d->N_z - 1);

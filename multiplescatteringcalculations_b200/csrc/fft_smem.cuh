@@ -234,20 +234,23 @@ template <int L> struct Pow2Plan {
 };
 
 // Stage (R, NS) for line l, butterflies j0, j0 + JS, ...; element idx of line l at
-// idx * P + l.
-template <int R, int NS, int L, int DIR, int P, int JS, typename C>
+// idx * P + l. HIN (first stage only): inputs idx >= L/2 are zero and not read.
+// HOUT (last stage only): outputs idx >= L/2 are not needed and not computed.
+template <int R, int NS, int L, int DIR, int P, int JS, bool HIN, bool HOUT, typename C>
 __device__ __forceinline__ void fft_stage_ct(const C* __restrict__ src, C* __restrict__ dst, const C* __restrict__ tw,
                                              int l, int j0) {
   constexpr int NB = L / R;
   constexpr int TSTEP = L / (NS * R);
   constexpr int ITER = (NB + JS - 1) / JS;
+  static_assert(!HIN || NS == 1, "pruned inputs on the first stage");
+  static_assert(!HOUT || NS * R == L, "pruned outputs on the last stage");
 #pragma unroll
   for (int it = 0; it < ITER; ++it) {
     const int j = j0 + it * JS;
     if (NB % JS != 0 && j >= NB) break;
     C v[R];
 #pragma unroll
-    for (int r = 0; r < R; ++r) v[r] = src[(j + r * NB) * P + l];
+    for (int r = 0; r < R; ++r) v[r] = (HIN && r * NB >= L / 2) ? czero<C>() : src[(j + r * NB) * P + l];
     const int kk = j & (NS - 1);
     if (NS > 1) {
 #pragma unroll
@@ -260,30 +263,36 @@ __device__ __forceinline__ void fft_stage_ct(const C* __restrict__ src, C* __res
     Dft<R, DIR, C>::run(v);
     const int idxD = (j - kk) * R + kk;
 #pragma unroll
-    for (int r = 0; r < R; ++r) dst[(idxD + r * NS) * P + l] = v[r];
+    for (int r = 0; r < R; ++r)
+      if (!HOUT || r * NS < L / 2) dst[(idxD + r * NS) * P + l] = v[r];
   }
 }
 
-template <int S, int L, int DIR, int P, int JS, typename C>
+template <int S, int L, int DIR, int P, int JS, bool HIN, bool HOUT, typename C>
 __device__ __forceinline__ void fft_stages_ct(C* src, C* dst, const C* tw, int l, int j0, bool active) {
   using PL = Pow2Plan<L>;
   if constexpr (S < PL::NSTAGES) {
-    if (active) fft_stage_ct<PL::radix(S), PL::ns(S), L, DIR, P, JS>(src, dst, tw, l, j0);
+    constexpr bool hin = HIN && S == 0;
+    constexpr bool hout = HOUT && S == PL::NSTAGES - 1;
+    if (active) fft_stage_ct<PL::radix(S), PL::ns(S), L, DIR, P, JS, hin, hout>(src, dst, tw, l, j0);
     __syncthreads();
-    fft_stages_ct<S + 1, L, DIR, P, JS>(dst, src, tw, l, j0, active);
+    fft_stages_ct<S + 1, L, DIR, P, JS, HIN, HOUT>(dst, src, tw, l, j0, active);
   }
 }
 
 // Full transform of the NLINES lines of tile a (pitch P), b the second tile; the
 // block has NTHR threads. Returns the tile holding the result. Ends with a barrier.
-template <int L, int DIR, int P, int NLINES, int NTHR, typename C>
+// HIN: the inputs idx >= L/2 are zero (zero padding to L >= 2n); they need not be
+// set in the tile. HOUT: only the outputs idx < L/2 are used; the others are left
+// undefined.
+template <int L, int DIR, int P, int NLINES, int NTHR, bool HIN = false, bool HOUT = false, typename C>
 __device__ __forceinline__ C* fft_tile_ct(C* a, C* b, const C* tw, int tid) {
   constexpr int JS = NTHR / NLINES;
   static_assert(JS >= 1, "at least one thread per line");
   const bool active = tid < JS * NLINES;
   const int l = tid % NLINES;
   const int j0 = tid / NLINES;
-  fft_stages_ct<0, L, DIR, P, JS>(a, b, tw, l, j0, active);
+  fft_stages_ct<0, L, DIR, P, JS, HIN, HOUT>(a, b, tw, l, j0, active);
   return (Pow2Plan<L>::NSTAGES % 2 == 0) ? a : b;
 }
 

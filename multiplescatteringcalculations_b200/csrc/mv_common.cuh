@@ -59,10 +59,18 @@ constexpr int ZBZ_THREADS = 288;
 constexpr int ZBZ_MAX_LINES = 144;
 constexpr int ZBZ_SMEM_LIMIT = 227 * 1024 - 2048;  // opt-in maximum less the static tables
 
+// Stored kernel-spectrum entry of element type T (complex, 8 or 16 bytes).
+template <typename T> struct KEnt;
+template <> struct KEnt<float> { using type = float2; };
+template <> struct KEnt<double> { using type = double2; };
+template <typename T> using kent = typename KEnt<T>::type;
+__host__ __device__ inline float2 kent_pack(double2 v, float2*) { return make_float2((float)v.x, (float)v.y); }
+__host__ __device__ inline double2 kent_pack(double2 v, double2*) { return v; }
+
 struct ZbzLayout {
   int KX;       // kx per quadrant; 4 KX column slots per block, KX in {4, 2, 1}
   int NXC;      // kx chunks of the octant, ceil(Hx / KX)
-  int CS;       // elements of one block's spectrum slice [e][kz][j], a 16-byte multiple
+  int CS;       // entries of one block's spectrum slice [e][kz][j]
   int ksm;      // 1: the slice is staged in shared memory
   size_t smem;  // dynamic shared memory of a block
 };
@@ -74,7 +82,8 @@ struct ZbzLayout {
 // (e * Hz + kz) * KX + j, kx = xc * KX + j (zero beyond Hx).
 template <typename T> constexpr ZbzLayout zbz_layout(int Lz, int Hz, int Hx, int E, bool oct) {
   const size_t es = sizeof(cx<T>);
-  const int al = (int)(16 / es);
+  const size_t ek = sizeof(kent<T>);
+  const int al = (int)(16 / ek);  // slices start 16-byte aligned
   auto tiles = [&](int kx) { return es * ((size_t)Lz + 2 * (size_t)Lz * (36 * kx + 1)); };
   auto make = [&](int kx, int ksm) {
     ZbzLayout L{};
@@ -82,7 +91,7 @@ template <typename T> constexpr ZbzLayout zbz_layout(int Lz, int Hz, int Hx, int
     L.NXC = oct ? (Hx + kx - 1) / kx : 0;
     L.CS = oct ? (E * Hz * kx + al - 1) / al * al : 0;
     L.ksm = ksm;
-    L.smem = tiles(kx) + (ksm ? es * (size_t)L.CS : 0);
+    L.smem = tiles(kx) + (ksm ? ek * (size_t)L.CS : 0);
     return L;
   };
   const size_t two = (size_t)(ZBZ_SMEM_LIMIT / 2);
@@ -97,7 +106,7 @@ template <typename T> constexpr ZbzLayout zbz_layout(int Lz, int Hz, int Hx, int
 template <typename T> inline ZbzLayout zbz_layout(const Geo& g, int E) {
   return zbz_layout<T>(g.Lz, g.Hz, g.Hx, E, g.oct != 0);
 }
-// elements of the stored kernel spectrum of type T
+// entries (kent<T>) of the stored kernel spectrum of type T
 template <typename T> inline size_t khat_elems_t(const Geo& g, int E) {
   if (!g.oct) return (size_t)E * g.Hz * g.Hy * g.Hx;
   const ZbzLayout L = zbz_layout<T>(g, E);

@@ -15,8 +15,10 @@ __device__ __forceinline__ cx<T> tau_component(const cx<T>* __restrict__ x, cons
 }
 
 // Block (i-tile of TR rows, layer n, component c): tau rows along y into a tile
-// [y][row] (zero for y >= M), FFT along y, store W[c][n][ky][i0 + row].
-template <typename T, bool POW2>
+// [y][row] (zero for y >= M), FFT along y, store W[c][n][ky][i0 + row]. LC > 0:
+// compile-time power-of-two Ly = LC; a thread keeps y = tid % LC. PR (with LC):
+// M <= LC/2, the first FFT stage reads only y < LC/2.
+template <typename T, bool POW2, int LC, bool PR>
 __global__ void __launch_bounds__(256, 4) k_t0_fft_y(const cx<T>* __restrict__ x, const double* scale,
                                                      const cx<T>* __restrict__ t4, cx<T>* __restrict__ W, Geo g,
                                                      FftPlan1D pl, const cx<T>* __restrict__ twg, const int* done) {
@@ -24,31 +26,50 @@ __global__ void __launch_bounds__(256, 4) k_t0_fft_y(const cx<T>* __restrict__ x
   using C = cx<T>;
   constexpr int TR = Tile<T>::W;
   constexpr int P = TR + 1;
+  constexpr int NT = 256;
   extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int Ly = LC > 0 ? LC : g.Ly;
   C* tw = reinterpret_cast<C*>(smem_raw);
-  C* ta = tw + g.Ly;
-  C* tb = ta + (size_t)g.Ly * P;
-  const int tid = threadIdx.x, nthr = blockDim.x;
+  C* ta = tw + Ly;
+  C* tb = ta + (size_t)Ly * P;
+  const int tid = threadIdx.x;
   const int c = blockIdx.z, n = blockIdx.y, i0 = blockIdx.x * TR;
   const int nr = min(TR, g.M - i0);
   const T s = load_scale<T>(scale);
-  for (int t = tid; t < g.Ly; t += nthr) tw[t] = twg[t];
+  for (int t = tid; t < Ly; t += NT) tw[t] = twg[t];
+  const int base = (n * g.M + i0) * g.M;
+  const C* res;
   // rows r < nr hold tau; y >= M and rows >= nr are zero
-  {
-    QR w(tid, nthr, g.Ly);  // (row, y)
-    const int base = (n * g.M + i0) * g.M;
-    for (int it = tid; it < TR * g.Ly; it += nthr, w.next()) {
+  if constexpr (LC > 0) {
+    constexpr int QS = NT / LC;
+    const int y = tid % LC, q0 = tid / LC;
+    if (!PR || y < LC / 2) {
+#pragma unroll
+      for (int k = 0; k < (TR + QS - 1) / QS; ++k) {
+        const int q = q0 + k * QS;
+        if (QS > TR && q >= TR) break;
+        C v = czero<C>();
+        if (y < g.M && q < nr) v = s * tau_component<T>(x, t4, g.nsite, base + q * g.M + y, c);
+        ta[y * P + q] = v;
+      }
+    }
+    __syncthreads();
+    res = fft_tile_ct<LC, -1, P, TR, NT, PR, false>(ta, tb, tw, tid);
+  } else {
+    QR w(tid, NT, Ly);  // (row, y)
+    for (int it = tid; it < TR * Ly; it += NT, w.next()) {
       C v = czero<C>();
       if (w.r < g.M && w.q < nr) v = s * tau_component<T>(x, t4, g.nsite, base + w.q * g.M + w.r, c);
       ta[w.r * P + w.q] = v;
     }
+    __syncthreads();
+    res = fft_tile<-1, POW2>(ta, tb, P, TR, pl, tw, tid, NT);
   }
-  __syncthreads();
-  const C* res = fft_tile<-1, POW2>(ta, tb, P, TR, pl, tw, tid, nthr);
   C* Wl = W + ((size_t)(c * g.Nz + n) * g.Ly) * g.Lx + i0;
-  for (int it = tid; it < TR * g.Ly; it += nthr) {
-    const int r = it & (TR - 1), ky = it / TR;  // TR is a power of two
-    if (r < nr) Wl[(size_t)ky * g.Lx + r] = res[ky * P + r];
+  const int r = tid & (TR - 1);  // TR is a power of two dividing NT
+  if (r < nr) {
+#pragma unroll 4
+    for (int ky = tid / TR; ky < Ly; ky += NT / TR) Wl[(size_t)ky * g.Lx + r] = res[ky * P + r];
   }
 }
 
@@ -60,15 +81,25 @@ int launch_t0_fft_y(msc_plan* pl, const cx<T>* x, const double* scale, cx<T>* W,
   const int nthr = 256;
   const size_t sm = sizeof(cx<T>) * ((size_t)g.Ly + 2 * (size_t)g.Ly * (TR + 1));
   dim3 grid((unsigned)((g.M + TR - 1) / TR), (unsigned)g.Nz, 9);
-#define CALL(P2)                                                                                   \
-  {                                                                                                \
-    MSC_CUDA(prep_kernel((const void*)k_t0_fft_y<T, P2>));                                         \
-    k_t0_fft_y<T, P2><<<grid, nthr, sm, pl->stream>>>(x, scale, t4, W, g, pl->fxy, tw, done);      \
-    ::msc::note_launch();                                                                          \
+  const void* kern;
+  const bool pr = 2 * g.M <= g.Ly;
+#define LEN(LL) kern = pr ? (const void*)k_t0_fft_y<T, true, LL, true> : (const void*)k_t0_fft_y<T, true, LL, false>;
+  switch (g.Ly) {
+    case 16: LEN(16) break;
+    case 32: LEN(32) break;
+    case 64: LEN(64) break;
+    case 128: LEN(128) break;
+    case 256: LEN(256) break;
+    default:
+      kern = pl->fxy.pow2 ? (const void*)k_t0_fft_y<T, true, 0, false> : (const void*)k_t0_fft_y<T, false, 0, false>;
   }
-  MSC_POW2_DISPATCH(pl->fxy.pow2, CALL);
-#undef CALL
-  MSC_CUDA(cudaGetLastError());
+#undef LEN
+  MSC_CUDA(prep_kernel(kern));
+  Geo gg = g;
+  FftPlan1D ff = pl->fxy;
+  void* args[] = {(void*)&x, (void*)&scale, (void*)&t4, (void*)&W, (void*)&gg, (void*)&ff, (void*)&tw, (void*)&done};
+  MSC_CUDA(cudaLaunchKernel(kern, grid, dim3(nthr), args, sm, pl->stream));
+  ::msc::note_launch();
   return MSC_OK;
 }
 template int launch_t0_fft_y<float>(msc_plan*, const float2*, const double*, float2*, const float2*, const int*);

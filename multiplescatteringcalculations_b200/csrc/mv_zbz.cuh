@@ -35,68 +35,75 @@ template <typename C> __device__ __forceinline__ void reflect(C* v, int f) {
     }
 }
 
-// NP field vectors multiplied by one kernel block (entries from ld(e)), in place.
-// SYM (E = 45): entry e enumerates i <= j row-major and holds (K D)_ij with
-// D = diag(1 x6, 2 x3), symmetric for the point propagator; K_ij = (K D)_ij / D_j.
-// FULL (E = 81): K_ij row-major.
-template <bool SYM, int NP> struct BlockMul;
-
-template <int NP> struct BlockMul<true, NP> {
-  static constexpr int E = 45;
-  template <typename C, typename LD> static __device__ __forceinline__ void run(LD ld, C (*t)[9]) {
-    C acc[NP][9];
+// One field vector t multiplied by one kernel block, in place; ld(e) returns the
+// stored entry e. SYM (E = 45): entry e enumerates i <= j row-major and holds
+// (K D)_ij with D = diag(1 x6, 2 x3), symmetric for the point propagator;
+// K_ij = (K D)_ij / D_j. FULL (E = 81): K_ij row-major.
+//
+// complex128: plain complex FMAs.
+template <bool SYM, typename LD> __device__ __forceinline__ void block_mul(LD ld, double2* t) {
+  double2 acc[9];
 #pragma unroll
-    for (int p = 0; p < NP; ++p)
-#pragma unroll
-      for (int j = 0; j < 9; ++j) {
-        if (j >= 6) {
-          t[p][j].x *= 0.5f;
-          t[p][j].y *= 0.5f;
-        }
-        acc[p][j] = czero<C>();
-      }
-    int e = 0;
-#pragma unroll
-    for (int i = 0; i < 9; ++i) {
-#pragma unroll
-      for (int j = i; j < 9; ++j, ++e) {
-        const C m = ld(e);
-#pragma unroll
-        for (int p = 0; p < NP; ++p) {
-          fma_(acc[p][i], m, t[p][j]);
-          if (i != j) fma_(acc[p][j], m, t[p][i]);
-        }
-      }
+  for (int j = 0; j < 9; ++j) {
+    if (SYM && j >= 6) {
+      t[j].x *= 0.5;
+      t[j].y *= 0.5;
     }
-#pragma unroll
-    for (int p = 0; p < NP; ++p)
-#pragma unroll
-      for (int j = 0; j < 9; ++j) t[p][j] = acc[p][j];
+    acc[j] = czero<double2>();
   }
-};
-
-template <int NP> struct BlockMul<false, NP> {
-  static constexpr int E = 81;
-  template <typename C, typename LD> static __device__ __forceinline__ void run(LD ld, C (*t)[9]) {
-    C acc[NP][9];
-#pragma unroll
-    for (int p = 0; p < NP; ++p)
-#pragma unroll
-      for (int j = 0; j < 9; ++j) acc[p][j] = czero<C>();
+  if constexpr (SYM) {
+    int e = 0;
 #pragma unroll
     for (int i = 0; i < 9; ++i)
 #pragma unroll
-      for (int j = 0; j < 9; ++j) {
-        const C m = ld(i * 9 + j);
-#pragma unroll
-        for (int p = 0; p < NP; ++p) fma_(acc[p][i], m, t[p][j]);
+      for (int j = i; j < 9; ++j, ++e) {
+        const double2 m = ld(e);
+        fma_(acc[i], m, t[j]);
+        if (i != j) fma_(acc[j], m, t[i]);
       }
+  } else {
 #pragma unroll
-    for (int p = 0; p < NP; ++p)
+    for (int i = 0; i < 9; ++i)
 #pragma unroll
-      for (int j = 0; j < 9; ++j) t[p][j] = acc[p][j];
+      for (int j = 0; j < 9; ++j) fma_(acc[i], ld(i * 9 + j), t[j]);
   }
-};
+#pragma unroll
+  for (int j = 0; j < 9; ++j) t[j] = acc[j];
+}
+
+// complex64: m t = m.x (t.x, t.y) + m.y (-t.y, t.x), two paired FP32 FMAs per
+// complex FMA; (-t.y, t.x) is formed once per vector.
+template <bool SYM, typename LD> __device__ __forceinline__ void block_mul(LD ld, float2* t) {
+  float2 tr[9], acc[9];
+#pragma unroll
+  for (int j = 0; j < 9; ++j) {
+    if (SYM && j >= 6) t[j] = __fmul2_rn(t[j], make_float2(0.5f, 0.5f));
+    tr[j] = make_float2(-t[j].y, t[j].x);
+    acc[j] = make_float2(0.f, 0.f);
+  }
+  auto cfma = [&](float2& a, const float2& m, int j) {
+    a = __ffma2_rn(make_float2(m.x, m.x), t[j], a);
+    a = __ffma2_rn(make_float2(m.y, m.y), tr[j], a);
+  };
+  if constexpr (SYM) {
+    int e = 0;
+#pragma unroll
+    for (int i = 0; i < 9; ++i)
+#pragma unroll
+      for (int j = i; j < 9; ++j, ++e) {
+        const float2 m = ld(e);
+        cfma(acc[i], m, j);
+        if (i != j) cfma(acc[j], m, i);
+      }
+  } else {
+#pragma unroll
+    for (int i = 0; i < 9; ++i)
+#pragma unroll
+      for (int j = 0; j < 9; ++j) cfma(acc[i], ld(i * 9 + j), j);
+  }
+#pragma unroll
+  for (int j = 0; j < 9; ++j) t[j] = acc[j];
+}
 
 // Block (blockIdx.x = kx chunk, blockIdx.y = ky_o), ZBZ_THREADS threads. Lines of
 // the tile: line c * NC + s for component c and column slot s < NC = 4 KX; element
@@ -104,16 +111,18 @@ template <int NP> struct BlockMul<false, NP> {
 // staged)] [twiddles Lz] [tile a] [tile b]. All global reads are cp.async copies
 // issued together and awaited once.
 //
-// LC > 0: compile-time Lz = LC (a power of two) and KX = KXC; LC = 0: both from
-// the plan and the layout at run time. The block size is a multiple of NL and of
+// LC > 0: compile-time Lz = LC (a power of two, so N_z <= Lz/2: the forward
+// transform reads only kz < Lz/2 and the inverse computes only kz < Lz/2) and
+// KX = KXC; LC = 0: both from the plan and the layout at run time. The block size is a multiple of NL and of
 // 8 KX, so a thread keeps one line in the load and store loops and one slot in
 // the multiply.
 template <typename T, int LC, int KXC, bool SYM, bool OCT, bool POW2>
-__global__ void __launch_bounds__(ZBZ_THREADS, 2) k_zbz(cx<T>* __restrict__ W, const cx<T>* __restrict__ khat, Geo g,
+__global__ void __launch_bounds__(ZBZ_THREADS, 2) k_zbz(cx<T>* __restrict__ W, const kent<T>* __restrict__ khat, Geo g,
                                                         ZbzLayout lay, FftPlan1D pl, const cx<T>* __restrict__ twg,
                                                         const int* done) {
   if (done && *done) return;
   using C = cx<T>;
+  using KE = kent<T>;
   constexpr bool CT = LC > 0;
   constexpr int NT = ZBZ_THREADS;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -123,8 +132,8 @@ __global__ void __launch_bounds__(ZBZ_THREADS, 2) k_zbz(cx<T>* __restrict__ W, c
   const int NC = 4 * KX, NL = 9 * NC, P = NL + 1;
   const int Lz = CT ? LC : pl.L;
   const bool ksm = OCT && lay.ksm;
-  C* ks = reinterpret_cast<C*>(smem_raw);
-  C* tw = ks + (ksm ? lay.CS : 0);
+  KE* ks = reinterpret_cast<KE*>(smem_raw);
+  C* tw = reinterpret_cast<C*>(ks + (ksm ? lay.CS : 0));
   C* ta = tw + Lz;
   C* tb = ta + (size_t)Lz * P;
   const int tid = threadIdx.x;
@@ -132,9 +141,9 @@ __global__ void __launch_bounds__(ZBZ_THREADS, 2) k_zbz(cx<T>* __restrict__ W, c
   const long long cstride = (long long)g.Nz * plane;
   const int kyo = blockIdx.y;
   const int x0 = blockIdx.x * (OCT ? KX : NC);
-  const C* kblk = OCT ? khat + ((long long)kyo * lay.NXC + blockIdx.x) * lay.CS : khat;
+  const KE* kblk = OCT ? khat + ((long long)kyo * lay.NXC + blockIdx.x) * lay.CS : khat;
   if (ksm) {
-    const int n16 = (int)(lay.CS * sizeof(C) / 16);
+    const int n16 = (int)(lay.CS * sizeof(KE) / 16);
     for (int i = tid; i < n16; i += NT)
       cp_async16(reinterpret_cast<unsigned char*>(ks) + 16 * i, reinterpret_cast<const unsigned char*>(kblk) + 16 * i);
   }
@@ -165,8 +174,9 @@ __global__ void __launch_bounds__(ZBZ_THREADS, 2) k_zbz(cx<T>* __restrict__ W, c
   const int line = tid % NL, r0 = tid / NL, RS = NT / NL;
   const long long o = loff[line];
   {
-    const int nrow = (CT && LC % (NT / (36 * (CT ? KXC : 1))) == 0) ? LC / (NT / (36 * (CT ? KXC : 1)))
-                                                                  : (Lz - r0 + RS - 1) / RS;
+    // compile time: only rows kz < Lz/2 are read by the pruned first FFT stage (N_z <= Lz/2)
+    const int nrow = (CT && (LC / 2) % (NT / (36 * (CT ? KXC : 1))) == 0) ? (LC / 2) / (NT / (36 * (CT ? KXC : 1)))
+                                                                        : (Lz - r0 + RS - 1) / RS;
 #pragma unroll 4
     for (int k = 0; k < nrow; ++k) {
       const int kz = r0 + k * RS;
@@ -177,7 +187,7 @@ __global__ void __launch_bounds__(ZBZ_THREADS, 2) k_zbz(cx<T>* __restrict__ W, c
   cp_async_wait_all();
   __syncthreads();
   C* res;
-  if constexpr (CT) res = fft_tile_ct<LC, -1, 36 * KXC + 1, 36 * KXC, NT>(ta, tb, tw, tid);
+  if constexpr (CT) res = fft_tile_ct<LC, -1, 36 * KXC + 1, 36 * KXC, NT, true, false>(ta, tb, tw, tid);
   else res = fft_tile<-1, POW2>(ta, tb, P, NL, pl, tw, tid, NT);
   C* oth = (res == ta) ? tb : ta;
   if (OCT) {
@@ -195,20 +205,20 @@ __global__ void __launch_bounds__(ZBZ_THREADS, 2) k_zbz(cx<T>* __restrict__ W, c
         const int kz = side ? Lz - kp : kp;
         const int ko = kp * KX + j;
         C* ra = res + kz * P + s;
-        C t[1][9];
+        C t[9];
 #pragma unroll
-        for (int c = 0; c < 9; ++c) t[0][c] = ra[c * NC];
-        reflect(t[0], f0);
+        for (int c = 0; c < 9; ++c) t[c] = ra[c * NC];
+        reflect(t, f0);
         if (ksm) {
           auto ld = [&](int e) { return ks[e * estr + ko]; };
-          BlockMul<SYM, 1>::run(ld, t);
+          block_mul<SYM>(ld, t);
         } else {
           auto ld = [&](int e) { return __ldg(kblk + e * estr + ko); };
-          BlockMul<SYM, 1>::run(ld, t);
+          block_mul<SYM>(ld, t);
         }
-        reflect(t[0], f0);
+        reflect(t, f0);
 #pragma unroll
-        for (int c = 0; c < 9; ++c) ra[c * NC] = t[0][c];
+        for (int c = 0; c < 9; ++c) ra[c * NC] = t[c];
       }
     }
   } else {
@@ -217,20 +227,20 @@ __global__ void __launch_bounds__(ZBZ_THREADS, 2) k_zbz(cx<T>* __restrict__ W, c
     for (int it = tid; it < nitem; it += NT) {
       const int s = it % NC, kz = it / NC;
       if (loff[s] < 0) continue;
-      const C* kb = khat + ((long long)kz * g.Hy + kyo) * g.Hx + (x0 + s);
+      const KE* kb = khat + ((long long)kz * g.Hy + kyo) * g.Hx + (x0 + s);
       auto ld = [&](int e) { return __ldg(kb + (long long)e * estride); };
       C* ra = res + kz * P + s;
-      C t[1][9];
+      C t[9];
 #pragma unroll
-      for (int c = 0; c < 9; ++c) t[0][c] = ra[c * NC];
-      BlockMul<SYM, 1>::run(ld, t);
+      for (int c = 0; c < 9; ++c) t[c] = ra[c * NC];
+      block_mul<SYM>(ld, t);
 #pragma unroll
-      for (int c = 0; c < 9; ++c) ra[c * NC] = t[0][c];
+      for (int c = 0; c < 9; ++c) ra[c * NC] = t[c];
     }
   }
   __syncthreads();
   const C* out;
-  if constexpr (CT) out = fft_tile_ct<LC, +1, 36 * KXC + 1, 36 * KXC, NT>(res, oth, tw, tid);
+  if constexpr (CT) out = fft_tile_ct<LC, +1, 36 * KXC + 1, 36 * KXC, NT, false, true>(res, oth, tw, tid);
   else out = fft_tile<+1, POW2>(res, oth, P, NL, pl, tw, tid, NT);
   if (o >= 0) {
     const int nrow = (g.Nz - r0 + RS - 1) / RS;
@@ -248,7 +258,7 @@ template <typename T> constexpr int zbz_kx_ct(int L, int E) { return zbz_layout<
 template <typename T>
 int launch_zbz(msc_plan* pl, cx<T>* W, const int* done) {
   const Geo& g = pl->g;
-  const cx<T>* kh = (const cx<T>*)(sizeof(T) == 8 ? pl->khat64.p : pl->khat32.p);
+  const kent<T>* kh = (const kent<T>*)(sizeof(T) == 8 ? pl->khat64.p : pl->khat32.p);
   const cx<T>* tw = (const cx<T>*)(sizeof(T) == 8 ? pl->tw64_z.p : pl->tw32_z.p);
   const ZbzLayout lay = zbz_layout<T>(g, pl->E);
   if (lay.smem > (size_t)ZBZ_SMEM_LIMIT) {
@@ -259,7 +269,7 @@ int launch_zbz(msc_plan* pl, cx<T>* W, const int* done) {
   dim3 grid(g.oct ? (unsigned)lay.NXC : (unsigned)((g.Lx + 4 * lay.KX - 1) / (4 * lay.KX)),
             (unsigned)(g.oct ? g.Hy : g.Ly));
   const void* kern = nullptr;
-  // compile-time kernels: octant spectrum, Lz in {16, 32, 64}
+  // compile-time kernels: octant spectrum, Lz in {8, 16, 32, 64, 128}
 #define CT_CASE(LZ)                                                                                  \
   case LZ:                                                                                           \
     if (sym && lay.KX == zbz_kx_ct<T>(LZ, 45))                                                       \
@@ -268,9 +278,11 @@ int launch_zbz(msc_plan* pl, cx<T>* W, const int* done) {
       kern = (const void*)k_zbz<T, LZ, zbz_kx_ct<T>(LZ, 81), false, true, true>;                      \
     break;
   if (g.oct) switch (g.Lz) {
+      CT_CASE(8)
       CT_CASE(16)
       CT_CASE(32)
       CT_CASE(64)
+      CT_CASE(128)
       default: break;
     }
 #undef CT_CASE

@@ -265,11 +265,11 @@ int launch_fft_strided(msc_plan* pl, const cx<T>* in, long long es, long long S1
                        int n_out, const FftPlan1D& f, const cx<T>* tw, int dir, const int* done);
 
 // Copy the spectrum box kz < Hz, ky < Hy, kx < Hx of the transformed work array
-// K[e][z][y][x] into the stored layout of element type T: blocked slices of the
+// K[e][z][y][x] into the stored layout of element type T (entries kent<T>): blocked slices of the
 // fused z pass for an octant spectrum (zero in the padding and beyond Hx), plain
 // [e][kz][ky][kx] for a full one.
 template <typename T>
-__global__ void k_khat_pack(const double2* __restrict__ K, cx<T>* __restrict__ out, Geo g, int E, ZbzLayout lay,
+__global__ void k_khat_pack(const double2* __restrict__ K, kent<T>* __restrict__ out, Geo g, int E, ZbzLayout lay,
                             long long n) {
   const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
@@ -295,10 +295,10 @@ __global__ void k_khat_pack(const double2* __restrict__ K, cx<T>* __restrict__ o
     e = (int)(t / g.Hz);
   }
   const double2 v = ok ? K[(((long long)e * g.Lz + kz) * g.Ly + ky) * g.Lx + kx] : make_double2(0.0, 0.0);
-  out[i] = from_d<cx<T>>(v);
+  out[i] = kent_pack(v, (kent<T>*)nullptr);
 }
 
-template <typename T> static int launch_khat_pack(msc_plan* pl, const double2* K, cx<T>* out, int E) {
+template <typename T> static int launch_khat_pack(msc_plan* pl, const double2* K, kent<T>* out, int E) {
   const Geo& g = pl->g;
   const long long n = (long long)khat_elems_t<T>(g, E);
   k_khat_pack<T><<<ceil_div(n, 256), 256, 0, pl->stream>>>(K, out, g, E, zbz_layout<T>(g, E), n);

@@ -111,6 +111,57 @@ def test_matvec_random_sizes_vs_oracle(M, Nz, per, va):
     assert_allclose(got, want, rtol=1e-10, atol=1e-12 * np.abs(want).max())
 
 
+@pytest.mark.parametrize("M,Nz,per,va", [
+    (8, 4, 0, 0),     # Lz 8 (one pruned radix-8 stage), Lxy 15
+    (16, 8, 0, 0),    # Lz 16, Lxy 32 pruned
+    (16, 16, 1, 1),   # Lz 32 volume averaged, Lxy 16 periodic (unpruned)
+    (32, 5, 0, 1),    # Lz 16 volume averaged, Lxy 63 (radices 7, 3, 3)
+    (64, 2, 1, 0),    # Lxy 64 periodic, Lz 4
+    (20, 33, 0, 0),   # Lz 128 (one block per column set), Lxy 40
+    (24, 12, 0, 0),   # Lz 32, Lxy 48
+    (28, 6, 0, 0),    # Lz 16, Lxy 56
+])
+def test_matvec_compiled_lengths_vs_oracle(M, Nz, per, va):
+    """The compile-time FFT kernels (power-of-two lengths, pruned first and last
+    stages when the data fill at most half the padded line) in both precisions."""
+    rng = np.random.default_rng(M * 1000 + Nz)
+    g = SlabGeometry(M, Nz, 1.0)
+    mat = random_slab_material(g, REF, CONTRAST, 0.5, seed=M * 7 + Nz)
+    t4 = O.t0_scalars(OMEGA, 1.0, REF.alpha, REF.beta, REF.rho, mat.Dlambda, mat.Dmu, mat.Drho)
+    kh = O.build_slab_kernels(M, Nz, 1.0, OMEGA, REF.alpha, REF.beta, REF.rho, periodic=bool(per),
+                              volume_averaged=bool(va))
+    x = rng.standard_normal(Nz * M * M * 9) + 1j * rng.standard_normal(Nz * M * M * 9)
+    want = O.slab_matvec(x, t4, kh, M, Nz, periodic=bool(per))
+    plan = SlabPlan(g, REF, periodic=bool(per))
+    plan.build_t0(mat, OMEGA)
+    plan.build_g0(OMEGA, volume_averaged=bool(va))
+    xt = torch.from_numpy(x.reshape(Nz, M, M, 9))
+    got = plan.matvec(xt, "complex128").cpu().numpy().ravel()
+    assert _rel(got, want) < 1e-12
+    got32 = plan.matvec(xt, "complex64").cpu().numpy().ravel()
+    assert _rel(got32, want) < 1e-5
+
+
+def test_bloch_matvec_compiled_lengths_vs_oracle():
+    """Full (non-octant) spectrum with Lxy 16 periodic and Lz 16."""
+    M, Nz = 16, 8
+    g = SlabGeometry(M, Nz, 1.0)
+    mat = random_slab_material(g, REF, CONTRAST, 0.5, seed=11)
+    kpar = (0.011, 0.004)
+    t4 = O.t0_scalars(OMEGA, 1.0, REF.alpha, REF.beta, REF.rho, mat.Dlambda, mat.Dmu, mat.Drho)
+    kh = O.build_slab_kernels(M, Nz, 1.0, OMEGA, REF.alpha, REF.beta, REF.rho, periodic=True,
+                              phase_xy=(kpar[0] * 2.0, kpar[1] * 2.0))
+    rng = np.random.default_rng(3)
+    x = rng.standard_normal(Nz * M * M * 9) + 1j * rng.standard_normal(Nz * M * M * 9)
+    want = O.slab_matvec(x, t4, kh, M, Nz, periodic=True)
+    plan = SlabPlan(g, REF, periodic=True)
+    plan.build_t0(mat, OMEGA)
+    plan.build_g0(OMEGA, kpar=kpar)
+    xt = torch.from_numpy(x.reshape(Nz, M, M, 9))
+    assert _rel(plan.matvec(xt, "complex128").cpu().numpy().ravel(), want) < 1e-12
+    assert _rel(plan.matvec(xt, "complex64").cpu().numpy().ravel(), want) < 1e-5
+
+
 def test_matvec_identity_when_T_zero():
     g = SlabGeometry(5, 3, 1.0)
     zero = MaterialContrast(0.0, 0.0, 0.0)
