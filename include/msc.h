@@ -132,10 +132,15 @@ int msc_matvec_noalloc(msc_plan* plan, const void* x, void* y, int precision);
  * Non-convergence returns MSC_NOT_CONVERGED with x the best iterate. */
 int msc_solve(msc_plan* plan, const void* b, void* x, const msc_solve_opts* opts, msc_solve_stats* stats);
 
-/* Specular periodic R_PP (host out[2] = re, im) of psi (complex128, device).
- * bloch = 1 demodulates the sources by exp(-i k_par.x), k_par the plan's Bloch wavevector.
+/* Flags of msc_rpp_periodic. */
+#define MSC_RPP_BLOCH 1             /* demodulate the sources by exp(-i k_par.x), k_par the plan's Bloch wavevector */
+#define MSC_RPP_PLANE_WAVE_MOMENT 2 /* moment term with |k| = omega/alpha instead of the reference's kz
+                                       (the two agree at p = 0; see the reference formula below) */
+
+/* Specular periodic R_PP (host out[2] = re, im) of psi (complex128, device) at
+ * horizontal slowness p. flags = 0 is the reference formula.
  * Replaces slab_rpp_periodic (slab_scattering.py:672-735). */
-int msc_rpp_periodic(msc_plan* plan, const void* psi, double omega, double p, int bloch, double* out);
+int msc_rpp_periodic(msc_plan* plan, const void* psi, double omega, double p, int flags, double* out);
 
 /* Reflected far-field amplitudes (host out[6] = R_PP, R_PS, R_SP as re, im).
  * Replaces slab_reflected_field (slab_scattering.py:589-669). */

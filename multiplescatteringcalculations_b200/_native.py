@@ -24,6 +24,8 @@ MSC_ERR_NONFINITE = -6
 
 MSC_COMPLEX64 = 0
 MSC_COMPLEX128 = 1
+MSC_RPP_BLOCH = 1
+MSC_RPP_PLANE_WAVE_MOMENT = 2
 MSC_SOLVE_MIXED = 0
 MSC_SOLVE_FP64 = 1
 MSC_WAVE_P = 0

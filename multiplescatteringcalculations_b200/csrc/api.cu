@@ -312,9 +312,10 @@ int msc_solve(msc_plan* pl, const void* b, void* x, const msc_solve_opts* o, msc
   return solve(pl, (const double2*)b, (double2*)x, o, st);
 }
 
-int msc_rpp_periodic(msc_plan* pl, const void* psi, double omega, double p, int bloch, double* out) {
+int msc_rpp_periodic(msc_plan* pl, const void* psi, double omega, double p, int flags, double* out) {
   if (!pl || !psi || !out) { set_error("null argument"); return MSC_ERR_INVALID; }
-  return rpp_periodic(pl, (const double2*)psi, omega, p, bloch, out);
+  if (flags & ~(MSC_RPP_BLOCH | MSC_RPP_PLANE_WAVE_MOMENT)) { set_error("unknown R_PP flags %d", flags); return MSC_ERR_INVALID; }
+  return rpp_periodic(pl, (const double2*)psi, omega, p, flags, out);
 }
 
 int msc_reflected_field(msc_plan* pl, const void* psi, double omega, const double* k_hat, double* out) {

@@ -73,15 +73,18 @@ __global__ void __launch_bounds__(NT) k_layer_means(const double2* __restrict__ 
 }
 
 // R_PP = -i/(2 kz d^2 rho alpha^2) sum_l Q_l exp(i kz z_l),
-// Q_l = -rh.f - i kz rh.sigma.rh, rh = (-eta alpha, p alpha, 0), kz = omega eta.
+// Q_l = -rh.f - i km rh.sigma.rh, rh = (-eta alpha, p alpha, 0), kz = omega eta.
+// km = kz is the reference's moment factor; plane_wave = 1 takes km = omega/alpha,
+// the magnitude of the gradient of the reflected plane wave (equal at p = 0).
 __global__ void k_rpp_combine(const double2* __restrict__ means, int Nz, double a, double omega, double alpha,
-                              double rho, double p, double2* out) {
+                              double rho, double p, int plane_wave, double2* out) {
   if (threadIdx.x != 0) return;
   // eta = sqrt(1/alpha^2 - p^2) on the Im >= 0 (then Re >= 0) branch (kennett_layers.py:273-284)
   const double s = 1.0 / alpha;
   const double T = (s + p) * (s - p);
   double2 eta = T >= 0 ? make_double2(sqrt(T), 0.0) : make_double2(0.0, sqrt(-T));
   const double2 kz = make_double2(omega * eta.x, omega * eta.y);
+  const double2 km = plane_wave ? make_double2(omega / alpha, 0.0) : kz;
   const double2 rh0 = make_double2(-eta.x * alpha, -eta.y * alpha);
   const double rh1 = p * alpha;
   const double d = 2.0 * a;
@@ -93,7 +96,7 @@ __global__ void k_rpp_combine(const double2* __restrict__ means, int Nz, double 
     // rh.sigma.rh = rh0^2 s00 + 2 rh0 rh1 s01 + rh1^2 s11
     const double2 srr = rh0 * rh0 * s00 + 2.0 * rh1 * (rh0 * s01) + (rh1 * rh1) * s11;
     const double2 rf = rh0 * m[0] + rh1 * m[1];
-    const double2 q = make_double2(-rf.x, -rf.y) - mul_i<1>(kz * srr);
+    const double2 q = make_double2(-rf.x, -rf.y) - mul_i<1>(km * srr);
     const double zl = (l + 0.5) * d;
     const double2 ph = make_double2(-kz.y * zl, kz.x * zl);  // i kz z
     const double mag = exp(ph.x);
@@ -108,7 +111,8 @@ __global__ void k_rpp_combine(const double2* __restrict__ means, int Nz, double 
   *out = mul_i<-1>(inv) * tot;
 }
 
-int rpp_periodic(msc_plan* pl, const double2* psi, double omega, double p, int bloch, double* out) {
+int rpp_periodic(msc_plan* pl, const double2* psi, double omega, double p, int flags, double* out) {
+  const int bloch = flags & MSC_RPP_BLOCH;
   if (!pl->has_t0) {
     set_error("rpp_periodic needs build_t0 first");
     return MSC_ERR_STATE;
@@ -119,7 +123,8 @@ int rpp_periodic(msc_plan* pl, const double2* psi, double omega, double p, int b
   double2* res = means + (size_t)9 * g.Nz;
   k_layer_means<256><<<g.Nz, 256, 0, pl->stream>>>(psi, (const double2*)pl->t4_64.p, g.M, g.nsite, pl->desc.a,
                                                    bloch ? 1 : 0, pl->kpar[0], pl->kpar[1], means); ::msc::note_launch();
-  k_rpp_combine<<<1, 32, 0, pl->stream>>>(means, g.Nz, pl->desc.a, omega, pl->desc.alpha, pl->desc.rho, p, res); ::msc::note_launch();
+  k_rpp_combine<<<1, 32, 0, pl->stream>>>(means, g.Nz, pl->desc.a, omega, pl->desc.alpha, pl->desc.rho, p,
+                                  (flags & MSC_RPP_PLANE_WAVE_MOMENT) ? 1 : 0, res); ::msc::note_launch();
   MSC_CUDA(cudaGetLastError());
   double2 h;
   MSC_CUDA(cudaMemcpyAsync(&h, res, sizeof(double2), cudaMemcpyDeviceToHost, pl->stream));

@@ -110,7 +110,7 @@ int launch_matvec(msc_plan* pl, const cx<T>* x, const double* scale, cx<T>* y, c
 template <typename T>
 int launch_matvec_ws(msc_plan* pl, const cx<T>* x, const double* scale, cx<T>* y, cx<T>* W, const int* done);
 
-int rpp_periodic(msc_plan* pl, const double2* psi_ref, double omega, double p, int bloch, double* out);
+int rpp_periodic(msc_plan* pl, const double2* psi_ref, double omega, double p, int flags, double* out);
 int reflected_field(msc_plan* pl, const double2* psi_ref, double omega, const double* k_hat, double* out);
 int solve(msc_plan* pl, const double2* b_ref, double2* x_ref, const msc_solve_opts* o, msc_solve_stats* st);
 void gmres_free(msc_plan* pl);

@@ -294,10 +294,18 @@ class SlabPlan:
                  "residual": st.residual}
         return xx, stats
 
-    def rpp_periodic(self, psi: torch.Tensor, omega: float, p: float = 0.0, bloch: bool = False) -> complex:
+    def rpp_periodic(self, psi: torch.Tensor, omega: float, p: float = 0.0, bloch: bool = False,
+                     moment: str = "reference") -> complex:
+        """Specular R_PP at horizontal slowness p. ``moment="reference"`` is the
+        reference's formula (slab_scattering.py:672-735), whose strain-moment term
+        carries the vertical wavenumber kz; ``moment="plane_wave"`` uses |k| = omega/alpha,
+        the gradient of the reflected plane wave. The two agree at p = 0."""
+        if moment not in ("reference", "plane_wave"):
+            raise ValueError(f"moment must be 'reference' or 'plane_wave', got {moment!r}")
+        flags = (N.MSC_RPP_BLOCH if bloch else 0) | (N.MSC_RPP_PLANE_WAVE_MOMENT if moment == "plane_wave" else 0)
         pp = psi.to(device=self.device, dtype=torch.complex128).contiguous()
         out = (C.c_double * 2)()
-        N.check(self.lib.msc_rpp_periodic(self.handle, _ptr(pp), float(omega), float(p), int(bool(bloch)), out),
+        N.check(self.lib.msc_rpp_periodic(self.handle, _ptr(pp), float(omega), float(p), flags, out),
                 "msc_rpp_periodic")
         return complex(out[0], out[1])
 
@@ -478,14 +486,19 @@ def _observable_plan(result: SlabResult, T_local, device) -> SlabPlan:
     return plan
 
 
-def slab_rpp_periodic(result: SlabResult, T_local, *, p: float = 0.0, device=None) -> complex:
+def slab_rpp_periodic(result: SlabResult, T_local, *, p: float = 0.0, device=None,
+                      moment: str = "reference") -> complex:
     """Specular P->P reflection of a periodic slab by the Weyl sum (replaces
     ``slab_rpp_periodic``, slab_scattering.py:672-735). ``T_local`` is the
     (N_z, M, M, 9, 9) T-matrices or the (4, N_z, M, M) scalars. For a result
-    solved with ``bloch=True`` the sources are demodulated by the Bloch phase."""
+    solved with ``bloch=True`` the sources are demodulated by the Bloch phase.
+    ``moment="plane_wave"`` replaces the reference's kz in the strain-moment term by
+    omega/alpha (identical at p = 0; at oblique p it is the form that matches the
+    Kennett layer reflectivity)."""
     plan = _observable_plan(result, T_local, device)
     try:
-        return plan.rpp_periodic(torch.from_numpy(np.ascontiguousarray(result.psi)), result.omega, p, result.bloch)
+        return plan.rpp_periodic(torch.from_numpy(np.ascontiguousarray(result.psi)), result.omega, p, result.bloch,
+                                 moment)
     finally:
         plan.close()
 

@@ -704,10 +704,12 @@ def vertical_slowness(s, p):
     return eta
 
 
-def rpp_periodic(psi, T_local, M, N_z, a, omega, alpha, rho, p=0.0, demod=None):
+def rpp_periodic(psi, T_local, M, N_z, a, omega, alpha, rho, p=0.0, demod=None, moment="reference"):
     """Weyl-sum specular R_PP of a periodic slab (``slab_rpp_periodic``,
     slab_scattering.py:672-735). ``demod`` (addition of this build) multiplies
-    the sources by the Bloch demodulation before the lateral mean."""
+    the sources by the Bloch demodulation before the lateral mean.
+    ``moment="plane_wave"`` (addition of this build) puts omega/alpha instead of
+    the reference's kz in the strain-moment term; the two agree at p = 0."""
     if T_local.ndim == 4 and T_local.shape[0] == 4:
         src = apply_t0(T_local, psi)
     else:
@@ -723,7 +725,8 @@ def rpp_periodic(psi, T_local, M, N_z, a, omega, alpha, rho, p=0.0, demod=None):
     for l in range(N_z):
         f = np.mean(src[l, :, :, :3], axis=(0, 1))
         sig = _voigt_to_tensor(np.mean(src[l, :, :, 3:], axis=(0, 1)))
-        q = -np.dot(rh, f) - 1j * kz * np.dot(rh, sig @ rh)
+        km = omega / alpha if moment == "plane_wave" else kz
+        q = -np.dot(rh, f) - 1j * km * np.dot(rh, sig @ rh)
         tot += q * np.exp(1j * kz * z[l])
     return complex(-1j / (2.0 * kz * d**2 * rho * alpha**2) * tot)
 

@@ -287,6 +287,38 @@ def test_born_scaling():
     assert_allclose(np.abs(s2[m] / s1[m]), 2.0, rtol=0.02)
 
 
+@pytest.mark.parametrize("precision", ["mixed", "fp64"])
+def test_bloch_oblique_rpp_vs_kennett_and_oracle(golden, precision):
+    """Oblique P incidence (p = 1e-4 s/m, 30 degrees) on a uniform layer through the
+    Bloch-phased periodic solve: R_PP in both moment forms equals the oracle's, and
+    the plane-wave form is within 1% of the Kennett layer reflectivity."""
+    z = golden("kennett.npz")
+    ref = _medium(z)
+    om, a, M = float(z["omega"]), 1.0, 4
+    p = float(z["ps"][-1])
+    g = SlabGeometry(M, 1, a)
+    for ic in (0, 1):
+        dl, dm, dr = (np.full((1, M, M), v) for v in z["contrasts"][ic])
+        mat = SlabMaterial(dl, dm, dr, ref)
+        s = p * ref.alpha
+        kh = np.array([np.sqrt(1.0 - s * s), s, 0.0])
+        res = compute_slab_scattering_gpu(g, mat, om, kh, "P", gmres_tol=1e-11, periodic=True, bloch=True,
+                                          precision=precision)
+        phase = (om * p * 2.0 * a, 0.0)
+        ora = O.solve(M, 1, a, ref.alpha, ref.beta, ref.rho, dl, dm, dr, om, kh, "P", gmres_tol=1e-12,
+                      periodic=True, phase_xy=phase)
+        demod = O.bloch_demodulation(M, 1, a, phase)
+        for moment in ("reference", "plane_wave"):
+            got = slab_rpp_periodic(res, res.t0, p=p, moment=moment)
+            want = O.rpp_periodic(ora["psi"], ora["t4"], M, 1, a, om, ref.alpha, ref.rho, p=p, demod=demod,
+                                  moment=moment)
+            assert abs(got - want) <= 1e-7 * abs(want)
+        K = z[f"rpp_p_c{ic}_H2"][-1]
+        assert abs(slab_rpp_periodic(res, res.t0, p=p, moment="plane_wave") - K) < 0.01 * abs(K)
+    with pytest.raises(ValueError, match="moment"):
+        slab_rpp_periodic(res, res.t0, p=p, moment="bogus")
+
+
 def test_oblique_random_solve_vs_oracle():
     """Aperiodic oblique SV at ka 0.5 with +-20 % i.i.d. contrast: both precisions."""
     ref = ReferenceMedium(3000.0, 1732.0, 2500.0)
