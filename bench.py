@@ -192,7 +192,10 @@ def run_ours(args, wl, rank, world, local_rank):
         plan.build_t0(mat_dev, omega)
         plan.build_g0(omega)
         psi0 = plan.incident(omega, k_hat, wl["wave"])
-        x, st = plan.solve(psi0, tol=wl["tol"], max_iter=1000, restart=30, precision="mixed")
+        if args.precond != "none":
+            plan.set_nearfield()
+        x, st = plan.solve(psi0, tol=wl["tol"], max_iter=1000, restart=30, precision="mixed",
+                           preconditioner=None if args.precond == "none" else args.precond)
         stats.update(st)
         stats["rpp"] = plan.rpp_periodic(x, omega)
         return x
@@ -250,6 +253,27 @@ def run_ours(args, wl, rank, world, local_rank):
     torch.cuda.synchronize()
     ms64 = e0.elapsed_time(e1) / nrep64
 
+    # ---- the other mixed-precision variant (with / without the near-field preconditioner) ----
+    other = "nearfield" if args.precond == "none" else "none"
+
+    def step_other():
+        plan.build_t0(mat_dev, omega)
+        plan.build_g0(omega)
+        psi0 = plan.incident(omega, k_hat, wl["wave"])
+        if other != "none":
+            plan.set_nearfield()
+        return plan.solve(psi0, tol=wl["tol"], max_iter=1000, restart=30, precision="mixed",
+                          preconditioner=None if other == "none" else other)[1]
+
+    step_other()
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(nrep64):
+        st_o = step_other()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms_o = e0.elapsed_time(e1) / nrep64
+
     # ---- roofline of the complex64 matvec, timed live ----
     x32 = torch.randn(geom.N_z, geom.M, geom.M, 9, dtype=torch.complex64, device=dev)
     Lz, Lx, Ly = plan.fft_sizes()
@@ -290,9 +314,12 @@ def run_ours(args, wl, rank, world, local_rank):
         "config": {"workload": args.workload, **_cfg_desc(wl), "fft": [Lz, Lx, Ly]},
         "gpu_launches": int(launches),
         "solve": {"n_matvec": stats["n_matvec"], "n_matvec64": stats["n_matvec64"], "n_outer": stats["n_outer"],
+                  "n_precond": stats["n_precond"], "pc_fallback": stats["pc_fallback"], "precond": args.precond,
                   "residual": stats["residual"], "rpp": [stats["rpp"].real, stats["rpp"].imag]},
         "fp64": {"ms_per_solve": ms64, "n_matvec": st64["n_matvec"], "residual": st64["residual"],
                  "speedup_mixed_vs_fp64": ms64 / (ms_max / args.steps)},
+        f"mixed_precond_{other}": {"ms_per_solve": ms_o, "n_matvec": st_o["n_matvec"], "n_precond": st_o["n_precond"],
+                                   "residual": st_o["residual"]},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": traffic, "kernel": "complex64 matvec (5 launches + 2 layout transposes)",
                      "us_per_matvec": t_mv * 1e6, "alg_bytes": b_alg,
@@ -373,6 +400,8 @@ def main(argv=None) -> int:
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="cfg2", choices=sorted(WORKLOADS))
+    ap.add_argument("--precond", default="none", choices=["none", "nearfield"],
+                    help="right preconditioner of the timed mixed-precision solves")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--solve-only", action="store_true", help="timed solves only (for profiler launch lists)")

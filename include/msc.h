@@ -39,6 +39,7 @@ enum msc_status {
 enum msc_precision { MSC_COMPLEX64 = 0, MSC_COMPLEX128 = 1 };
 enum msc_solver_precision { MSC_SOLVE_MIXED = 0, MSC_SOLVE_FP64 = 1 };
 enum msc_wave { MSC_WAVE_P = 0, MSC_WAVE_S = 1 };
+enum msc_preconditioner { MSC_PC_NONE = 0, MSC_PC_NEARFIELD = 1 };
 
 typedef struct msc_slab_desc {
   int32_t M;         /* lateral cubes per side (SlabGeometry.M) */
@@ -60,6 +61,7 @@ typedef struct msc_solve_opts {
   int32_t initial_guess;  /* 0 = Born (x0 = psi0), 1 = zero */
   double inner_tol;       /* mixed precision: relative tolerance of each complex64 inner solve (0 = default) */
   int32_t ortho;          /* Arnoldi: 0 = default (mixed: CGS1, fp64: CGS2), 1 = CGS1, 2 = CGS2 */
+  int32_t preconditioner; /* msc_preconditioner: right preconditioner of flexible GMRES */
 } msc_solve_opts;
 
 typedef struct msc_solve_stats {
@@ -68,6 +70,8 @@ typedef struct msc_solve_stats {
   int32_t n_outer;       /* refinement sweeps (mixed) or restart cycles (fp64) */
   int32_t status;        /* msc_status of the solve */
   double residual;       /* true relative residual in FP64 (reference: gmres_residual) */
+  int32_t n_precond;     /* preconditioner applications */
+  int32_t pc_fallback;   /* 1: a preconditioned cycle failed to reduce the residual; plain GMRES finished */
 } msc_solve_stats;
 
 typedef struct msc_plan msc_plan;
@@ -124,6 +128,21 @@ int msc_matvec(msc_plan* plan, const void* x, void* y, int precision);
  * current, before any stream capture). All calls share the array: calls whose GPU
  * work overlaps race on it. No counterpart in the reference. */
 int msc_matvec_noalloc(msc_plan* plan, const void* x, void* y, int precision);
+
+/* Near-field polynomial preconditioner (an addition of this library; the reference
+ * solves unpreconditioned). S_l x = (G_nn + dG_l)(T0 x) with G_nn the 27 nearest-
+ * neighbour 9x9 blocks of the slab kernel (self term zero, zero outside the slab)
+ * and P = sum_{l=0..L} c_l S_l ... S_1. The default, degree 2 with c = 1, is the
+ * truncated Neumann series of (I - G_nn T0)^{-1}. msc_set_nearfield sets the degree
+ * L in [1, 6], the coefficients (2(L+1) doubles re/im, NULL = all ones) and
+ * per-layer block corrections (L x 27 x 81 complex128 re/im, NULL = none); the
+ * settings hold until changed and survive build_g0. */
+int msc_set_nearfield(msc_plan* plan, int degree, const double* coef, const double* dblocks);
+/* The 27 x 9 x 9 blocks G_nn (complex128 re/im into out[2 x 27 x 81]) of the last
+ * build_g0; offset o = ((dz+1) 3 + dx+1) 3 + dy+1, out block a,b: y_a += G_ab tau_b(v - o). */
+int msc_nearfield_blocks(const msc_plan* plan, double* out);
+/* z = P x, fields (N_z, M, M, 9) on the device in the precision given. */
+int msc_precondition(msc_plan* plan, const void* x, void* z, int precision);
 
 /* Solve (I - G0 T0) x = b; b, x complex128 (N_z, M, M, 9). Restarted GMRES with
  * CGS2 Arnoldi and FP64 Givens/least squares; precision MIXED runs complex64

@@ -26,6 +26,8 @@ MSC_COMPLEX64 = 0
 MSC_COMPLEX128 = 1
 MSC_RPP_BLOCH = 1
 MSC_RPP_PLANE_WAVE_MOMENT = 2
+MSC_PC_NONE = 0
+MSC_PC_NEARFIELD = 1
 MSC_SOLVE_MIXED = 0
 MSC_SOLVE_FP64 = 1
 MSC_WAVE_P = 0
@@ -55,6 +57,7 @@ class SolveOpts(C.Structure):
         ("initial_guess", C.c_int32),
         ("inner_tol", C.c_double),
         ("ortho", C.c_int32),
+        ("preconditioner", C.c_int32),
     ]
 
 
@@ -65,6 +68,8 @@ class SolveStats(C.Structure):
         ("n_outer", C.c_int32),
         ("status", C.c_int32),
         ("residual", C.c_double),
+        ("n_precond", C.c_int32),
+        ("pc_fallback", C.c_int32),
     ]
 
 
@@ -83,6 +88,9 @@ SIGNATURES = {
     "msc_matvec": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int]),
     "msc_matvec_noalloc": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int]),
     "msc_solve": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(SolveOpts), C.POINTER(SolveStats)]),
+    "msc_set_nearfield": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]),
+    "msc_nearfield_blocks": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "msc_precondition": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int]),
     "msc_rpp_periodic": (C.c_int, [C.c_void_p, C.c_void_p, C.c_double, C.c_double, C.c_int, C.c_void_p]),
     "msc_reflected_field": (C.c_int, [C.c_void_p, C.c_void_p, C.c_double, C.c_void_p, C.c_void_p]),
     "msc_status_string": (C.c_char_p, [C.c_int]),

@@ -5,6 +5,7 @@
 #include <cstring>
 
 #include "mv_common.cuh"
+#include "pc.cuh"
 
 namespace msc {
 
@@ -200,6 +201,13 @@ int msc_plan_destroy(msc_plan* pl) {
   if (pl->stream) cudaStreamSynchronize(pl->stream);
   else cudaDeviceSynchronize();
   gmres_free(pl);
+  if (pl->nf) {
+    dfree(pl, pl->nf->g64_dev);
+    dfree(pl, pl->nf->tmp32);
+    dfree(pl, pl->nf->tmp64);
+    delete pl->nf;
+    pl->nf = nullptr;
+  }
   DBuf* bufs[] = {&pl->tw64_z, &pl->tw64_xy, &pl->tw32_z, &pl->tw32_xy, &pl->t4_64, &pl->t4_32, &pl->khat64,
                   &pl->khat32, &pl->va_blocks, &pl->g0_scratch, &pl->W64, &pl->W32, &pl->f64a, &pl->f64b, &pl->f32a, &pl->f32b,
                   &pl->red, &pl->status};
@@ -292,6 +300,58 @@ int msc_matvec(msc_plan* pl, const void* x, void* y, int precision) {
     MSC_TRY((launch_ref_to_soa<float, float>(pl, (const float2*)x, (float2*)pl->f32a.p)));
     MSC_TRY(launch_matvec<float>(pl, (const float2*)pl->f32a.p, nullptr, (float2*)pl->f32b.p, nullptr));
     MSC_TRY((launch_soa_to_ref<float, float>(pl, (const float2*)pl->f32b.p, (float2*)y)));
+  } else {
+    set_error("precision must be 0 (complex64) or 1 (complex128)");
+    return MSC_ERR_INVALID;
+  }
+  return MSC_OK;
+}
+
+int msc_set_nearfield(msc_plan* pl, int degree, const double* coef, const double* dblocks) {
+  if (!pl) { set_error("null plan"); return MSC_ERR_INVALID; }
+  if (degree < 1 || degree > NF_MAXL) { set_error("degree must be in [1, %d], got %d", NF_MAXL, degree); return MSC_ERR_INVALID; }
+  if (!pl->nf) pl->nf = new NearField();
+  NearField* nf = pl->nf;
+  nf->L = degree;
+  for (int l = 0; l <= NF_MAXL; ++l)
+    nf->coef[l] = (coef && l <= degree) ? make_double2(coef[2 * l], coef[2 * l + 1]) : make_double2(1.0, 0.0);
+  if (dblocks) {
+    nf->dg.assign((size_t)degree * NF_OFFS * 81, make_double2(0, 0));
+    for (size_t i = 0; i < nf->dg.size(); ++i) nf->dg[i] = make_double2(dblocks[2 * i], dblocks[2 * i + 1]);
+  } else {
+    nf->dg.clear();
+  }
+  nf->dirty = true;
+  return MSC_OK;
+}
+
+int msc_nearfield_blocks(const msc_plan* pl, double* out) {
+  if (!pl || !out) { set_error("null argument"); return MSC_ERR_INVALID; }
+  if (!pl->nf || !pl->nf->ready) { set_error("the near-field blocks need build_g0 first"); return MSC_ERR_STATE; }
+  for (int i = 0; i < NF_OFFS * 81; ++i) {
+    out[2 * i] = pl->nf->g64[i].x;
+    out[2 * i + 1] = pl->nf->g64[i].y;
+  }
+  return MSC_OK;
+}
+
+int msc_precondition(msc_plan* pl, const void* x, void* z, int precision) {
+  if (!pl || !x || !z) { set_error("null argument"); return MSC_ERR_INVALID; }
+  if (x == z) { set_error("x and z may not alias"); return MSC_ERR_INVALID; }
+  if (!pl->has_t0) { set_error("the preconditioner needs build_t0 first"); return MSC_ERR_STATE; }
+  const size_t n = field_elems(pl->g);
+  if (precision == MSC_COMPLEX128) {
+    MSC_TRY(dalloc(pl, pl->f64a, sizeof(double2) * n));
+    MSC_TRY(dalloc(pl, pl->f64b, sizeof(double2) * n));
+    MSC_TRY((launch_ref_to_soa<double, double>(pl, (const double2*)x, (double2*)pl->f64a.p)));
+    MSC_TRY(nearfield_apply<double>(pl, (const double2*)pl->f64a.p, nullptr, (double2*)pl->f64b.p, nullptr));
+    MSC_TRY((launch_soa_to_ref<double, double>(pl, (const double2*)pl->f64b.p, (double2*)z)));
+  } else if (precision == MSC_COMPLEX64) {
+    MSC_TRY(dalloc(pl, pl->f32a, sizeof(float2) * n));
+    MSC_TRY(dalloc(pl, pl->f32b, sizeof(float2) * n));
+    MSC_TRY((launch_ref_to_soa<float, float>(pl, (const float2*)x, (float2*)pl->f32a.p)));
+    MSC_TRY(nearfield_apply<float>(pl, (const float2*)pl->f32a.p, nullptr, (float2*)pl->f32b.p, nullptr));
+    MSC_TRY((launch_soa_to_ref<float, float>(pl, (const float2*)pl->f32b.p, (float2*)z)));
   } else {
     set_error("precision must be 0 (complex64) or 1 (complex128)");
     return MSC_ERR_INVALID;

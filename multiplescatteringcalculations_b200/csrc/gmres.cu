@@ -17,6 +17,7 @@
 #include <cmath>
 #include <vector>
 
+#include "pc.cuh"
 #include "plan.cuh"
 
 namespace msc {
@@ -41,6 +42,7 @@ struct GmresWork {
   int m = 0;
   size_t n = 0;
   DBuf V32, V64;          // (m+1) x n Krylov basis
+  DBuf Z32, Z64;          // m x n preconditioned directions (flexible GMRES)
   DBuf x64, r64, ax64;    // FP64 iterate, residual, A x
   DBuf d32, r32;          // inner correction and right-hand side (complex64)
   DBuf state;             // GState
@@ -341,7 +343,15 @@ __global__ void k_givens(GState* st, HessPtr h, int m, int j) {
     const double aa = cabs_(a);
     double c;
     double2 s;
-    if (bb == 0.0) {
+    if (aa == 0.0 && bb == 0.0) {
+      // A v_j (or A P v_j) = 0: the column adds nothing; the cycle ends on the previous
+      // columns with the residual estimate unchanged
+      h.cs[j] = 1.0;
+      h.sn[j] = make_double2(0, 0);
+      st->res = cabs_(h.g[j]);
+      st->status = MSC_BREAKDOWN;
+      stop = 2;
+    } else if (bb == 0.0) {
       c = 1.0;
       s = make_double2(0, 0);
     } else if (aa == 0.0) {
@@ -355,6 +365,7 @@ __global__ void k_givens(GState* st, HessPtr h, int m, int j) {
       s = make_double2(ph.x * bb / r, ph.y * bb / r);  // (a/|a|) conj(b)/r with b real
       col[j] = make_double2(ph.x * r, ph.y * r);
     }
+    if (stop != 2) {
     col[j + 1] = make_double2(0, 0);
     h.cs[j] = c;
     h.sn[j] = s;
@@ -377,13 +388,14 @@ __global__ void k_givens(GState* st, HessPtr h, int m, int j) {
       end = true;
     }
     stop = end ? 1 : 0;
+    }
   }
   __syncthreads();
   for (int i = l; i <= j + 1; i += 32) Hc[i] = col[i];
   if (stop) {
     __syncthreads();
     if (l == 0) {
-      const int k = j + 1;
+      const int k = stop == 2 ? j : j + 1;
       st->k = k;
       for (int i = k - 1; i >= 0; --i) {
         double2 v = h.g[i];
@@ -399,14 +411,14 @@ __global__ void k_givens(GState* st, HessPtr h, int m, int j) {
   }
 }
 
-// x += sum_{i<k} y_i s_i V_i, with k from the state
+// x += sum_{i<k} y_i s_i V_i, with k from the state (s_i = 1 when scale is null)
 template <typename T, typename TX, int NV>
 __global__ void __launch_bounds__(NTH) k_update_x(cx<TX>* __restrict__ x, const cx<T>* __restrict__ V, size_t n,
                                                   const double* scale, const double2* y, const GState* st) {
   __shared__ double2 cf[NV];
   const int k = st->k;
   if (threadIdx.x < NV)
-    cf[threadIdx.x] = threadIdx.x < k ? scale[threadIdx.x] * y[threadIdx.x] : make_double2(0, 0);
+    cf[threadIdx.x] = threadIdx.x < k ? (scale ? scale[threadIdx.x] : 1.0) * y[threadIdx.x] : make_double2(0, 0);
   __syncthreads();
   if (k == 0) return;
   for (size_t e = (size_t)blockIdx.x * NTH + threadIdx.x; e < n; e += (size_t)gridDim.x * NTH) {
@@ -502,7 +514,7 @@ static int ensure_work(msc_plan* pl, int m) {
 void gmres_free(msc_plan* pl) {
   GmresWork* gw = pl->gw;
   if (!gw) return;
-  dfree(pl, gw->V32); dfree(pl, gw->V64); dfree(pl, gw->x64); dfree(pl, gw->r64); dfree(pl, gw->ax64);
+  dfree(pl, gw->V32); dfree(pl, gw->V64); dfree(pl, gw->Z32); dfree(pl, gw->Z64); dfree(pl, gw->x64); dfree(pl, gw->r64); dfree(pl, gw->ax64);
   dfree(pl, gw->d32); dfree(pl, gw->r32); dfree(pl, gw->state); dfree(pl, gw->hess); dfree(pl, gw->part);
   if (gw->hstate) cudaFreeHost(gw->hstate);
   for (auto& e : gw->ev)
@@ -514,14 +526,26 @@ void gmres_free(msc_plan* pl) {
 // One restarted GMRES(m) solve of A x = rhs in precision T (x in/out, same precision).
 // Stops when the residual estimate <= tol_abs or after max_mv operator applications.
 // Returns the number of matvecs used in *n_mv and the final estimate in *res.
+//
+// With `pc` the solve is flexible GMRES with the near-field preconditioner on the
+// right: z_j = P(v_j), w = A z_j, x += Z y. A cycle that leaves the residual
+// estimate above 0.99 of its initial value turns the preconditioner off for the
+// rest of the solve (*pc_off = 1): plain GMRES is the fallback.
 template <typename T>
 static int gmres_core(msc_plan* pl, int m, const cx<T>* rhs, cx<T>* x, bool x_zero, double tol_abs, int max_mv,
-                      int* n_mv, double* res, int* status, bool cgs2) {
+                      int* n_mv, double* res, int* status, bool cgs2, bool pc, int* n_pc, int* pc_off) {
   GmresWork* gw = pl->gw;
   GState* st = (GState*)gw->state.p;
   HessPtr h = hess_ptrs(gw);
   const size_t n = gw->n;
   cx<T>* V = (cx<T>*)(sizeof(T) == 8 ? gw->V64.p : gw->V32.p);
+  bool use_pc = pc;
+  cx<T>* Z = nullptr;
+  if (use_pc) {
+    DBuf& zb = sizeof(T) == 8 ? gw->Z64 : gw->Z32;
+    MSC_TRY(dalloc(pl, zb, sizeof(cx<T>) * (size_t)gw->m * n));
+    Z = (cx<T>*)zb.p;
+  }
   const int* done = &st->done;
   int used = 0;
   *status = MSC_NOT_CONVERGED;
@@ -548,8 +572,15 @@ static int gmres_core(msc_plan* pl, int m, const cx<T>* rhs, cx<T>* x, bool x_ze
     int pending = 0;  // index of the event holding the newest state
     for (int j = 0; j < m && !cycle_over; ++j) {
       if (used + 1 > max_mv) break;
-      // Arnoldi step j: w = A v_j into V[j+1]
-      MSC_TRY(launch_matvec<T>(pl, V + (size_t)j * n, h.scale + j, V + (size_t)(j + 1) * n, done));
+      // Arnoldi step j: w = A v_j (or A P v_j) into V[j+1]
+      if (use_pc) {
+        cx<T>* zj = Z + (size_t)j * n;
+        MSC_TRY(nearfield_apply<T>(pl, V + (size_t)j * n, h.scale + j, zj, done));
+        ++*n_pc;
+        MSC_TRY(launch_matvec<T>(pl, zj, nullptr, V + (size_t)(j + 1) * n, done));
+      } else {
+        MSC_TRY(launch_matvec<T>(pl, V + (size_t)j * n, h.scale + j, V + (size_t)(j + 1) * n, done));
+      }
       ++used;
       ++enq;
       cx<T>* w = V + (size_t)(j + 1) * n;
@@ -573,6 +604,7 @@ static int gmres_core(msc_plan* pl, int m, const cx<T>* rhs, cx<T>* x, bool x_ze
       if (gw->hstate[pending].done) {
         cycle_over = true;  // step j early-exits on the device
         --used;             // ... and applies no operator
+        if (use_pc) --*n_pc;
       }
       pending = slot;
     }
@@ -583,10 +615,12 @@ static int gmres_core(msc_plan* pl, int m, const cx<T>* rhs, cx<T>* x, bool x_ze
     MSC_CUDA(cudaStreamSynchronize(pl->stream));
     GState cur;
     MSC_CUDA(cudaMemcpy(&cur, st, sizeof(GState), cudaMemcpyDeviceToHost));
-    // x += V y (k columns)
+    // x += V y (k columns), or Z y with the preconditioner
     if (cur.k > 0) {
       const int nb = std::min<long long>(NB, ceil_div((long long)n, NTH));
-      k_update_x<T, T, 32><<<nb, NTH, 0, pl->stream>>>(x, V, n, h.scale, h.y, st); ::msc::note_launch();
+      if (use_pc) k_update_x<T, T, 32><<<nb, NTH, 0, pl->stream>>>(x, Z, n, nullptr, h.y, st);
+      else k_update_x<T, T, 32><<<nb, NTH, 0, pl->stream>>>(x, V, n, h.scale, h.y, st);
+      ::msc::note_launch();
       MSC_CUDA(cudaGetLastError());
     }
     *res = cur.res;
@@ -597,6 +631,13 @@ static int gmres_core(msc_plan* pl, int m, const cx<T>* rhs, cx<T>* x, bool x_ze
     if (cur.converged) {
       *status = MSC_OK;
       break;
+    }
+    // A preconditioned cycle that leaves the residual estimate above 0.99 of its
+    // start (a breakdown of A P included) turns the preconditioner off.
+    if (use_pc && cur.res > 0.99 * cur.beta) {
+      use_pc = false;
+      *pc_off = 1;
+      continue;
     }
     if (cur.status == MSC_BREAKDOWN) {
       *status = MSC_OK;
@@ -645,6 +686,15 @@ int solve(msc_plan* pl, const double2* b_ref, double2* x_ref, const msc_solve_op
   s.status = MSC_NOT_CONVERGED;
   const double tol = o->tol > 0 ? o->tol : 1e-6;
   const int max_mv = o->max_iter > 0 ? o->max_iter : 500;
+  if (o->preconditioner < 0 || o->preconditioner > 1) {
+    set_error("unknown preconditioner %d", o->preconditioner);
+    return MSC_ERR_INVALID;
+  }
+  const bool pc = o->preconditioner == MSC_PC_NEARFIELD;
+  if (pc && (!pl->nf || !pl->nf->ready)) {
+    set_error("the near-field preconditioner needs build_g0 first");
+    return MSC_ERR_STATE;
+  }
   if (bnorm == 0.0) {
     MSC_CUDA(cudaMemsetAsync(x, 0, sizeof(double2) * n, pl->stream));
     s.status = MSC_OK;
@@ -653,7 +703,7 @@ int solve(msc_plan* pl, const double2* b_ref, double2* x_ref, const msc_solve_op
     int used = 0, st = 0;
     double est = 0;
     MSC_TRY(gmres_core<double>(pl, m, b, x, o->initial_guess != 0, tol * bnorm, max_mv, &used, &est, &st,
-                               o->ortho != 1));
+                               o->ortho != 1, pc, &s.n_precond, &s.pc_fallback));
     s.n_matvec = used;
     s.n_matvec64 = used;
     s.status = st;
@@ -698,7 +748,8 @@ int solve(msc_plan* pl, const double2* b_ref, double2* x_ref, const msc_solve_op
       const double target = std::max(inner, 0.5 * tol / res);
       int iu = 0, ist = 0;
       double est = 0;
-      MSC_TRY(gmres_core<float>(pl, m, r32, d, true, target, max_mv - used, &iu, &est, &ist, o->ortho == 2));
+      MSC_TRY(gmres_core<float>(pl, m, r32, d, true, target, max_mv - used, &iu, &est, &ist, o->ortho == 2,
+                                pc && !s.pc_fallback, &s.n_precond, &s.pc_fallback));
       used += iu;
       ++outer;
       if (ist == MSC_ERR_NONFINITE) {

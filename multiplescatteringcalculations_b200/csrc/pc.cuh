@@ -1,0 +1,45 @@
+// Near-field preconditioner of the slab operator A = I - G0 T0.
+//
+// S x = G_nn (T0 x), G_nn the 27-point nearest-neighbour part of the spatial
+// kernel (offsets |dz|, |dx|, |dy| <= 1, self term zero), zero outside the slab.
+// The preconditioner is the polynomial P x = sum_l c_l S^l x, l = 0..L; the
+// truncated Neumann series of A^{-1} = sum (G0 T0)^l restricted to the near field
+// is c = (1, 1, ..., 1). A learned preconditioner sets the coefficients and adds
+// corrections to the stencil blocks of each layer (pc.cu).
+#pragma once
+#include "plan.cuh"
+
+namespace msc {
+
+constexpr int NF_OFFS = 27;   // stencil offsets, o = ((dz + 1) * 3 + dx + 1) * 3 + dy + 1
+constexpr int NF_MAXL = 6;    // polynomial degree limit
+
+// Stencil blocks of one layer in complex64: y_a(v) += g[o][a][b] tau_b(v - o).
+struct NFStencil32 {
+  float2 g[NF_OFFS * 81];
+};
+
+// Per-plan state of the preconditioner.
+struct NearField {
+  NearField() {
+    for (auto& c : coef) c = make_double2(1.0, 0.0);
+  }
+  bool ready = false;          // blocks extracted from the current G0
+  int L = 2;                   // degree
+  double2 coef[NF_MAXL + 1];   // c_0..c_L
+  std::vector<double2> g64;    // [27][9][9] physical near-field blocks (host copy)
+  std::vector<double2> dg;     // [L][27][9][9] learned block corrections (empty = none)
+  DBuf g64_dev;                // [L][27][81] complex128 blocks per layer (fp64 path)
+  std::vector<NFStencil32> s32;  // complex64 blocks per layer (kernel parameters)
+  DBuf tmp32, tmp64;           // two field-size work vectors per precision
+  bool dirty = true;           // layer blocks to rebuild from g64, dg
+};
+
+// Extract the near-field blocks from the spatial kernel of the G0 build (values
+// times `scale`).
+int nearfield_extract(msc_plan* pl, const double2* Ks_spatial, double scale);
+// z = P(s v), s = *scale (1 when null); `done` as in the matvec.
+template <typename T>
+int nearfield_apply(msc_plan* pl, const cx<T>* v, const double* scale, cx<T>* z, const int* done);
+
+}  // namespace msc

@@ -49,6 +49,7 @@ struct DBuf {
 };
 
 struct GmresWork;
+struct NearField;
 
 }  // namespace msc
 
@@ -84,6 +85,8 @@ struct msc_plan {
   msc::DBuf status;
   // GMRES workspace (lazily grown)
   msc::GmresWork* gw = nullptr;
+  // near-field preconditioner (blocks from the last G0 build, coefficients)
+  msc::NearField* nf = nullptr;
   int64_t bytes = 0;
 };
 

@@ -4,6 +4,7 @@
 
 #include "physics.cuh"
 #include "mv_common.cuh"
+#include "pc.cuh"
 #include "plan.cuh"
 
 namespace msc {
@@ -348,6 +349,8 @@ int launch_g0(msc_plan* pl, double omega, const double* kpar, int va, int n_orde
   k_g0_spatial<<<(unsigned)ceil_div(npts, 128), 128, 0, pl->stream>>>((double2*)ks.p, (const double*)pl->va_blocks.p, p); ::msc::note_launch();
   MSC_CUDA(cudaGetLastError());
   double2* K = (double2*)ks.p;
+  // near-field blocks for the preconditioner, before the transforms overwrite K
+  MSC_TRY(nearfield_extract(pl, K, p.scale));
   const double2* twxy = (const double2*)pl->tw64_xy.p;
   const double2* twz = (const double2*)pl->tw64_z.p;
   const long long plane = (long long)g.Ly * g.Lx, vol = (long long)g.Lz * plane;

@@ -276,10 +276,15 @@ class SlabPlan:
 
     def solve(self, b: torch.Tensor, *, tol: float, max_iter: int, restart: int = 30, precision: str = "mixed",
               initial_guess: str = "born", inner_tol: float = 0.0, x: torch.Tensor | None = None,
-              ortho: str = "auto"):
-        """Solve (I - G0 T0) x = b; returns (x, stats dict)."""
+              ortho: str = "auto", preconditioner: str | None = None):
+        """Solve (I - G0 T0) x = b; returns (x, stats dict). ``preconditioner="nearfield"``
+        runs flexible GMRES with the near-field polynomial on the right (the plan's
+        settings from ``set_nearfield``; plain GMRES takes over if it stalls)."""
         if precision not in ("mixed", "fp64"):
             raise ValueError(f"precision must be 'mixed' or 'fp64', got {precision!r}")
+        pcs = {None: N.MSC_PC_NONE, "none": N.MSC_PC_NONE, "nearfield": N.MSC_PC_NEARFIELD}
+        if preconditioner not in pcs:
+            raise ValueError(f"preconditioner must be None or 'nearfield', got {preconditioner!r}")
         bb = b.to(device=self.device, dtype=torch.complex128).contiguous()
         xx = torch.empty_like(bb) if x is None else x
         if ortho not in ("auto", "cgs1", "cgs2"):
@@ -287,12 +292,48 @@ class SlabPlan:
         opts = N.SolveOpts(float(tol), int(max_iter), int(restart),
                            N.MSC_SOLVE_MIXED if precision == "mixed" else N.MSC_SOLVE_FP64,
                            0 if initial_guess == "born" else 1, float(inner_tol),
-                           {"auto": 0, "cgs1": 1, "cgs2": 2}[ortho])
+                           {"auto": 0, "cgs1": 1, "cgs2": 2}[ortho], pcs[preconditioner])
         st = N.SolveStats()
         status = N.check(self.lib.msc_solve(self.handle, _ptr(bb), _ptr(xx), C.byref(opts), C.byref(st)), "msc_solve")
         stats = {"n_matvec": st.n_matvec, "n_matvec64": st.n_matvec64, "n_outer": st.n_outer, "status": status,
-                 "residual": st.residual}
+                 "residual": st.residual, "n_precond": st.n_precond, "pc_fallback": bool(st.pc_fallback)}
         return xx, stats
+
+    def set_nearfield(self, degree: int = 2, coef=None, dblocks=None) -> None:
+        """Near-field polynomial preconditioner P = sum_l c_l S_l ... S_1 with
+        S_l x = (G_nn + dG_l)(T0 x): ``coef`` (degree + 1 complex, default all ones:
+        the truncated Neumann series), ``dblocks`` (degree x 27 x 9 x 9 complex block
+        corrections, default none)."""
+        c = None
+        if coef is not None:
+            cc = np.asarray(coef, dtype=np.complex128).ravel()
+            if cc.size != degree + 1:
+                raise ValueError(f"coef needs {degree + 1} entries, got {cc.size}")
+            c = np.ascontiguousarray(np.stack([cc.real, cc.imag], -1).ravel())
+        d = None
+        if dblocks is not None:
+            dd = np.asarray(dblocks, dtype=np.complex128)
+            if dd.shape != (degree, 27, 9, 9):
+                raise ValueError(f"dblocks must have shape ({degree}, 27, 9, 9), got {dd.shape}")
+            d = np.ascontiguousarray(np.stack([dd.real, dd.imag], -1).ravel())
+        N.check(self.lib.msc_set_nearfield(self.handle, int(degree), None if c is None else c.ctypes.data,
+                                           None if d is None else d.ctypes.data), "msc_set_nearfield")
+
+    def nearfield_blocks(self) -> NDArray:
+        """The (27, 9, 9) near-field blocks G_nn of the last build_g0."""
+        out = np.empty(2 * 27 * 81)
+        N.check(self.lib.msc_nearfield_blocks(self.handle, out.ctypes.data), "msc_nearfield_blocks")
+        return (out[0::2] + 1j * out[1::2]).reshape(27, 9, 9)
+
+    def precondition(self, x: torch.Tensor, precision: str = "complex128") -> torch.Tensor:
+        """z = P x for a (N_z, M, M, 9) field."""
+        dt = torch.complex128 if precision == "complex128" else torch.complex64
+        xx = x.to(device=self.device, dtype=dt).contiguous()
+        z = torch.empty_like(xx)
+        N.check(self.lib.msc_precondition(self.handle, _ptr(xx), _ptr(z),
+                                          N.MSC_COMPLEX128 if dt == torch.complex128 else N.MSC_COMPLEX64),
+                "msc_precondition")
+        return z
 
     def rpp_periodic(self, psi: torch.Tensor, omega: float, p: float = 0.0, bloch: bool = False,
                      moment: str = "reference") -> complex:
@@ -426,14 +467,26 @@ def compute_slab_scattering_gpu(
     plan of the same geometry). ``dtype`` is accepted for compatibility
     (complex64 or complex128); the arithmetic is set by ``precision`` and the
     returned field is always complex128 with its FP64 true residual.
-    ``preconditioner`` must be None.
+    ``preconditioner``: None (plain GMRES), "nearfield" (flexible GMRES with the
+    near-field Neumann polynomial of the plan's settings), or a
+    ``NearFieldPreconditioner`` (its degree, coefficients and learned block
+    corrections); plain GMRES finishes the solve if a preconditioned cycle stalls.
     """
     if wave_type not in ("P", "S"):
         raise ValueError(f"wave_type must be 'P' or 'S', got '{wave_type}'")
     if dtype is not None and dtype not in (torch.complex64, torch.complex128):
         raise ValueError(f"dtype must be torch.complex64 or torch.complex128, got {dtype}")
+    pc_mode = None
     if preconditioner is not None:
-        raise ValueError("preconditioner must be None in this version")
+        if isinstance(preconditioner, str):
+            if preconditioner not in ("nearfield", "none"):
+                raise ValueError(f"preconditioner must be None, 'nearfield' or a NearFieldPreconditioner, "
+                                 f"got {preconditioner!r}")
+            pc_mode = None if preconditioner == "none" else "nearfield"
+        elif hasattr(preconditioner, "install"):
+            pc_mode = "nearfield"
+        else:
+            raise ValueError(f"unsupported preconditioner {preconditioner!r}")
     if bloch and not periodic:
         raise ValueError("bloch=True needs periodic=True")
     if plan is None:
@@ -444,8 +497,13 @@ def compute_slab_scattering_gpu(
     plan.build_t0(material, omega)
     plan.build_g0(omega, kpar=kp, volume_averaged=volume_averaged, n_orders=n_orders)
     psi0 = plan.incident(omega, k_hat, wave_type)
+    if pc_mode is not None:
+        if hasattr(preconditioner, "install"):
+            preconditioner.install(plan)
+        else:
+            plan.set_nearfield()
     x, st = plan.solve(psi0, tol=gmres_tol, max_iter=max_iter, restart=restart, precision=precision,
-                       initial_guess=initial_guess, inner_tol=inner_tol, ortho=ortho)
+                       initial_guess=initial_guess, inner_tol=inner_tol, ortho=ortho, preconditioner=pc_mode)
     if st["residual"] > gmres_tol:
         warnings.warn(
             f"GPU GMRES did not converge: rel_res={st['residual']:.2e} after {st['n_matvec']} matvecs",

@@ -767,3 +767,48 @@ def reflected_field(psi, T_local, M, N_z, a, omega, alpha, beta, rho, k_hat):
         sv = np.cross(cross, rh)
         sv = sv / np.linalg.norm(sv)
     return R_PP, complex(np.dot(sv, uS)), R_PP
+
+
+# ---------------------------------------------------------------------------
+# 9. Near-field polynomial preconditioner (an addition of this build; the
+#    reference solves without a preconditioner)
+# ---------------------------------------------------------------------------
+
+
+def nearfield_blocks(M, N_z, a, omega, alpha, beta, rho, *, volume_averaged=False, n_orders=2):
+    """The 27 nearest-neighbour 9x9 blocks of the slab kernel, index
+    o = ((dz+1)*3 + dx+1)*3 + dy+1, zero at the self term and for offsets the
+    lattice does not have (N_z = 1 or M = 1)."""
+    ker = slab_kernel_spatial(M, N_z, a, omega, alpha, beta, rho, volume_averaged=volume_averaged,
+                              n_orders=n_orders)
+    out = np.zeros((27, 9, 9), dtype=complex)
+    for o in range(27):
+        dz, dx, dy = o // 9 - 1, (o // 3) % 3 - 1, o % 3 - 1
+        if abs(dz) < N_z and abs(dx) < M and abs(dy) < M:
+            out[o] = ker[dz + N_z - 1, dx + M - 1, dy + M - 1]
+    return out
+
+
+def nearfield_stencil(x, t4, blocks, M, N_z):
+    """y(v) = sum_o G_o (T0 x)(v - o) over the 27 offsets (the self block included:
+    zero for the kernel, a pointwise block for a corrected layer), zero outside the
+    slab; x flat (N_z, M, M, 9)."""
+    tau = apply_t0(t4, x.reshape(N_z, M, M, 9))
+    tp = np.zeros((N_z + 2, M + 2, M + 2, 9), dtype=complex)
+    tp[1:-1, 1:-1, 1:-1] = tau
+    y = np.zeros((N_z, M, M, 9), dtype=complex)
+    for o in range(27):
+        dz, dx, dy = o // 9 - 1, (o // 3) % 3 - 1, o % 3 - 1
+        y += tp[1 - dz:1 - dz + N_z, 1 - dx:1 - dx + M, 1 - dy:1 - dy + M] @ blocks[o].T
+    return y.ravel()
+
+
+def nearfield_precondition(x, t4, blocks, M, N_z, coef=(1, 1, 1), dblocks=None):
+    """P x = sum_l c_l h_l, h_0 = x, h_l = (G_nn + dG_l) T0 h_{l-1}."""
+    h = np.asarray(x, dtype=complex).ravel()
+    out = coef[0] * h
+    for l in range(1, len(coef)):
+        b = blocks if dblocks is None else blocks + dblocks[l - 1]
+        h = nearfield_stencil(h, t4, b, M, N_z)
+        out = out + coef[l] * h
+    return out

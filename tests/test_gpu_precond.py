@@ -1,0 +1,120 @@
+"""Near-field polynomial preconditioner and flexible GMRES on the GPU (through the
+C-ABI), against the oracle's restatement (oracle/slab_oracle.py, section 9).
+
+The preconditioner is an addition of this library (the reference solves without
+one); it is judged by the oracle's stencil on the same inputs and by the FP64
+true residual of the preconditioned solve.
+"""
+
+import numpy as np
+import pytest
+import torch
+
+from oracle import slab_oracle as O
+
+pytestmark = pytest.mark.gpu
+
+if not torch.cuda.is_available():  # pragma: no cover
+    pytest.skip("needs a CUDA device", allow_module_level=True)
+
+from multiplescatteringcalculations_b200 import (  # noqa: E402
+    MaterialContrast,
+    ReferenceMedium,
+    SlabGeometry,
+    SlabPlan,
+    compute_slab_scattering_gpu,
+    gaussian_random_field_material,
+    random_slab_material,
+)
+
+REF = ReferenceMedium(3000.0, 1732.0, 2500.0)
+
+
+def _rel(a, b):
+    return np.linalg.norm(np.asarray(a) - np.asarray(b)) / np.linalg.norm(np.asarray(b))
+
+
+def _grf_problem(seed, M=16, Nz=8):
+    """GRF slab with (correlation length, std, ka, angle, wave) drawn from the seed,
+    the distribution of the learned-preconditioner workload at a smaller size."""
+    r = np.random.default_rng(seed)
+    ell, std, ka = r.uniform(2, 6), r.uniform(0.1, 0.3), r.uniform(0.3, 1.0)
+    g = SlabGeometry(M, Nz, 1.0)
+    mat = gaussian_random_field_material(g, REF, correlation_length=ell, std=std, seed=seed)
+    th = r.uniform(0, np.deg2rad(40))
+    kh = np.array([np.cos(th), np.sin(th), 0.0])
+    wave = "P" if r.random() < 0.5 else "S"
+    return g, mat, ka * REF.beta, kh, wave
+
+
+@pytest.mark.parametrize("va", [False, True])
+def test_nearfield_blocks_match_oracle(va):
+    M, Nz, om = 5, 3, 500.0
+    g = SlabGeometry(M, Nz, 1.0)
+    plan = SlabPlan(g, REF)
+    plan.build_t0(random_slab_material(g, REF, MaterialContrast(1e9, 5e8, 100.0), 0.5, seed=1), om)
+    plan.build_g0(om, volume_averaged=va)
+    want = O.nearfield_blocks(M, Nz, 1.0, om, REF.alpha, REF.beta, REF.rho, volume_averaged=va)
+    assert _rel(plan.nearfield_blocks(), want) < 1e-13
+
+
+@pytest.mark.parametrize("M,Nz", [(16, 8), (7, 5), (33, 2)])
+def test_precondition_matches_oracle(M, Nz):
+    om = 0.7 * REF.beta
+    g = SlabGeometry(M, Nz, 1.0)
+    mat = random_slab_material(g, REF, MaterialContrast(2e9, 1e9, 300.0), 0.5, seed=M + Nz)
+    plan = SlabPlan(g, REF)
+    plan.build_t0(mat, om)
+    plan.build_g0(om)
+    t4 = O.t0_scalars(om, 1.0, REF.alpha, REF.beta, REF.rho, mat.Dlambda, mat.Dmu, mat.Drho)
+    blocks = O.nearfield_blocks(M, Nz, 1.0, om, REF.alpha, REF.beta, REF.rho)
+    rng = np.random.default_rng(0)
+    x = rng.standard_normal(Nz * M * M * 9) + 1j * rng.standard_normal(Nz * M * M * 9)
+    xt = torch.from_numpy(x.reshape(Nz, M, M, 9))
+    # default: degree 2, coefficients 1 (truncated Neumann series)
+    want = O.nearfield_precondition(x, t4, blocks, M, Nz)
+    assert _rel(plan.precondition(xt).cpu().numpy().ravel(), want) < 1e-12
+    assert _rel(plan.precondition(xt, "complex64").cpu().numpy().ravel(), want) < 1e-5
+    # degree 3 with coefficients and block corrections
+    coef = np.array([1.0, 0.8 + 0.1j, 0.5 - 0.2j, 0.1j])
+    dbl = (rng.standard_normal((3, 27, 9, 9)) + 1j * rng.standard_normal((3, 27, 9, 9))) * 0.1 * np.abs(blocks).max()
+    plan.set_nearfield(3, coef, dbl)
+    want = O.nearfield_precondition(x, t4, blocks, M, Nz, coef, dbl)
+    assert _rel(plan.precondition(xt).cpu().numpy().ravel(), want) < 1e-12
+    assert _rel(plan.precondition(xt, "complex64").cpu().numpy().ravel(), want) < 1e-5
+    with pytest.raises(ValueError):
+        plan.set_nearfield(7)
+
+
+@pytest.mark.parametrize("precision", ["mixed", "fp64"])
+def test_fgmres_nearfield_on_a_hard_slab(precision):
+    """A strongly scattering GRF slab on which plain GMRES(30) needs hundreds of
+    matvecs: the near-field preconditioned solve reaches the same tolerance with
+    several times fewer operator applications and the same field."""
+    g, mat, om, kh, wave = _grf_problem(124)
+    plain = compute_slab_scattering_gpu(g, mat, om, kh, wave, gmres_tol=1e-8, max_iter=3000, precision=precision)
+    pc = compute_slab_scattering_gpu(g, mat, om, kh, wave, gmres_tol=1e-8, max_iter=3000, precision=precision,
+                                     preconditioner="nearfield")
+    assert plain.gmres_residual < 1e-8 and pc.gmres_residual < 1e-8
+    assert not pc.stats["pc_fallback"]
+    assert pc.stats["n_precond"] > 0
+    assert pc.n_gmres_iter * 2.5 < plain.n_gmres_iter
+    assert _rel(pc.psi, plain.psi) < 1e-6
+
+
+def test_fgmres_falls_back_to_plain_gmres():
+    """A preconditioner that maps everything to zero cannot reduce the residual: the
+    first cycle stalls, plain GMRES finishes the solve."""
+    g, mat, om, kh, wave = _grf_problem(125)
+    plan = SlabPlan(g, REF)
+    plan.build_t0(mat, om)
+    plan.build_g0(om)
+    psi0 = plan.incident(om, kh, wave)
+    plan.set_nearfield(1, [0.0, 0.0])
+    x, st = plan.solve(psi0, tol=1e-8, max_iter=2000, preconditioner="nearfield")
+    assert st["pc_fallback"]
+    assert st["residual"] < 1e-8
+    ref, st0 = plan.solve(psi0, tol=1e-8, max_iter=2000)
+    assert _rel(x.cpu().numpy(), ref.cpu().numpy()) < 1e-6
+    with pytest.raises(ValueError):
+        plan.solve(psi0, tol=1e-8, max_iter=10, preconditioner="bogus")
