@@ -21,27 +21,38 @@ void set_error(const char* fmt, ...) {
   va_end(ap);
 }
 
+// Plan buffers come from the stream-ordered allocator on the plan's stream: an
+// allocation or a release never synchronises the device, so plans on different
+// streams (the batch workers) build and solve concurrently. A reallocation bumps
+// the plan's generation, which invalidates its captured solver graphs.
 int dalloc(msc_plan* pl, DBuf& b, size_t bytes) {
   if (b.p && b.bytes >= bytes) return MSC_OK;
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(pl->stream, &cs) == cudaSuccess && cs != cudaStreamCaptureStatusNone) {
+    set_error("internal: device allocation while a solver cycle is being captured");
+    return MSC_ERR_STATE;
+  }
   if (b.p) dfree(pl, b);
   if (bytes == 0) bytes = 16;
   void* p = nullptr;
-  cudaError_t e = cudaMalloc(&p, bytes);
+  cudaError_t e = cudaMallocAsync(&p, bytes, pl->stream);
   if (e != cudaSuccess) {
     cudaGetLastError();
-    set_error("cudaMalloc of %zu bytes failed: %s", bytes, cudaGetErrorString(e));
+    set_error("cudaMallocAsync of %zu bytes failed: %s", bytes, cudaGetErrorString(e));
     return MSC_ERR_NOMEM;
   }
   b.p = p;
   b.bytes = bytes;
   pl->bytes += (int64_t)bytes;
+  ++pl->gen;
   return MSC_OK;
 }
 
 void dfree(msc_plan* pl, DBuf& b) {
   if (b.p) {
-    cudaFree(b.p);
+    cudaFreeAsync(b.p, pl->stream);
     pl->bytes -= (int64_t)b.bytes;
+    ++pl->gen;
   }
   b.p = nullptr;
   b.bytes = 0;
@@ -145,7 +156,7 @@ int msc_plan_create(const msc_slab_desc* d, void* stream, msc_plan** out) {
   }
   msc_plan* pl = new msc_plan();
   pl->desc = *d;
-  pl->stream = (cudaStream_t)stream;
+  pl->user = (cudaStream_t)stream;
   cudaGetDevice(&pl->device);
   Geo& g = pl->g;
   g.M = d->M;
@@ -183,12 +194,24 @@ int msc_plan_create(const msc_slab_desc* d, void* stream, msc_plan** out) {
     set_error("Lz=%d exceeds the shared memory of the fused z pass (Lz <= 192, N_z <= 96)", Lz);
     return MSC_ERR_UNSUPPORTED;
   }
+  if (cudaStreamCreateWithFlags(&pl->stream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreateWithFlags(&pl->ev_in, cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreateWithFlags(&pl->ev_out, cudaEventDisableTiming) != cudaSuccess) {
+    cudaGetLastError();
+    if (pl->stream) cudaStreamDestroy(pl->stream);
+    if (pl->ev_in) cudaEventDestroy(pl->ev_in);
+    delete pl;
+    set_error("could not create the plan's stream");
+    return MSC_ERR_CUDA;
+  }
+  StreamFence fence(pl);
   int s = build_twiddles(pl);
   if (s == MSC_OK) s = dalloc(pl, pl->status, 64);
   if (s == MSC_OK && cudaMemsetAsync(pl->status.p, 0, 64, pl->stream) != cudaSuccess) s = MSC_ERR_CUDA;
   if (s == MSC_OK) s = dalloc(pl, pl->W64, sizeof(double2) * ws_elems(g));
   if (s == MSC_OK) s = dalloc(pl, pl->W32, sizeof(float2) * ws_elems(g));
   if (s != MSC_OK) {
+    fence.pl = nullptr;
     msc_plan_destroy(pl);
     return s;
   }
@@ -212,13 +235,18 @@ int msc_plan_destroy(msc_plan* pl) {
                   &pl->khat32, &pl->va_blocks, &pl->g0_scratch, &pl->W64, &pl->W32, &pl->f64a, &pl->f64b, &pl->f32a, &pl->f32b,
                   &pl->red, &pl->status};
   for (DBuf* b : bufs) dfree(pl, *b);
+  cudaStreamSynchronize(pl->stream);
+  if (pl->ev_in) cudaEventDestroy(pl->ev_in);
+  if (pl->ev_out) cudaEventDestroy(pl->ev_out);
+  if (pl->stream) cudaStreamDestroy(pl->stream);
   delete pl;
   return MSC_OK;
 }
 
 int msc_plan_set_stream(msc_plan* pl, void* stream) {
   if (!pl) { set_error("null plan"); return MSC_ERR_INVALID; }
-  pl->stream = (cudaStream_t)stream;
+  // the plan's own stream stays; later calls are ordered after `stream`
+  pl->user = (cudaStream_t)stream;
   return MSC_OK;
 }
 
@@ -233,6 +261,7 @@ int msc_plan_fft_sizes(const msc_plan* pl, int32_t* o) {
 int64_t msc_plan_device_bytes(const msc_plan* pl) { return pl ? pl->bytes : 0; }
 
 int msc_build_t0(msc_plan* pl, const double* dlam, const double* dmu, const double* drho, double omega) {
+  StreamFence fence(pl);
   if (!pl || !dlam || !dmu || !drho) { set_error("null argument"); return MSC_ERR_INVALID; }
   if (!(omega > 0)) { set_error("omega must be > 0, got %g", omega); return MSC_ERR_INVALID; }
   MSC_TRY(launch_t0(pl, dlam, dmu, drho, omega));
@@ -242,6 +271,7 @@ int msc_build_t0(msc_plan* pl, const double* dlam, const double* dmu, const doub
 }
 
 int msc_t0_scalars(const msc_plan* pl, void* out) {
+  StreamFence fence(const_cast<msc_plan*>(pl));
   if (!pl || !out) { set_error("null argument"); return MSC_ERR_INVALID; }
   if (!pl->has_t0) { set_error("build_t0 first"); return MSC_ERR_STATE; }
   MSC_CUDA(cudaMemcpyAsync(out, pl->t4_64.p, sizeof(double2) * 4 * pl->g.nsite, cudaMemcpyDeviceToDevice, pl->stream));
@@ -249,6 +279,7 @@ int msc_t0_scalars(const msc_plan* pl, void* out) {
 }
 
 int msc_set_t0_scalars(msc_plan* pl, const void* t4, double omega) {
+  StreamFence fence(pl);
   if (!pl || !t4) { set_error("null argument"); return MSC_ERR_INVALID; }
   const size_t n = (size_t)4 * pl->g.nsite;
   MSC_TRY(dalloc(pl, pl->t4_64, sizeof(double2) * n));
@@ -261,6 +292,7 @@ int msc_set_t0_scalars(msc_plan* pl, const void* t4, double omega) {
 }
 
 int msc_build_g0(msc_plan* pl, double omega, const double* kpar, int volume_averaged, int n_orders) {
+  StreamFence fence(pl);
   if (!pl) { set_error("null plan"); return MSC_ERR_INVALID; }
   if (!(omega > 0)) { set_error("omega must be > 0, got %g", omega); return MSC_ERR_INVALID; }
   if (n_orders < 0) { set_error("n_orders must be >= 0"); return MSC_ERR_INVALID; }
@@ -280,11 +312,13 @@ int msc_build_g0(msc_plan* pl, double omega, const double* kpar, int volume_aver
 }
 
 int msc_incident(msc_plan* pl, double omega, const double* k_hat, int wave_type, void* psi0) {
+  StreamFence fence(pl);
   if (!pl || !k_hat || !psi0) { set_error("null argument"); return MSC_ERR_INVALID; }
   return launch_incident(pl, omega, k_hat, wave_type, (double2*)psi0, nullptr, false);
 }
 
 int msc_matvec(msc_plan* pl, const void* x, void* y, int precision) {
+  StreamFence fence(pl);
   if (!pl || !x || !y) { set_error("null argument"); return MSC_ERR_INVALID; }
   if (x == y) { set_error("x and y may not alias"); return MSC_ERR_INVALID; }
   const size_t n = field_elems(pl->g);
@@ -322,6 +356,7 @@ int msc_set_nearfield(msc_plan* pl, int degree, const double* coef, const double
     nf->dg.clear();
   }
   nf->dirty = true;
+  ++pl->gen;
   return MSC_OK;
 }
 
@@ -336,6 +371,7 @@ int msc_nearfield_blocks(const msc_plan* pl, double* out) {
 }
 
 int msc_precondition(msc_plan* pl, const void* x, void* z, int precision) {
+  StreamFence fence(pl);
   if (!pl || !x || !z) { set_error("null argument"); return MSC_ERR_INVALID; }
   if (x == z) { set_error("x and z may not alias"); return MSC_ERR_INVALID; }
   if (!pl->has_t0) { set_error("the preconditioner needs build_t0 first"); return MSC_ERR_STATE; }
@@ -360,6 +396,7 @@ int msc_precondition(msc_plan* pl, const void* x, void* z, int precision) {
 }
 
 int msc_solve(msc_plan* pl, const void* b, void* x, const msc_solve_opts* o, msc_solve_stats* st) {
+  StreamFence fence(pl);
   if (!pl || !b || !x || !o) { set_error("null argument"); return MSC_ERR_INVALID; }
   if (o->precision != MSC_SOLVE_MIXED && o->precision != MSC_SOLVE_FP64) {
     set_error("precision must be mixed (0) or fp64 (1)");
@@ -373,12 +410,14 @@ int msc_solve(msc_plan* pl, const void* b, void* x, const msc_solve_opts* o, msc
 }
 
 int msc_rpp_periodic(msc_plan* pl, const void* psi, double omega, double p, int flags, double* out) {
+  StreamFence fence(pl);
   if (!pl || !psi || !out) { set_error("null argument"); return MSC_ERR_INVALID; }
   if (flags & ~(MSC_RPP_BLOCH | MSC_RPP_PLANE_WAVE_MOMENT)) { set_error("unknown R_PP flags %d", flags); return MSC_ERR_INVALID; }
   return rpp_periodic(pl, (const double2*)psi, omega, p, flags, out);
 }
 
 int msc_reflected_field(msc_plan* pl, const void* psi, double omega, const double* k_hat, double* out) {
+  StreamFence fence(pl);
   if (!pl || !psi || !k_hat || !out) { set_error("null argument"); return MSC_ERR_INVALID; }
   return reflected_field(pl, (const double2*)psi, omega, k_hat, out);
 }

@@ -32,6 +32,7 @@ struct GState {
   int converged;  // |g_{j+1}| <= tol_abs
   int status;     // msc_status of the cycle
   int k;          // columns in the least-squares solution
+  int steps;      // Arnoldi steps run in the cycle (operator applications)
   double tol_abs; // target on |g_{j+1}|
   double beta;    // initial residual norm of the cycle
   double res;     // current residual estimate
@@ -50,6 +51,14 @@ struct GmresWork {
   DBuf part;              // partial sums [NB][33]
   GState* hstate = nullptr;  // pinned host mirror
   cudaEvent_t ev[2] = {nullptr, nullptr};
+  // captured Arnoldi cycles, [precision][preconditioned]
+  struct Graph {
+    cudaGraphExec_t exec = nullptr;
+    int m = 0;
+    bool cgs2 = false;
+    uint64_t gen = 0;
+    bool warm = false;  // a cycle of this kind ran uncaptured: kernel attributes set, buffers allocated
+  } graph[2][2];
 };
 
 constexpr int NB = 592;     // blocks of the multi-vector kernels (4 per SM)
@@ -292,6 +301,7 @@ __global__ void k_cycle_init(GState* st, HessPtr h, int m, double tol_abs) {
   st->res = beta;
   st->tol_abs = tol_abs;
   st->k = 0;
+  st->steps = 0;
   st->status = MSC_OK;
   st->converged = 0;
   st->done = 0;
@@ -328,6 +338,7 @@ __global__ void k_givens(GState* st, HessPtr h, int m, int j) {
   }
   __syncthreads();
   if (l == 0) {
+    st->steps = j + 1;
     const double hn = sqrt(h.nrm[0].x);
     col[j + 1] = make_double2(hn, 0);
     h.scale[j + 1] = hn > 0 ? 1.0 / hn : 0.0;
@@ -517,6 +528,9 @@ void gmres_free(msc_plan* pl) {
   dfree(pl, gw->V32); dfree(pl, gw->V64); dfree(pl, gw->Z32); dfree(pl, gw->Z64); dfree(pl, gw->x64); dfree(pl, gw->r64); dfree(pl, gw->ax64);
   dfree(pl, gw->d32); dfree(pl, gw->r32); dfree(pl, gw->state); dfree(pl, gw->hess); dfree(pl, gw->part);
   if (gw->hstate) cudaFreeHost(gw->hstate);
+  for (auto& row : gw->graph)
+    for (auto& gr : row)
+      if (gr.exec) cudaGraphExecDestroy(gr.exec);
   for (auto& e : gw->ev)
     if (e) cudaEventDestroy(e);
   delete gw;
@@ -565,24 +579,15 @@ static int gmres_core(msc_plan* pl, int m, const cx<T>* rhs, cx<T>* x, bool x_ze
     k_cycle_init<<<1, 32, 0, pl->stream>>>(st, h, m, tol_abs); ::msc::note_launch();
     MSC_CUDA(cudaGetLastError());
     int enq = 0;  // steps enqueued in this cycle
-    bool cycle_over = false;
-    // state after cycle init
-    MSC_CUDA(cudaMemcpyAsync(&gw->hstate[0], st, sizeof(GState), cudaMemcpyDeviceToHost, pl->stream));
-    MSC_CUDA(cudaEventRecord(gw->ev[0], pl->stream));
-    int pending = 0;  // index of the event holding the newest state
-    for (int j = 0; j < m && !cycle_over; ++j) {
-      if (used + 1 > max_mv) break;
+    auto step = [&](int j) -> int {
       // Arnoldi step j: w = A v_j (or A P v_j) into V[j+1]
       if (use_pc) {
         cx<T>* zj = Z + (size_t)j * n;
         MSC_TRY(nearfield_apply<T>(pl, V + (size_t)j * n, h.scale + j, zj, done));
-        ++*n_pc;
         MSC_TRY(launch_matvec<T>(pl, zj, nullptr, V + (size_t)(j + 1) * n, done));
       } else {
         MSC_TRY(launch_matvec<T>(pl, V + (size_t)j * n, h.scale + j, V + (size_t)(j + 1) * n, done));
       }
-      ++used;
-      ++enq;
       cx<T>* w = V + (size_t)(j + 1) * n;
       MSC_TRY(mdot<T>(pl, gw, V, j + 1, h.scale, w, h.h1, done));
       if (cgs2) {
@@ -594,27 +599,78 @@ static int gmres_core(msc_plan* pl, int m, const cx<T>* rhs, cx<T>* x, bool x_ze
         MSC_CUDA(cudaMemsetAsync(h.h2, 0, sizeof(double2) * (j + 1), pl->stream));
         MSC_TRY((maxpy<T, true>(pl, gw, V, j + 1, h.scale, h.h1, w, &h.nrm[0], done)));
       }
-      k_givens<<<1, 32, 0, pl->stream>>>(st, h, m, j); ::msc::note_launch();
+      k_givens<<<1, 32, 0, pl->stream>>>(st, h, m, j);
+      ::msc::note_launch();
       MSC_CUDA(cudaGetLastError());
-      const int slot = (pending + 1) & 1;
-      MSC_CUDA(cudaMemcpyAsync(&gw->hstate[slot], st, sizeof(GState), cudaMemcpyDeviceToHost, pl->stream));
-      MSC_CUDA(cudaEventRecord(gw->ev[slot], pl->stream));
-      // check the state of the previous step (lagged by one step)
-      MSC_CUDA(cudaEventSynchronize(gw->ev[pending]));
-      if (gw->hstate[pending].done) {
-        cycle_over = true;  // step j early-exits on the device
-        --used;             // ... and applies no operator
-        if (use_pc) --*n_pc;
-      }
-      pending = slot;
-    }
-    if (!cycle_over) {
-      MSC_CUDA(cudaEventSynchronize(gw->ev[pending]));
-    }
-    // cycles that ended at step j (and not before) are visible in the newest state
-    MSC_CUDA(cudaStreamSynchronize(pl->stream));
+      return MSC_OK;
+    };
     GState cur;
-    MSC_CUDA(cudaMemcpy(&cur, st, sizeof(GState), cudaMemcpyDeviceToHost));
+    auto& gr = gw->graph[sizeof(T) == 8 ? 1 : 0][use_pc ? 1 : 0];
+    // A whole cycle as one captured graph: m steps whose kernels return at once
+    // after the device flag `done` is set. Used from the second cycle of a plan
+    // generation on (buffers allocated, kernel attributes set) and when the budget
+    // covers m steps.
+    const bool graph_ok = gr.exec && gr.m == m && gr.cgs2 == cgs2 && gr.gen == pl->gen;
+    if ((graph_ok || gr.warm) && used + m <= max_mv) {
+      if (!graph_ok) {
+        if (use_pc) MSC_TRY(nearfield_refresh(pl));
+        if (gr.exec) cudaGraphExecDestroy(gr.exec);
+        gr.exec = nullptr;
+        cudaGraph_t graph = nullptr;
+        MSC_CUDA(cudaStreamBeginCapture(pl->stream, cudaStreamCaptureModeThreadLocal));
+        int cs = MSC_OK;
+        for (int j = 0; j < m && cs == MSC_OK; ++j) cs = step(j);
+        const cudaError_t ce = cudaStreamEndCapture(pl->stream, &graph);
+        if (cs != MSC_OK) {
+          if (graph) cudaGraphDestroy(graph);
+          return cs;
+        }
+        MSC_CUDA(ce);
+        const cudaError_t ie = cudaGraphInstantiate(&gr.exec, graph, 0);
+        cudaGraphDestroy(graph);
+        MSC_CUDA(ie);
+        gr.m = m;
+        gr.cgs2 = cgs2;
+        gr.gen = pl->gen;
+      }
+      MSC_CUDA(cudaGraphLaunch(gr.exec, pl->stream));
+      ::msc::note_launch();
+      MSC_CUDA(cudaMemcpyAsync(&gw->hstate[0], st, sizeof(GState), cudaMemcpyDeviceToHost, pl->stream));
+      MSC_CUDA(cudaStreamSynchronize(pl->stream));
+      cur = gw->hstate[0];
+      used += cur.steps;
+      enq = cur.steps;
+      if (use_pc) *n_pc += cur.steps;
+    } else {
+      bool cycle_over = false;
+      // state after cycle init
+      MSC_CUDA(cudaMemcpyAsync(&gw->hstate[0], st, sizeof(GState), cudaMemcpyDeviceToHost, pl->stream));
+      MSC_CUDA(cudaEventRecord(gw->ev[0], pl->stream));
+      int pending = 0;  // index of the event holding the newest state
+      for (int j = 0; j < m && !cycle_over; ++j) {
+        if (used + 1 > max_mv) break;
+        MSC_TRY(step(j));
+        ++used;
+        ++enq;
+        if (use_pc) ++*n_pc;
+        const int slot = (pending + 1) & 1;
+        MSC_CUDA(cudaMemcpyAsync(&gw->hstate[slot], st, sizeof(GState), cudaMemcpyDeviceToHost, pl->stream));
+        MSC_CUDA(cudaEventRecord(gw->ev[slot], pl->stream));
+        // check the state of the previous step (lagged by one step)
+        MSC_CUDA(cudaEventSynchronize(gw->ev[pending]));
+        if (gw->hstate[pending].done) {
+          cycle_over = true;  // step j early-exits on the device
+          --used;             // ... and applies no operator
+          if (use_pc) --*n_pc;
+        }
+        pending = slot;
+      }
+      // cycles that ended at step j (and not before) are visible in the newest state
+      MSC_CUDA(cudaMemcpyAsync(&gw->hstate[0], st, sizeof(GState), cudaMemcpyDeviceToHost, pl->stream));
+      MSC_CUDA(cudaStreamSynchronize(pl->stream));
+      cur = gw->hstate[0];
+      gr.warm = true;
+    }
     // x += V y (k columns), or Z y with the preconditioner
     if (cur.k > 0) {
       const int nb = std::min<long long>(NB, ceil_div((long long)n, NTH));

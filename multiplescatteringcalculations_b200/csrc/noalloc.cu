@@ -74,6 +74,7 @@ template <typename T> static size_t static_need(const Geo& g) {
 using namespace msc;
 
 extern "C" int msc_matvec_noalloc(msc_plan* pl, const void* x, void* y, int precision) {
+  StreamFence fence(pl);
   if (!pl || !x || !y) {
     set_error("null argument");
     return MSC_ERR_INVALID;

@@ -170,7 +170,7 @@ __global__ void __launch_bounds__(256) k_nf64(const double2* __restrict__ x, con
 }
 
 // Rebuild the per-layer blocks g64 + dg[l] (complex64 parameters, complex128 device copy).
-static int nearfield_refresh(msc_plan* pl) {
+int nearfield_refresh(msc_plan* pl) {
   NearField* nf = pl->nf;
   if (!nf->dirty) return MSC_OK;
   const int L = std::max(1, std::min(nf->L, NF_MAXL));
@@ -188,6 +188,7 @@ static int nearfield_refresh(msc_plan* pl) {
                            pl->stream));
   MSC_CUDA(cudaStreamSynchronize(pl->stream));
   nf->dirty = false;
+  ++pl->gen;
   return MSC_OK;
 }
 

@@ -38,6 +38,8 @@ struct NearField {
 // Extract the near-field blocks from the spatial kernel of the G0 build (values
 // times `scale`).
 int nearfield_extract(msc_plan* pl, const double2* Ks_spatial, double scale);
+// Rebuild the per-layer blocks after a change (synchronises the plan's stream).
+int nearfield_refresh(msc_plan* pl);
 // z = P(s v), s = *scale (1 when null); `done` as in the matvec.
 template <typename T>
 int nearfield_apply(msc_plan* pl, const cx<T>* v, const double* scale, cx<T>* z, const int* done);

@@ -56,7 +56,12 @@ struct NearField;
 struct msc_plan {
   msc_slab_desc desc;
   msc::Geo g;
+  // All work of a plan runs on its own non-blocking stream (capturable into graphs);
+  // every entry point orders it after the caller's stream `user` and the caller's
+  // stream after it (StreamFence).
   cudaStream_t stream = nullptr;
+  cudaStream_t user = nullptr;
+  cudaEvent_t ev_in = nullptr, ev_out = nullptr;
   int device = 0;
   msc::FftPlan1D fz, fxy;
   // twiddles exp(-2 pi i t / L) for Lz and Lxy
@@ -88,9 +93,30 @@ struct msc_plan {
   // near-field preconditioner (blocks from the last G0 build, coefficients)
   msc::NearField* nf = nullptr;
   int64_t bytes = 0;
+  // bumped by every (re)allocation, spectrum build and preconditioner change: the
+  // captured solver graphs of an older generation are stale
+  uint64_t gen = 1;
 };
 
 namespace msc {
+
+// Orders the plan's stream after the caller's on entry and the caller's after the
+// plan's on exit.
+struct StreamFence {
+  msc_plan* pl;
+  explicit StreamFence(msc_plan* p) : pl(p) {
+    if (pl && pl->ev_in) {
+      cudaEventRecord(pl->ev_in, pl->user);
+      cudaStreamWaitEvent(pl->stream, pl->ev_in, 0);
+    }
+  }
+  ~StreamFence() {
+    if (pl && pl->ev_out) {
+      cudaEventRecord(pl->ev_out, pl->stream);
+      cudaStreamWaitEvent(pl->user, pl->ev_out, 0);
+    }
+  }
+};
 
 int dalloc(msc_plan* pl, DBuf& b, size_t bytes);
 void dfree(msc_plan* pl, DBuf& b);

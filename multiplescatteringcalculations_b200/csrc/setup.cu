@@ -1,6 +1,7 @@
 // Per-frequency setup on the device: twiddle tables, T0 (4 scalars per voxel),
 // the incident plane wave, layout conversions, and the G0 spectrum build.
 #include <algorithm>
+#include <cstring>
 
 #include "physics.cuh"
 #include "mv_common.cuh"
@@ -312,7 +313,9 @@ int launch_g0(msc_plan* pl, double omega, const double* kpar, int va, int n_orde
   // The kernel is mirror symmetric in each axis, K(R_a r) = S_a K(r) S_a, and its
   // spectrum is stored on the octant kz <= Lz/2, ky <= Ly/2, kx <= Lx/2. The
   // Bloch-phased kernel loses the symmetry in x and y and is stored in full.
+  const Geo before = pl->g;
   set_spectrum_box(pl->g, kpar == nullptr);
+  if (memcmp(&before, &pl->g, sizeof(Geo)) != 0) ++pl->gen;  // kernels take the geometry by value
   const Geo& g = pl->g;
   const int E = va ? 81 : 45;
   if (pl->khat64.p && pl->E != E) {
