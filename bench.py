@@ -46,6 +46,9 @@ WORKLOADS = {
     "cfg2": dict(M=64, N_z=16, ka=0.5, angle=20.0, wave="P", mat=("grf", 3.0, 0.15), tol=1e-10, periodic=False),
     "cfg1": dict(M=16, N_z=4, ka=0.2, angle=0.0, wave="P", mat=("iid", 0.10), tol=1e-10, periodic=True),
     "cfg5": dict(M=256, N_z=32, ka=1.0, angle=30.0, wave="S", mat=("grf", 3.0, 0.40), tol=1e-8, periodic=True),
+    # 256 uneven slabs: M ~ U{16,24,...,96}, N_z ~ U{4..24}, ka ~ U[0.1,1], theta ~ U[0,40 deg],
+    # P/SV 50/50, i.i.d. +-20 %, aperiodic; one msc_batch_solve call per step
+    "cfg3": dict(batch=256, tol=1e-8, periodic=False, mat=("iid", 0.20)),
 }
 ALPHA, BETA, RHO, A = 3000.0, 1732.0, 2500.0, 1.0
 
@@ -361,6 +364,96 @@ def run_ours(args, wl, rank, world, local_rank):
     return 0
 
 
+def batch_problems(wl: dict, seed: int):
+    """The cfg3 slabs, drawn from `seed`."""
+    from multiplescatteringcalculations_b200 import BatchProblem, ReferenceMedium, SlabGeometry, uniform_random_material
+
+    ref = ReferenceMedium(ALPHA, BETA, RHO)
+    r = np.random.default_rng(seed)
+    out = []
+    for i in range(wl["batch"]):
+        M = int(r.choice(np.arange(16, 97, 8)))
+        Nz = int(r.integers(4, 25))
+        ka = r.uniform(0.1, 1.0)
+        th = r.uniform(0.0, np.deg2rad(40.0))
+        wave = "P" if r.random() < 0.5 else "S"
+        g = SlabGeometry(M, Nz, A)
+        mat = uniform_random_material(g, ref, wl["mat"][1], seed=seed * 1000 + i)
+        out.append(BatchProblem(g, mat, ka * BETA / A, np.array([np.cos(th), np.sin(th), 0.0]), wave,
+                                periodic=wl["periodic"]))
+    return out
+
+
+def run_batch(args, wl, rank, world, local_rank) -> int:
+    """cfg3: one step = one msc_batch_solve over the 256 slabs (host arrays in, fields
+    and R_PP out); ranks solve disjoint batches (weak scaling). Also times a sample of
+    the same slabs as a sequential loop of single solves."""
+    import torch
+    import torch.distributed as dist
+
+    from multiplescatteringcalculations_b200 import _native, compute_slab_scattering_batch, compute_slab_scattering_gpu
+
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    lib = _native.load()
+    probs = batch_problems(wl, seed=1000 + rank)
+    kw = dict(gmres_tol=wl["tol"], max_iter=2000, precision="mixed",
+              preconditioner=None if args.precond == "none" else args.precond)
+    warm = batch_problems(dict(wl, batch=16), seed=7)
+    for _ in range(args.warmup):
+        compute_slab_scattering_batch(warm, workers=args.workers, **kw)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    n0 = lib.msc_launch_count()
+    with ClockSampler(local_rank) as clk:
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            sols, info = compute_slab_scattering_batch(probs, workers=args.workers, **kw)
+        torch.cuda.synchronize()
+        dt = time.perf_counter() - t0
+    launches = lib.msc_launch_count() - n0
+    t = torch.tensor([dt], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    dt = float(t.item())
+    value = world * args.steps * len(probs) / dt
+    bad = [i for i, s in enumerate(sols) if s.status != 0]
+    if bad:
+        raise RuntimeError(f"batch items {bad[:8]} did not converge")
+    seq = probs[: min(len(probs), 64)]
+    for pr in seq[:4]:
+        compute_slab_scattering_gpu(pr.geometry, pr.material, pr.omega, pr.k_hat, pr.wave_type, device=dev, **kw)
+    torch.cuda.synchronize()
+    t1 = time.perf_counter()
+    for pr in seq:
+        compute_slab_scattering_gpu(pr.geometry, pr.material, pr.omega, pr.k_hat, pr.wave_type, device=dev, **kw)
+    torch.cuda.synchronize()
+    seq_rate = len(seq) / (time.perf_counter() - t1)
+    nmv = [s.n_gmres_iter for s in sols]
+    ns = sum(p.geometry.N_z * p.geometry.M ** 2 for p in probs)
+    line = {
+        "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": dt / args.steps * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "c64+c128", "data": "synthetic",
+        "config": {"workload": "cfg3", "slabs": len(probs), "M": "U{16,24,...,96}", "N_z": "U{4..24}",
+                   "ka": "U[0.1,1]", "incidence_deg": "U[0,40]", "wave": "P/SV 50/50", "material": "iid +-20%",
+                   "tol": wl["tol"], "periodic": wl["periodic"], "precond": args.precond,
+                   "l2": "inputs larger than L2 (the batch's spectra and fields)"},
+        "gpu_launches": int(launches),
+        "batch": {"workers": info["workers"], "n_matvec_mean": float(np.mean(nmv)), "n_matvec_max": int(max(nmv)),
+                  "voxels": int(ns), "sequential_solves_per_s": seq_rate, "sequential_sample": len(seq),
+                  "speedup_vs_sequential": value / world / seq_rate},
+        "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": int(3 * 8 * ns),
+                "d2h_bytes_per_step": int(9 * 16 * ns),
+                "note": "the batch API takes host arrays and returns host fields"},
+        "clocks": clk.summary(),
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    return 0
+
+
 def run_matvecs(wl: dict, n: int) -> int:
     """Plan + T0 + G0 of the workload, then 3 untimed and n timed complex64 operator
     applications through msc_matvec (each: 2 layout transposes and the matvec
@@ -402,6 +495,7 @@ def main(argv=None) -> int:
     ap.add_argument("--workload", default="cfg2", choices=sorted(WORKLOADS))
     ap.add_argument("--precond", default="none", choices=["none", "nearfield"],
                     help="right preconditioner of the timed mixed-precision solves")
+    ap.add_argument("--workers", type=int, default=0, help="cfg3: batch worker threads (0 = autotune)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--solve-only", action="store_true", help="timed solves only (for profiler launch lists)")
@@ -416,6 +510,20 @@ def main(argv=None) -> int:
         return run_reference(args, wl, rank, world)
     if args.matvec_only:
         return run_matvecs(wl, args.matvec_only)
+    if "batch" in wl:
+        if world > 1:
+            import datetime
+
+            import torch
+            import torch.distributed as dist
+
+            torch.cuda.set_device(local_rank)
+            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+            try:
+                return run_batch(args, wl, rank, world, local_rank)
+            finally:
+                dist.destroy_process_group()
+        return run_batch(args, wl, rank, world, local_rank)
     if world > 1:
         import datetime
 

@@ -151,6 +151,36 @@ int msc_precondition(msc_plan* plan, const void* x, void* z, int precision);
  * Non-convergence returns MSC_NOT_CONVERGED with x the best iterate. */
 int msc_solve(msc_plan* plan, const void* b, void* x, const msc_solve_opts* opts, msc_solve_stats* stats);
 
+/* One slab of a batch (msc_batch_solve). Inputs are host memory read during the
+ * call; outputs are written in place. */
+typedef struct msc_batch_item {
+  msc_slab_desc desc;      /* geometry, background medium, periodicity, padding */
+  const double* dlam;      /* (N_z, M, M) contrasts, host float64 */
+  const double* dmu;
+  const double* drho;
+  double omega;            /* angular frequency */
+  double k_hat[3];         /* incidence direction (z, x, y) */
+  int32_t wave_type;       /* msc_wave */
+  int32_t bloch;           /* periodic only: Bloch-phased fold at the incidence's k_par */
+  void* psi;               /* out (may be NULL): (N_z, M, M, 9) complex128, host */
+  double rpp[2];           /* out: specular R_PP (re, im) by the Weyl sum of the solution */
+  msc_solve_stats stats;   /* out */
+  int32_t status;          /* out: msc_status of this item */
+  char error[160];         /* out: message of a failed item */
+} msc_batch_item;
+
+/* Solve n independent slabs (uneven sizes, frequencies and incidences) on the
+ * current device: T0 and G0 builds, incident field, solve with opts, R_PP and the
+ * field, per item. `workers` host threads with a stream and a plan cache each run
+ * items concurrently (0 = choose by timing the first items at 2, 4 and 8 workers;
+ * the count used is written to *workers_used when not NULL). Returns MSC_OK when
+ * every item converged, MSC_NOT_CONVERGED when any item failed or did not converge
+ * (its own status and message say which), negative only for errors of the call
+ * itself (arguments, streams). Replaces a loop of compute_slab_scattering_gpu calls
+ * (slab_scattering_gpu.py:158-256), e.g. the frequency loop of
+ * compute_ocean_bottom_reflection (ocean_bottom.py:290-307). */
+int msc_batch_solve(msc_batch_item* items, int n, const msc_solve_opts* opts, int workers, int* workers_used);
+
 /* Flags of msc_rpp_periodic. */
 #define MSC_RPP_BLOCH 1             /* demodulate the sources by exp(-i k_par.x), k_par the plan's Bloch wavevector */
 #define MSC_RPP_PLANE_WAVE_MOMENT 2 /* moment term with |k| = omega/alpha instead of the reference's kz

@@ -7,6 +7,8 @@ behind the C-ABI library ``libmsc_b200.so``.
 """
 
 from .slab import (  # noqa: F401
+    BatchProblem,
+    BatchSolution,
     MaterialContrast,
     ReferenceMedium,
     SlabGeometry,
@@ -14,6 +16,7 @@ from .slab import (  # noqa: F401
     SlabPlan,
     SlabResult,
     clear_plan_cache,
+    compute_slab_scattering_batch,
     compute_slab_scattering_gpu,
     compute_slab_tmatrices,
     gaussian_random_field_material,

@@ -73,6 +73,24 @@ class SolveStats(C.Structure):
     ]
 
 
+class BatchItem(C.Structure):
+    _fields_ = [
+        ("desc", SlabDesc),
+        ("dlam", C.c_void_p),
+        ("dmu", C.c_void_p),
+        ("drho", C.c_void_p),
+        ("omega", C.c_double),
+        ("k_hat", C.c_double * 3),
+        ("wave_type", C.c_int32),
+        ("bloch", C.c_int32),
+        ("psi", C.c_void_p),
+        ("rpp", C.c_double * 2),
+        ("stats", SolveStats),
+        ("status", C.c_int32),
+        ("error", C.c_char * 160),
+    ]
+
+
 # name -> (restype, argtypes); every entry point that include/msc.h declares
 SIGNATURES = {
     "msc_plan_create": (C.c_int, [C.POINTER(SlabDesc), C.c_void_p, C.POINTER(C.c_void_p)]),
@@ -89,6 +107,8 @@ SIGNATURES = {
     "msc_matvec_noalloc": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int]),
     "msc_solve": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(SolveOpts), C.POINTER(SolveStats)]),
     "msc_set_nearfield": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]),
+    "msc_batch_solve": (C.c_int, [C.POINTER(BatchItem), C.c_int, C.POINTER(SolveOpts), C.c_int,
+                                  C.POINTER(C.c_int)]),
     "msc_nearfield_blocks": (C.c_int, [C.c_void_p, C.c_void_p]),
     "msc_precondition": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int]),
     "msc_rpp_periodic": (C.c_int, [C.c_void_p, C.c_void_p, C.c_double, C.c_double, C.c_int, C.c_void_p]),

@@ -1,0 +1,241 @@
+// msc_batch_solve: many slab solves of uneven size, frequency and incidence on one
+// GPU.
+//
+// Small slabs cannot fill a B200 on their own (an Arnoldi step of a 16 x 16 x 4
+// slab is a few microseconds of launches on a few dozen SMs), so the batch runs
+// several solves at once: `workers` host threads each own a stream, a small cache
+// of plans (LRU, keyed by geometry and background) and pinned staging buffers, and
+// take items from a shared counter. Every plan's work runs on its own stream with
+// graph-captured GMRES cycles, so the solves of different workers overlap on the
+// device. With workers = 0 an online autotuner times the first items at 2, 4 and 8
+// workers and finishes the batch with the fastest. Items are independent: a failed
+// item records its status and the others continue.
+#include <algorithm>
+#include <atomic>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <thread>
+#include <vector>
+
+#include "plan.cuh"
+
+namespace msc {
+
+namespace {
+
+constexpr int BATCH_PLANS_PER_WORKER = 2;
+
+struct CachedPlan {
+  msc_slab_desc key;
+  msc_plan* plan = nullptr;
+  long long last_use = 0;
+};
+
+struct Worker {
+  cudaStream_t stream = nullptr;
+  std::vector<CachedPlan> plans;
+  long long tick = 0;
+  // device staging: contrasts (3 N float64), psi0 and x (9 N complex128 each)
+  void* dev = nullptr;
+  size_t dev_bytes = 0;
+  // pinned host staging for the contrasts and the solution
+  void* host = nullptr;
+  size_t host_bytes = 0;
+
+  Worker() = default;
+  Worker(const Worker&) = delete;
+  Worker& operator=(const Worker&) = delete;
+  ~Worker() {
+    for (auto& c : plans)
+      if (c.plan) msc_plan_destroy(c.plan);
+    if (dev) cudaFreeAsync(dev, stream);
+    if (stream) {
+      cudaStreamSynchronize(stream);
+      cudaStreamDestroy(stream);
+    }
+    if (host) cudaFreeHost(host);
+  }
+
+  int plan_for(const msc_slab_desc& d, msc_plan** out) {
+    ++tick;
+    for (auto& c : plans)
+      if (std::memcmp(&c.key, &d, sizeof(d)) == 0) {
+        c.last_use = tick;
+        *out = c.plan;
+        return MSC_OK;
+      }
+    if ((int)plans.size() >= BATCH_PLANS_PER_WORKER) {
+      auto it = std::min_element(plans.begin(), plans.end(),
+                                 [](const CachedPlan& a, const CachedPlan& b) { return a.last_use < b.last_use; });
+      msc_plan_destroy(it->plan);
+      plans.erase(it);
+    }
+    msc_plan* p = nullptr;
+    const int s = msc_plan_create(&d, stream, &p);
+    if (s != MSC_OK) return s;
+    CachedPlan c;
+    std::memcpy(&c.key, &d, sizeof(d));
+    c.plan = p;
+    c.last_use = tick;
+    plans.push_back(c);
+    *out = p;
+    return MSC_OK;
+  }
+
+  int staging(size_t dbytes, size_t hbytes) {
+    if (dev_bytes < dbytes) {
+      if (dev) cudaFreeAsync(dev, stream);
+      dev = nullptr;
+      dev_bytes = 0;
+      if (cudaMallocAsync(&dev, dbytes, stream) != cudaSuccess) {
+        cudaGetLastError();
+        set_error("batch: device staging of %zu bytes failed", dbytes);
+        return MSC_ERR_NOMEM;
+      }
+      dev_bytes = dbytes;
+    }
+    if (host_bytes < hbytes) {
+      cudaStreamSynchronize(stream);
+      if (host) cudaFreeHost(host);
+      host = nullptr;
+      host_bytes = 0;
+      if (cudaMallocHost(&host, hbytes) != cudaSuccess) {
+        cudaGetLastError();
+        set_error("batch: pinned staging of %zu bytes failed", hbytes);
+        return MSC_ERR_NOMEM;
+      }
+      host_bytes = hbytes;
+    }
+    return MSC_OK;
+  }
+
+  // One item end to end; its statistics and R_PP are written in place.
+  int solve(msc_batch_item& it, const msc_solve_opts& o) {
+    msc_plan* pl = nullptr;
+    MSC_TRY(plan_for(it.desc, &pl));
+    const size_t ns = (size_t)it.desc.N_z * it.desc.M * it.desc.M;
+    const size_t fb = sizeof(double2) * 9 * ns;
+    MSC_TRY(staging(3 * sizeof(double) * ns + 2 * fb, std::max(3 * sizeof(double) * ns, fb)));
+    double* dc = (double*)dev;
+    double2* psi0 = (double2*)(dc + 3 * ns);
+    double2* x = psi0 + 9 * ns;
+    double* hc = (double*)host;
+    MSC_CUDA(cudaStreamSynchronize(stream));  // the pinned buffer is free again
+    std::memcpy(hc, it.dlam, sizeof(double) * ns);
+    std::memcpy(hc + ns, it.dmu, sizeof(double) * ns);
+    std::memcpy(hc + 2 * ns, it.drho, sizeof(double) * ns);
+    MSC_CUDA(cudaMemcpyAsync(dc, hc, 3 * sizeof(double) * ns, cudaMemcpyHostToDevice, stream));
+    MSC_TRY(msc_build_t0(pl, dc, dc + ns, dc + 2 * ns, it.omega));
+    const double nk = std::sqrt(it.k_hat[0] * it.k_hat[0] + it.k_hat[1] * it.k_hat[1] + it.k_hat[2] * it.k_hat[2]);
+    const double speed = it.wave_type == MSC_WAVE_P ? it.desc.alpha : it.desc.beta;
+    double kpar[2] = {0.0, 0.0};
+    if (it.bloch) {
+      kpar[0] = it.omega / speed * it.k_hat[1] / nk;
+      kpar[1] = it.omega / speed * it.k_hat[2] / nk;
+    }
+    MSC_TRY(msc_build_g0(pl, it.omega, it.bloch ? kpar : nullptr, 0, 2));
+    MSC_TRY(msc_incident(pl, it.omega, it.k_hat, it.wave_type, psi0));
+    msc_solve_stats st{};
+    const int s = msc_solve(pl, psi0, x, &o, &st);
+    it.stats = st;
+    if (s < 0) return s;
+    // specular R_PP: at the horizontal slowness of the incidence for Bloch items,
+    // else at normal incidence (the reference's default)
+    const double p = it.bloch ? std::sqrt(it.k_hat[1] * it.k_hat[1] + it.k_hat[2] * it.k_hat[2]) / nk / speed : 0.0;
+    MSC_TRY(msc_rpp_periodic(pl, x, it.omega, p, it.bloch ? MSC_RPP_BLOCH : 0, it.rpp));
+    if (it.psi) {
+      MSC_CUDA(cudaMemcpyAsync(host, x, fb, cudaMemcpyDeviceToHost, stream));
+      MSC_CUDA(cudaStreamSynchronize(stream));
+      std::memcpy(it.psi, host, fb);
+    }
+    return s;
+  }
+};
+
+// Solve items [next, end) with w workers; returns the elapsed seconds.
+double run_workers(std::vector<Worker>& pool, int w, msc_batch_item* items, std::atomic<int>& next, int end,
+                   const msc_solve_opts& o, int device) {
+  const auto t0 = std::chrono::steady_clock::now();
+  std::vector<std::thread> th;
+  for (int i = 0; i < w; ++i) {
+    th.emplace_back([&, i]() {
+      cudaSetDevice(device);
+      Worker& wk = pool[i];
+      while (true) {
+        // claim the next item below `end` without moving the counter past it, so the
+        // items after a chunk stay for the next chunk
+        int k = next.load();
+        while (k < end && !next.compare_exchange_weak(k, k + 1)) {
+        }
+        if (k >= end) break;
+        msc_batch_item& it = items[k];
+        const int s = wk.solve(it, o);
+        it.status = s;
+        if (s < 0) {
+          std::strncpy(it.error, msc_last_error(), sizeof(it.error) - 1);
+          it.error[sizeof(it.error) - 1] = 0;
+        }
+      }
+    });
+  }
+  for (auto& t : th) t.join();
+  return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+}
+
+}  // namespace
+}  // namespace msc
+
+using namespace msc;
+
+extern "C" int msc_batch_solve(msc_batch_item* items, int n, const msc_solve_opts* opts, int workers,
+                               int* workers_used) {
+  if ((!items && n > 0) || !opts || n < 0) {
+    set_error("null argument");
+    return MSC_ERR_INVALID;
+  }
+  if (workers < 0 || workers > 64) {
+    set_error("workers must be in [0, 64], got %d", workers);
+    return MSC_ERR_INVALID;
+  }
+  for (int i = 0; i < n; ++i) {
+    msc_batch_item& it = items[i];
+    if (!it.dlam || !it.dmu || !it.drho) {
+      set_error("item %d: null contrast array", i);
+      return MSC_ERR_INVALID;
+    }
+    it.status = MSC_NOT_CONVERGED;
+    it.error[0] = 0;
+    it.rpp[0] = it.rpp[1] = 0.0;
+    std::memset(&it.stats, 0, sizeof(it.stats));
+  }
+  int device = 0;
+  MSC_CUDA(cudaGetDevice(&device));
+  const int maxw = workers > 0 ? workers : 8;
+  std::vector<Worker> pool(maxw);
+  for (auto& w : pool) MSC_CUDA(cudaStreamCreateWithFlags(&w.stream, cudaStreamNonBlocking));
+  std::atomic<int> next{0};
+  int chosen = workers;
+  if (workers == 0) {
+    // online autotune: a chunk of items at 2, 4 and 8 workers, time per item compared
+    const int chunk = std::max(2, std::min(16, n / 8));
+    double best = 1e300;
+    chosen = 2;
+    for (int w : {2, 4, 8}) {
+      const int start = next.load();
+      if (start >= n) break;
+      const int end = std::min(n, start + chunk * w / 2);
+      const double t = run_workers(pool, w, items, next, end, *opts, device);
+      const double per = t / std::max(1, end - start);
+      if (per < best) {
+        best = per;
+        chosen = w;
+      }
+    }
+  }
+  if (next.load() < n) run_workers(pool, chosen, items, next, n, *opts, device);
+  if (workers_used) *workers_used = chosen;
+  for (int i = 0; i < n; ++i)
+    if (items[i].status != MSC_OK) return MSC_NOT_CONVERGED;
+  return MSC_OK;
+}

@@ -530,6 +530,104 @@ def compute_slab_scattering_gpu(
 
 
 # ---------------------------------------------------------------------------
+# Batched solves
+# ---------------------------------------------------------------------------
+
+
+@dataclass
+class BatchProblem:
+    """One slab of a batch: geometry, material, frequency and incidence."""
+
+    geometry: SlabGeometry
+    material: SlabMaterial
+    omega: float
+    k_hat: NDArray
+    wave_type: str = "P"
+    periodic: bool = False
+    bloch: bool = False
+
+
+@dataclass
+class BatchSolution:
+    """Result of one batch item: the field (None when not requested), the specular
+    R_PP of the solution by the Weyl sum (at the Bloch slowness for ``bloch``
+    items, else at normal incidence), and the solver counters."""
+
+    psi: NDArray | None
+    rpp: complex
+    n_gmres_iter: int
+    gmres_residual: float
+    status: int
+    stats: dict
+
+
+def compute_slab_scattering_batch(problems, *, gmres_tol: float = 1e-6, max_iter: int = 500, restart: int = 30,
+                                  precision: str = "mixed", preconditioner: str | None = None,
+                                  initial_guess: str = "born", ortho: str = "auto", workers: int = 0,
+                                  return_fields: bool = True):
+    """Solve many independent slabs of uneven size, frequency and incidence on the
+    current GPU in one call (``msc_batch_solve``): per item the T0 and G0 builds,
+    the incident field, the solve and R_PP. ``workers`` host threads (each with its
+    own stream and plans) run items concurrently; 0 lets the library choose by
+    timing. Returns (list of BatchSolution, info) with info["workers"] the count
+    used. Items that fail or do not converge keep their own status; a warning names
+    them."""
+    if precision not in ("mixed", "fp64"):
+        raise ValueError(f"precision must be 'mixed' or 'fp64', got {precision!r}")
+    pcs = {None: N.MSC_PC_NONE, "none": N.MSC_PC_NONE, "nearfield": N.MSC_PC_NEARFIELD}
+    if preconditioner not in pcs:
+        raise ValueError(f"preconditioner must be None or 'nearfield', got {preconditioner!r}")
+    if ortho not in ("auto", "cgs1", "cgs2"):
+        raise ValueError(f"ortho must be 'auto', 'cgs1' or 'cgs2', got {ortho!r}")
+    problems = list(problems)
+    n = len(problems)
+    items = (N.BatchItem * max(1, n))()
+    keep, outs = [], []
+    for i, pr in enumerate(problems):
+        if pr.wave_type not in ("P", "S"):
+            raise ValueError(f"item {i}: wave_type must be 'P' or 'S', got '{pr.wave_type}'")
+        if pr.bloch and not pr.periodic:
+            raise ValueError(f"item {i}: bloch=True needs periodic=True")
+        g, ref = pr.geometry, pr.material.ref
+        arrs = [np.ascontiguousarray(np.asarray(a, dtype=np.float64).reshape(g.N_z, g.M, g.M))
+                for a in (pr.material.Dlambda, pr.material.Dmu, pr.material.Drho)]
+        keep.append(arrs)
+        it = items[i]
+        it.desc = N.SlabDesc(g.M, g.N_z, float(g.a), float(ref.alpha), float(ref.beta), float(ref.rho),
+                             int(bool(pr.periodic)), 0, 0)
+        it.dlam, it.dmu, it.drho = (a.ctypes.data for a in arrs)
+        it.omega = float(pr.omega)
+        kh = np.asarray(pr.k_hat, dtype=float).ravel()
+        for j in range(3):
+            it.k_hat[j] = float(kh[j])
+        it.wave_type = N.MSC_WAVE_P if pr.wave_type == "P" else N.MSC_WAVE_S
+        it.bloch = int(bool(pr.bloch))
+        out = np.empty((g.N_z, g.M, g.M, 9), dtype=np.complex128) if return_fields else None
+        outs.append(out)
+        it.psi = out.ctypes.data if out is not None else None
+    opts = N.SolveOpts(float(gmres_tol), int(max_iter), int(restart),
+                       N.MSC_SOLVE_MIXED if precision == "mixed" else N.MSC_SOLVE_FP64,
+                       0 if initial_guess == "born" else 1, 0.0, {"auto": 0, "cgs1": 1, "cgs2": 2}[ortho],
+                       pcs[preconditioner])
+    used = C.c_int(0)
+    lib = N.load()
+    N.check(lib.msc_batch_solve(items, n, C.byref(opts), int(workers), C.byref(used)), "msc_batch_solve")
+    sols, bad = [], []
+    for i in range(n):
+        it = items[i]
+        st = {"n_matvec": it.stats.n_matvec, "n_matvec64": it.stats.n_matvec64, "n_outer": it.stats.n_outer,
+              "residual": it.stats.residual, "n_precond": it.stats.n_precond,
+              "pc_fallback": bool(it.stats.pc_fallback)}
+        if it.status != 0:
+            bad.append((i, it.status, it.error.decode(errors="replace")))
+        sols.append(BatchSolution(psi=outs[i], rpp=complex(it.rpp[0], it.rpp[1]), n_gmres_iter=int(it.stats.n_matvec),
+                                  gmres_residual=float(it.stats.residual), status=int(it.status), stats=st))
+    if bad:
+        warnings.warn(f"{len(bad)} batch item(s) did not converge or failed: {bad[:4]}", stacklevel=2)
+    return sols, {"workers": int(used.value)}
+
+
+# ---------------------------------------------------------------------------
 # Observables (slab_scattering.py:589-735)
 # ---------------------------------------------------------------------------
 

@@ -61,3 +61,29 @@ def test_plan_create_rejects_bad_geometry():
         N.check(N.MSC_ERR_INVALID, "x") if False else N.check(
             lib.msc_plan_create(C.byref(N.SlabDesc(0, 2, 1.0, 3000.0, 1732.0, 2500.0, 0, 0, 0)), None, C.byref(h)),
             "msc_plan_create")
+
+
+def test_struct_layouts_match_the_header(tmp_path):
+    """The ctypes mirrors have the sizes and field offsets of the C structs."""
+    import ctypes as C
+    import shutil
+
+    from multiplescatteringcalculations_b200 import _native as N
+
+    cc = shutil.which("gcc") or shutil.which("cc")
+    if cc is None:
+        pytest.skip("no C compiler")
+    src = tmp_path / "sz.c"
+    src.write_text(
+        '#include <stdio.h>\n#include <stddef.h>\n#include "msc.h"\n'
+        "int main(void) {\n"
+        '  printf("%zu %zu %zu %zu %zu %zu %zu\\n", sizeof(msc_slab_desc), sizeof(msc_solve_opts),\n'
+        "         sizeof(msc_solve_stats), sizeof(msc_batch_item), offsetof(msc_batch_item, stats),\n"
+        "         offsetof(msc_batch_item, status), offsetof(msc_solve_opts, preconditioner));\n"
+        "  return 0;\n}\n")
+    exe = tmp_path / "sz"
+    subprocess.run([cc, "-I", str(ROOT / "include"), str(src), "-o", str(exe)], check=True)
+    got = [int(v) for v in subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split()]
+    want = [C.sizeof(N.SlabDesc), C.sizeof(N.SolveOpts), C.sizeof(N.SolveStats), C.sizeof(N.BatchItem),
+            N.BatchItem.stats.offset, N.BatchItem.status.offset, N.SolveOpts.preconditioner.offset]
+    assert got == want
