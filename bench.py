@@ -283,9 +283,9 @@ def run_ours(args, wl, rank, world, local_rank):
     import ctypes as C
 
     ns = geom.N_z * geom.M * geom.M
-    hy = Ly // 2 + 1
+    # octant kernel spectrum (kz <= Lz/2, ky <= Ly/2, kx <= Lx/2; 45 entries, complex64)
     E = 45
-    b_alg = E * hy * Lx * Lz * 8 + 4 * ns * 8 + 2 * 9 * ns * 8
+    b_alg = E * (Lz // 2 + 1) * (Ly // 2 + 1) * (Lx // 2 + 1) * 8 + 4 * ns * 8 + 2 * 9 * ns * 8
     b_alg_ref = 81 * Lz * Lx * Ly * 8 + 4 * ns * 8 + 2 * 9 * ns * 8
     # the SoA matvec (no layout conversion): measured through the internal launcher
     y32 = torch.empty_like(x32)
