@@ -49,6 +49,9 @@ WORKLOADS = {
     # 256 uneven slabs: M ~ U{16,24,...,96}, N_z ~ U{4..24}, ka ~ U[0.1,1], theta ~ U[0,40 deg],
     # P/SV 50/50, i.i.d. +-20 %, aperiodic; one msc_batch_solve call per step
     "cfg3": dict(batch=256, tol=1e-8, periodic=False, mat=("iid", 0.20)),
+    # held-out 64x64x16 GRF slabs of the learned-preconditioner distribution: correlation
+    # length U[2,6] cells, std U[0.1,0.3], ka U[0.3,1], angle U[0,40 deg], P/SV; aperiodic
+    "cfg4": dict(precond_eval=8, M=64, N_z=16, tol=1e-8, periodic=False),
 }
 ALPHA, BETA, RHO, A = 3000.0, 1732.0, 2500.0, 1.0
 
@@ -454,6 +457,92 @@ def run_batch(args, wl, rank, world, local_rank) -> int:
     return 0
 
 
+def cfg4_problem(wl: dict, seed: int):
+    from multiplescatteringcalculations_b200 import ReferenceMedium, SlabGeometry, gaussian_random_field_material
+
+    r = np.random.default_rng(seed)
+    ell, std, ka = r.uniform(2, 6), r.uniform(0.1, 0.3), r.uniform(0.3, 1.0)
+    ref = ReferenceMedium(ALPHA, BETA, RHO)
+    g = SlabGeometry(wl["M"], wl["N_z"], A)
+    mat = gaussian_random_field_material(g, ref, correlation_length=ell, std=std, seed=seed)
+    th = r.uniform(0, np.deg2rad(40))
+    wave = "P" if r.random() < 0.5 else "S"
+    return ref, g, mat, np.array([np.cos(th), np.sin(th), 0.0]), ka * BETA / A, wave, (ell, std, ka)
+
+
+def run_precond_eval(args, wl, rank, world, local_rank) -> int:
+    """cfg4: per held-out slab, the time to 1e-8 (FP64 true residual) of plain FP64
+    GMRES(30), mixed-precision GMRES(30) and mixed-precision flexible GMRES(30) with the
+    near-field preconditioner; each solve includes T0, G0, incident and R_PP. The line's
+    value is the preconditioned mixed solver's throughput over the slabs."""
+    import torch
+
+    from multiplescatteringcalculations_b200 import SlabPlan, _native
+
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    lib = _native.load()
+    variants = {"fp64": dict(precision="fp64", preconditioner=None),
+                "mixed": dict(precision="mixed", preconditioner=None),
+                "mixed_nearfield": dict(precision="mixed", preconditioner="nearfield")}
+    stream = torch.cuda.current_stream(dev)
+    rows = []
+    n0 = lib.msc_launch_count()
+    with ClockSampler(local_rank) as clk:
+        for k in range(wl["precond_eval"]):
+            ref, g, mat, kh, om, wave, par = cfg4_problem(wl, seed=5000 + 100 * rank + k)
+            plan = SlabPlan(g, ref, periodic=False, device=dev)
+            md = type(mat)(torch.from_numpy(mat.Dlambda).to(dev), torch.from_numpy(mat.Dmu).to(dev),
+                           torch.from_numpy(mat.Drho).to(dev), ref)
+            row = {"ell": par[0], "std": par[1], "ka": par[2], "wave": wave}
+            for name, v in variants.items():
+                def step():
+                    plan.build_t0(md, om)
+                    plan.build_g0(om)
+                    psi0 = plan.incident(om, kh, wave)
+                    if v["preconditioner"]:
+                        plan.set_nearfield()
+                    x, st = plan.solve(psi0, tol=wl["tol"], max_iter=6000, restart=30, precision=v["precision"],
+                                       preconditioner=v["preconditioner"])
+                    plan.rpp_periodic(x, om)
+                    return st
+                for _ in range(max(1, args.warmup)):
+                    step()
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                torch.cuda.synchronize()
+                e0.record(stream)
+                for _ in range(args.steps):
+                    st = step()
+                e1.record(stream)
+                torch.cuda.synchronize()
+                row[name] = {"ms": e0.elapsed_time(e1) / args.steps, "n_matvec": st["n_matvec"],
+                             "n_precond": st["n_precond"], "residual": st["residual"],
+                             "pc_fallback": st["pc_fallback"]}
+            rows.append(row)
+            plan.close()
+    launches = lib.msc_launch_count() - n0
+    ok = all(r[n]["residual"] <= wl["tol"] for r in rows for n in variants)
+    t = {n: float(np.sum([r[n]["ms"] for r in rows])) for n in variants}
+    line = {
+        "metric": METRIC, "value": 1e3 * len(rows) / t["mixed_nearfield"], "unit": "solves/s", "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": t["mixed_nearfield"] / len(rows),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "c64+c128", "data": "synthetic",
+        "config": {"workload": "cfg4", "lattice": f"{wl['M']}x{wl['M']}x{wl['N_z']}", "slabs": len(rows),
+                   "ell": "U[2,6]", "std": "U[0.1,0.3]", "ka": "U[0.3,1]", "incidence_deg": "U[0,40]",
+                   "wave": "P/SV", "tol": wl["tol"], "periodic": False, "restart": 30,
+                   "precond": "near-field Neumann polynomial, degree 2 (no trained network)",
+                   "l2": "inputs larger than L2 (G0 spectrum build per solve)"},
+        "gpu_launches": int(launches), "all_converged": ok,
+        "ms_per_solve": {n: t[n] / len(rows) for n in variants},
+        "speedup_vs_fp64_plain": {n: t["fp64"] / t[n] for n in variants},
+        "per_slab": rows,
+        "clocks": clk.summary(),
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    return 0
+
+
 def run_matvecs(wl: dict, n: int) -> int:
     """Plan + T0 + G0 of the workload, then 3 untimed and n timed complex64 operator
     applications through msc_matvec (each: 2 layout transposes and the matvec
@@ -510,6 +599,8 @@ def main(argv=None) -> int:
         return run_reference(args, wl, rank, world)
     if args.matvec_only:
         return run_matvecs(wl, args.matvec_only)
+    if "precond_eval" in wl:
+        return run_precond_eval(args, wl, rank, world, local_rank)
     if "batch" in wl:
         if world > 1:
             import datetime

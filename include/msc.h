@@ -136,7 +136,9 @@ int msc_matvec_noalloc(msc_plan* plan, const void* x, void* y, int precision);
  * truncated Neumann series of (I - G_nn T0)^{-1}. msc_set_nearfield sets the degree
  * L in [1, 6], the coefficients (2(L+1) doubles re/im, NULL = all ones) and
  * per-layer block corrections (L x 27 x 81 complex128 re/im, NULL = none); the
- * settings hold until changed and survive build_g0. */
+ * settings hold until changed and survive build_g0. Entries that the mirror symmetry
+ * of the lattice sets to zero (where the offset has a zero component along an axis,
+ * those odd under that axis' reflection) are not applied, corrections included. */
 int msc_set_nearfield(msc_plan* plan, int degree, const double* coef, const double* dblocks);
 /* The 27 x 9 x 9 blocks G_nn (complex128 re/im into out[2 x 27 x 81]) of the last
  * build_g0; offset o = ((dz+1) 3 + dx+1) 3 + dy+1, out block a,b: y_a += G_ab tau_b(v - o). */

@@ -226,6 +226,7 @@ int msc_plan_destroy(msc_plan* pl) {
   gmres_free(pl);
   if (pl->nf) {
     dfree(pl, pl->nf->g64_dev);
+    dfree(pl, pl->nf->g32_dev);
     dfree(pl, pl->nf->tmp32);
     dfree(pl, pl->nf->tmp64);
     delete pl->nf;

@@ -542,9 +542,9 @@ void gmres_free(msc_plan* pl) {
 // Returns the number of matvecs used in *n_mv and the final estimate in *res.
 //
 // With `pc` the solve is flexible GMRES with the near-field preconditioner on the
-// right: z_j = P(v_j), w = A z_j, x += Z y. A cycle that leaves the residual
-// estimate above 0.99 of its initial value turns the preconditioner off for the
-// rest of the solve (*pc_off = 1): plain GMRES is the fallback.
+// right: z_j = P(v_j), w = A z_j, x += Z y. A cycle that does not reduce the
+// residual estimate turns the preconditioner off for the rest of the solve
+// (*pc_off = 1): plain GMRES is the fallback.
 template <typename T>
 static int gmres_core(msc_plan* pl, int m, const cx<T>* rhs, cx<T>* x, bool x_zero, double tol_abs, int max_mv,
                       int* n_mv, double* res, int* status, bool cgs2, bool pc, int* n_pc, int* pc_off) {
@@ -633,6 +633,7 @@ static int gmres_core(msc_plan* pl, int m, const cx<T>* rhs, cx<T>* x, bool x_ze
         gr.cgs2 = cgs2;
         gr.gen = pl->gen;
       }
+      if (use_pc) MSC_TRY(nearfield_refresh(pl));  // new blocks (a new frequency) into the same buffers
       MSC_CUDA(cudaGraphLaunch(gr.exec, pl->stream));
       ::msc::note_launch();
       MSC_CUDA(cudaMemcpyAsync(&gw->hstate[0], st, sizeof(GState), cudaMemcpyDeviceToHost, pl->stream));
@@ -688,9 +689,10 @@ static int gmres_core(msc_plan* pl, int m, const cx<T>* rhs, cx<T>* x, bool x_ze
       *status = MSC_OK;
       break;
     }
-    // A preconditioned cycle that leaves the residual estimate above 0.99 of its
-    // start (a breakdown of A P included) turns the preconditioner off.
-    if (use_pc && cur.res > 0.99 * cur.beta) {
+    // A preconditioned cycle that fails to reduce the residual estimate at all (a
+    // breakdown of A P included) turns the preconditioner off; slow progress, which
+    // plain GMRES shows as well on hard slabs, does not.
+    if (use_pc && cur.res >= (1.0 - 1e-6) * cur.beta) {
       use_pc = false;
       *pc_off = 1;
       continue;

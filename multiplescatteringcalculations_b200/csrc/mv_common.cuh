@@ -7,6 +7,12 @@
 
 namespace msc {
 
+// Reflection parity of the 9 DOF [u_z, u_x, u_y, e_zz, e_xx, e_yy, 2e_xy, 2e_zy,
+// 2e_zx]: bit 0 odd under x -> -x, bit 1 under y -> -y, bit 2 under z -> -z.
+__host__ __device__ constexpr int dof_parity(int c) {
+  return c == 0 ? 4 : c == 1 ? 1 : c == 2 ? 2 : c < 6 ? 0 : c == 6 ? 3 : c == 7 ? 6 : 5;
+}
+
 // Lines per tile so that one tile row is 128 bytes: 16 (complex64) / 8 (complex128).
 template <typename T> struct Tile { static constexpr int W = 128 / (int)sizeof(cx<T>); };
 

@@ -20,12 +20,6 @@
 
 namespace msc {
 
-// Reflection parity of the 9 DOF [u_z, u_x, u_y, e_zz, e_xx, e_yy, 2e_xy, 2e_zy,
-// 2e_zx]: bit 0 odd under x -> -x, bit 1 under y -> -y, bit 2 under z -> -z.
-__host__ __device__ constexpr int dof_parity(int c) {
-  return c == 0 ? 4 : c == 1 ? 1 : c == 2 ? 2 : c < 6 ? 0 : c == 6 ? 3 : c == 7 ? 6 : 5;
-}
-
 template <typename C> __device__ __forceinline__ void reflect(C* v, int f) {
 #pragma unroll
   for (int c = 0; c < 9; ++c)

@@ -7,8 +7,15 @@
 // A block stages tau = T0 x on its tile plus a one-voxel halo in shared memory
 // (zero outside the slab) and each thread accumulates the 27 x 81 complex
 // products of its voxels (the self offset holds zero for G_nn and a learned
-// pointwise block for a corrected layer). In complex64 the blocks are a __grid_constant__ kernel
-// parameter, so every FMA takes its block entry from the constant bank.
+// pointwise block for a corrected layer). The block's 27 x 81 blocks are staged in
+// shared memory next to the halo tile and read as broadcasts.
+//
+// Mirror symmetry: where the offset has a zero component along an axis, the block is
+// invariant under that axis' reflection, so its entries odd under it vanish
+// (K_ab = 0 when dof_parity(a) ^ dof_parity(b) has the axis' bit). The kernel skips
+// those entries at compile time (1338 of the 2187 products remain); block corrections
+// are applied within the same pattern.
+#include <type_traits>
 #include <vector>
 
 #include "mv_common.cuh"
@@ -47,6 +54,7 @@ int nearfield_extract(msc_plan* pl, const double2* Ks, double scale) {
   if (!pl->nf) pl->nf = new NearField();
   NearField* nf = pl->nf;
   MSC_TRY(dalloc(pl, nf->g64_dev, sizeof(double2) * (size_t)(NF_MAXL + 1) * NF_OFFS * 81));
+  MSC_TRY(dalloc(pl, nf->g32_dev, sizeof(float2) * (size_t)(NF_MAXL + 1) * NF_OFFS * 81));
   double2* dst = (double2*)nf->g64_dev.p;
   k_nf_extract<<<ceil_div(NF_OFFS * 81, 256), 256, 0, pl->stream>>>(Ks, pl->g, pl->E, 1.0 / scale, dst);
   ::msc::note_launch();
@@ -60,26 +68,34 @@ int nearfield_extract(msc_plan* pl, const double2* Ks, double scale) {
 }
 
 // ---- stencil ------------------------------------------------------------------------------
-template <typename T> struct NFTile;
-template <> struct NFTile<float> {  // 256 threads, two voxels each along z
-  static constexpr int TZ = 4, TX = 8, TY = 16, VPT = 2;
-};
-template <> struct NFTile<double> {
+// Tile of 2 layers x 8 x 16 voxels, one voxel per thread: 256 threads; a 64 x 64 x 16
+// slab gives 256 blocks, one wave at two blocks per SM (halo tile 4 x 10 x 18 voxels).
+template <typename T> struct NFTile {
   static constexpr int TZ = 2, TX = 8, TY = 16, VPT = 1;
+  static constexpr int NT = (TZ / VPT) * TX * TY;
 };
 
-template <typename T, typename GF>
+template <typename T>
 __device__ __forceinline__ void nf_body(const cx<T>* __restrict__ x, const double* scale, const cx<T>* __restrict__ t4,
                                         cx<T>* __restrict__ h, cx<T>* __restrict__ acc, cx<T> ch, cx<T> c0, int init,
-                                        GF gf, const Geo& g) {
+                                        const cx<T>* __restrict__ G, const Geo& g) {
   using C = cx<T>;
   using TL = NFTile<T>;
   constexpr int TZ = TL::TZ, TX = TL::TX, TY = TL::TY, VPT = TL::VPT;
   constexpr int HZ = TZ + 2, HX = TX + 2, HY = TY + 2, HALO = HZ * HX * HY;
   constexpr int NT = (TZ / VPT) * TX * TY;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  C* tau = reinterpret_cast<C*>(smem_raw);  // [9][HALO]
+  // blocks: complex128 as they are; complex64 as pairs (g.x, g.x, g.y, g.y) for the
+  // paired FP32 FMAs
+  using GE = typename std::conditional<sizeof(T) == 4, float4, double2>::type;
+  GE* Gs = reinterpret_cast<GE*>(smem_raw);                  // [27][81]
+  C* tau = reinterpret_cast<C*>(Gs + NF_OFFS * 81);          // [9][HALO]
   const int tid = threadIdx.x;
+  for (int i = tid; i < NF_OFFS * 81; i += NT) {
+    const C v = __ldg(G + i);
+    if constexpr (sizeof(T) == 4) Gs[i] = make_float4(v.x, v.x, v.y, v.y);
+    else Gs[i] = v;
+  }
   const int nxb = (g.M + TX - 1) / TX;
   const int y0 = blockIdx.x * TY, x0 = (blockIdx.y % nxb) * TX, z0 = (blockIdx.y / nxb) * TZ;
   const T s = scale ? (T)(*scale) : (T)1;
@@ -119,6 +135,7 @@ __device__ __forceinline__ void nf_body(const cx<T>* __restrict__ x, const doubl
 #pragma unroll
   for (int o = 0; o < NF_OFFS; ++o) {
     const int dz = o / 9 - 1, dx = (o / 3) % 3 - 1, dy = o % 3 - 1;
+    const int zmask = (dx == 0 ? 1 : 0) | (dy == 0 ? 2 : 0) | (dz == 0 ? 4 : 0);
 #pragma unroll
     for (int p = 0; p < VPT; ++p) {
       // source voxel v - o in halo coordinates
@@ -126,10 +143,28 @@ __device__ __forceinline__ void nf_body(const cx<T>* __restrict__ x, const doubl
       C tb[9];
 #pragma unroll
       for (int b = 0; b < 9; ++b) tb[b] = tau[b * HALO + hi];
+      if constexpr (sizeof(T) == 4) {
+        float2 tr[9];
 #pragma unroll
-      for (int a = 0; a < 9; ++a)
+        for (int b = 0; b < 9; ++b) tr[b] = make_float2(-tb[b].y, tb[b].x);
 #pragma unroll
-        for (int b = 0; b < 9; ++b) fma_(out[p][a], gf(o * 81 + a * 9 + b), tb[b]);
+        for (int a = 0; a < 9; ++a)
+#pragma unroll
+          for (int b = 0; b < 9; ++b) {
+            if ((dof_parity(a) ^ dof_parity(b)) & zmask) continue;  // zero by symmetry
+            const float4 m = Gs[o * 81 + a * 9 + b];
+            out[p][a] = __ffma2_rn(make_float2(m.x, m.y), tb[b], out[p][a]);
+            out[p][a] = __ffma2_rn(make_float2(m.z, m.w), tr[b], out[p][a]);
+          }
+      } else {
+#pragma unroll
+        for (int a = 0; a < 9; ++a)
+#pragma unroll
+          for (int b = 0; b < 9; ++b) {
+            if ((dof_parity(a) ^ dof_parity(b)) & zmask) continue;  // zero by symmetry
+            fma_(out[p][a], Gs[o * 81 + a * 9 + b], tb[b]);
+          }
+      }
     }
   }
   const int yy = y0 + vy, xx = x0 + vx;
@@ -153,12 +188,12 @@ __device__ __forceinline__ void nf_body(const cx<T>* __restrict__ x, const doubl
   }
 }
 
-__global__ void __launch_bounds__(256) k_nf32(const float2* __restrict__ x, const double* scale,
+__global__ void __launch_bounds__(256, 2) k_nf32(const float2* __restrict__ x, const double* scale,
                                               const float2* __restrict__ t4, float2* __restrict__ h,
                                               float2* __restrict__ acc, float2 ch, float2 c0, int init,
-                                              const __grid_constant__ NFStencil32 S, Geo g, const int* done) {
+                                              const float2* __restrict__ G, Geo g, const int* done) {
   if (done && *done) return;
-  nf_body<float>(x, scale, t4, h, acc, ch, c0, init, [&](int i) { return S.g[i]; }, g);
+  nf_body<float>(x, scale, t4, h, acc, ch, c0, init, G, g);
 }
 
 __global__ void __launch_bounds__(256) k_nf64(const double2* __restrict__ x, const double* scale,
@@ -166,29 +201,28 @@ __global__ void __launch_bounds__(256) k_nf64(const double2* __restrict__ x, con
                                               double2* __restrict__ acc, double2 ch, double2 c0, int init,
                                               const double2* __restrict__ G, Geo g, const int* done) {
   if (done && *done) return;
-  nf_body<double>(x, scale, t4, h, acc, ch, c0, init, [&](int i) { return __ldg(G + i); }, g);
+  nf_body<double>(x, scale, t4, h, acc, ch, c0, init, G, g);
 }
 
-// Rebuild the per-layer blocks g64 + dg[l] (complex64 parameters, complex128 device copy).
+// Upload the per-layer blocks g64 + dg[l] (complex128 and complex64) to the device.
 int nearfield_refresh(msc_plan* pl) {
   NearField* nf = pl->nf;
   if (!nf->dirty) return MSC_OK;
   const int L = std::max(1, std::min(nf->L, NF_MAXL));
-  std::vector<double2> all((size_t)L * NF_OFFS * 81);
-  nf->s32.resize(L);
-  for (int l = 0; l < L; ++l) {
+  const size_t nb = (size_t)L * NF_OFFS * 81;
+  nf->h64.resize(nb);
+  nf->h32.resize(nb);
+  for (int l = 0; l < L; ++l)
     for (int i = 0; i < NF_OFFS * 81; ++i) {
       double2 v = nf->g64[i];
       if (!nf->dg.empty()) v = v + nf->dg[(size_t)l * NF_OFFS * 81 + i];
-      all[(size_t)l * NF_OFFS * 81 + i] = v;
-      nf->s32[l].g[i] = make_float2((float)v.x, (float)v.y);
+      nf->h64[(size_t)l * NF_OFFS * 81 + i] = v;
+      nf->h32[(size_t)l * NF_OFFS * 81 + i] = make_float2((float)v.x, (float)v.y);
     }
-  }
-  MSC_CUDA(cudaMemcpyAsync(nf->g64_dev.p, all.data(), sizeof(double2) * all.size(), cudaMemcpyHostToDevice,
-                           pl->stream));
+  MSC_CUDA(cudaMemcpyAsync(nf->g64_dev.p, nf->h64.data(), sizeof(double2) * nb, cudaMemcpyHostToDevice, pl->stream));
+  MSC_CUDA(cudaMemcpyAsync(nf->g32_dev.p, nf->h32.data(), sizeof(float2) * nb, cudaMemcpyHostToDevice, pl->stream));
   MSC_CUDA(cudaStreamSynchronize(pl->stream));
   nf->dirty = false;
-  ++pl->gen;
   return MSC_OK;
 }
 
@@ -209,7 +243,8 @@ int nearfield_apply(msc_plan* pl, const cx<T>* v, const double* scale, cx<T>* z,
   const cx<T>* t4 = (const cx<T>*)(sizeof(T) == 8 ? pl->t4_64.p : pl->t4_32.p);
   const int nxb = (g.M + TL::TX - 1) / TL::TX;
   dim3 grid((unsigned)((g.M + TL::TY - 1) / TL::TY), (unsigned)(nxb * ((g.Nz + TL::TZ - 1) / TL::TZ)));
-  const size_t sm = sizeof(cx<T>) * 9 * (TL::TZ + 2) * (TL::TX + 2) * (TL::TY + 2);
+  const size_t sm = (size_t)NF_OFFS * 81 * (sizeof(T) == 4 ? 16 : 16) +
+                    sizeof(cx<T>) * 9 * (TL::TZ + 2) * (TL::TX + 2) * (TL::TY + 2);
   const int L = std::max(1, std::min(nf->L, NF_MAXL));
   const void* kern = sizeof(T) == 8 ? (const void*)k_nf64 : (const void*)k_nf32;
   MSC_CUDA(prep_kernel(kern));
@@ -221,11 +256,12 @@ int nearfield_apply(msc_plan* pl, const cx<T>* v, const double* scale, cx<T>* z,
     const cx<T> ch = mk<T>((T)nf->coef[l].x, (T)nf->coef[l].y);
     const int init = l == 1 ? 1 : 0;
     if constexpr (sizeof(T) == 4) {
-      k_nf32<<<grid, 256, sm, pl->stream>>>((const float2*)in, sc, (const float2*)t4, (float2*)h, (float2*)z,
+      k_nf32<<<grid, TL::NT, sm, pl->stream>>>((const float2*)in, sc, (const float2*)t4, (float2*)h, (float2*)z,
                                              make_float2((float)ch.x, (float)ch.y),
-                                             make_float2((float)c0.x, (float)c0.y), init, nf->s32[l - 1], g, done);
+                                             make_float2((float)c0.x, (float)c0.y), init,
+                                             (const float2*)nf->g32_dev.p + (size_t)(l - 1) * NF_OFFS * 81, g, done);
     } else {
-      k_nf64<<<grid, 256, sm, pl->stream>>>((const double2*)in, sc, (const double2*)t4, (double2*)h, (double2*)z,
+      k_nf64<<<grid, TL::NT, sm, pl->stream>>>((const double2*)in, sc, (const double2*)t4, (double2*)h, (double2*)z,
                                              make_double2((double)ch.x, (double)ch.y),
                                              make_double2((double)c0.x, (double)c0.y), init,
                                              (const double2*)nf->g64_dev.p + (size_t)(l - 1) * NF_OFFS * 81, g, done);

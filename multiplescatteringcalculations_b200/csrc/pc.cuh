@@ -14,11 +14,6 @@ namespace msc {
 constexpr int NF_OFFS = 27;   // stencil offsets, o = ((dz + 1) * 3 + dx + 1) * 3 + dy + 1
 constexpr int NF_MAXL = 6;    // polynomial degree limit
 
-// Stencil blocks of one layer in complex64: y_a(v) += g[o][a][b] tau_b(v - o).
-struct NFStencil32 {
-  float2 g[NF_OFFS * 81];
-};
-
 // Per-plan state of the preconditioner.
 struct NearField {
   NearField() {
@@ -29,8 +24,12 @@ struct NearField {
   double2 coef[NF_MAXL + 1];   // c_0..c_L
   std::vector<double2> g64;    // [27][9][9] physical near-field blocks (host copy)
   std::vector<double2> dg;     // [L][27][9][9] learned block corrections (empty = none)
-  DBuf g64_dev;                // [L][27][81] complex128 blocks per layer (fp64 path)
-  std::vector<NFStencil32> s32;  // complex64 blocks per layer (kernel parameters)
+  // Per-layer blocks g64 + dg[l] on the device, [L][27][81], y_a(v) += g[o][a][b] tau_b(v - o).
+  // The kernels read them through these pointers, so a captured solver graph stays valid
+  // when the blocks change (a new frequency): only the buffers' contents are refreshed.
+  DBuf g64_dev, g32_dev;
+  std::vector<double2> h64;    // host staging of the refresh
+  std::vector<float2> h32;
   DBuf tmp32, tmp64;           // two field-size work vectors per precision
   bool dirty = true;           // layer blocks to rebuild from g64, dg
 };
@@ -38,7 +37,8 @@ struct NearField {
 // Extract the near-field blocks from the spatial kernel of the G0 build (values
 // times `scale`).
 int nearfield_extract(msc_plan* pl, const double2* Ks_spatial, double scale);
-// Rebuild the per-layer blocks after a change (synchronises the plan's stream).
+// Upload the per-layer blocks after a change (synchronises the plan's stream; must not
+// run while a graph is being captured).
 int nearfield_refresh(msc_plan* pl);
 // z = P(s v), s = *scale (1 when null); `done` as in the matvec.
 template <typename T>

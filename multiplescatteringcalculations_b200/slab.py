@@ -303,7 +303,8 @@ class SlabPlan:
         """Near-field polynomial preconditioner P = sum_l c_l S_l ... S_1 with
         S_l x = (G_nn + dG_l)(T0 x): ``coef`` (degree + 1 complex, default all ones:
         the truncated Neumann series), ``dblocks`` (degree x 27 x 9 x 9 complex block
-        corrections, default none)."""
+        corrections, default none; entries outside the lattice's mirror-symmetry
+        pattern are not applied)."""
         c = None
         if coef is not None:
             cc = np.asarray(coef, dtype=np.complex128).ravel()
@@ -510,10 +511,16 @@ def compute_slab_scattering_gpu(
             stacklevel=2,
         )
     t4 = plan.t0_scalars()
-    psi = x.cpu().numpy()
+    # device -> host through pinned buffers of torch's caching host allocator (one
+    # synchronisation; the returned arrays own their buffers)
+    host = [torch.empty(t.shape, dtype=t.dtype, pin_memory=True) for t in (x, psi0, t4)]
+    for h, t in zip(host, (x, psi0, t4)):
+        h.copy_(t, non_blocking=True)
+    torch.cuda.current_stream(plan.device).synchronize()
+    psi_h, psi0_h, t4_h = host
     res = SlabResult(
-        psi=psi,
-        psi0=psi0.cpu().numpy(),
+        psi=psi_h.numpy(),
+        psi0=psi0_h.numpy(),
         geometry=geometry,
         material=material,
         omega=float(omega),
@@ -522,7 +529,7 @@ def compute_slab_scattering_gpu(
         n_gmres_iter=int(st["n_matvec"]),
         gmres_residual=float(st["residual"]),
         periodic=bool(periodic),
-        t0=t4.cpu().numpy(),
+        t0=t4_h.numpy(),
         bloch=bool(bloch),
         stats=st,
     )

@@ -789,10 +789,28 @@ def nearfield_blocks(M, N_z, a, omega, alpha, beta, rho, *, volume_averaged=Fals
     return out
 
 
+_DOF_PARITY = np.array([4, 1, 2, 0, 0, 0, 3, 6, 5])  # bits: odd under x, y, z reflection
+
+
+def nearfield_symmetry_mask():
+    """(27, 9, 9) mask of the block entries the mirror symmetry allows: entry (a, b) of an
+    offset with a zero component along an axis vanishes when the DOF pair is odd under
+    that axis' reflection."""
+    mask = np.ones((27, 9, 9), dtype=bool)
+    odd = _DOF_PARITY[:, None] ^ _DOF_PARITY[None, :]
+    for o in range(27):
+        dz, dx, dy = o // 9 - 1, (o // 3) % 3 - 1, o % 3 - 1
+        zm = (1 if dx == 0 else 0) | (2 if dy == 0 else 0) | (4 if dz == 0 else 0)
+        mask[o] = (odd & zm) == 0
+    return mask
+
+
 def nearfield_stencil(x, t4, blocks, M, N_z):
     """y(v) = sum_o G_o (T0 x)(v - o) over the 27 offsets (the self block included:
-    zero for the kernel, a pointwise block for a corrected layer), zero outside the
-    slab; x flat (N_z, M, M, 9)."""
+    zero for the kernel, a pointwise block for a corrected layer), with the entries
+    outside the mirror-symmetry pattern dropped, zero outside the slab; x flat
+    (N_z, M, M, 9)."""
+    blocks = blocks * nearfield_symmetry_mask()
     tau = apply_t0(t4, x.reshape(N_z, M, M, 9))
     tp = np.zeros((N_z + 2, M + 2, M + 2, 9), dtype=complex)
     tp[1:-1, 1:-1, 1:-1] = tau
