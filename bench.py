@@ -175,7 +175,7 @@ def run_reference(args, wl, rank, world):
 def _cfg_desc(wl):
     return {"lattice": f"{wl['M']}x{wl['M']}x{wl['N_z']}", "ka": wl["ka"], "incidence_deg": wl["angle"],
             "wave": wl["wave"], "material": list(wl["mat"]), "tol": wl["tol"], "periodic": wl["periodic"],
-            "restart": 30, "l2": "inputs larger than L2 (G0 spectrum build and matvec stream > 126 MB per step)"}
+            "l2": "inputs larger than L2 (G0 spectrum build and matvec stream > 126 MB per step)"}
 
 
 def run_ours(args, wl, rank, world, local_rank):
@@ -200,7 +200,7 @@ def run_ours(args, wl, rank, world, local_rank):
         psi0 = plan.incident(omega, k_hat, wl["wave"])
         if args.precond != "none":
             plan.set_nearfield()
-        x, st = plan.solve(psi0, tol=wl["tol"], max_iter=1000, restart=30, precision="mixed",
+        x, st = plan.solve(psi0, tol=wl["tol"], max_iter=1000, restart=args.restart, precision="mixed",
                            preconditioner=None if args.precond == "none" else args.precond)
         stats.update(st)
         stats["rpp"] = plan.rpp_periodic(x, omega)
@@ -246,7 +246,7 @@ def run_ours(args, wl, rank, world, local_rank):
         plan.build_t0(mat_dev, omega)
         plan.build_g0(omega)
         psi0 = plan.incident(omega, k_hat, wl["wave"])
-        return plan.solve(psi0, tol=wl["tol"], max_iter=1000, restart=30, precision="fp64")[1]
+        return plan.solve(psi0, tol=wl["tol"], max_iter=1000, restart=args.restart, precision="fp64")[1]
 
     step64()
     torch.cuda.synchronize()
@@ -268,7 +268,7 @@ def run_ours(args, wl, rank, world, local_rank):
         psi0 = plan.incident(omega, k_hat, wl["wave"])
         if other != "none":
             plan.set_nearfield()
-        return plan.solve(psi0, tol=wl["tol"], max_iter=1000, restart=30, precision="mixed",
+        return plan.solve(psi0, tol=wl["tol"], max_iter=1000, restart=args.restart, precision="mixed",
                           preconditioner=None if other == "none" else other)[1]
 
     step_other()
@@ -317,7 +317,7 @@ def run_ours(args, wl, rank, world, local_rank):
         "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "c64+c128", "data": "synthetic",
-        "config": {"workload": args.workload, **_cfg_desc(wl), "fft": [Lz, Lx, Ly]},
+        "config": {"workload": args.workload, **_cfg_desc(wl), "restart": args.restart, "fft": [Lz, Lx, Ly]},
         "gpu_launches": int(launches),
         "solve": {"n_matvec": stats["n_matvec"], "n_matvec64": stats["n_matvec64"], "n_outer": stats["n_outer"],
                   "n_precond": stats["n_precond"], "pc_fallback": stats["pc_fallback"], "precond": args.precond,
@@ -585,6 +585,7 @@ def main(argv=None) -> int:
     ap.add_argument("--precond", default="none", choices=["none", "nearfield"],
                     help="right preconditioner of the timed mixed-precision solves")
     ap.add_argument("--workers", type=int, default=0, help="cfg3: batch worker threads (0 = autotune)")
+    ap.add_argument("--restart", type=int, default=30, help="GMRES restart length of the timed solves")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--solve-only", action="store_true", help="timed solves only (for profiler launch lists)")

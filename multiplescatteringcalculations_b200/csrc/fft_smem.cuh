@@ -296,4 +296,45 @@ __device__ __forceinline__ C* fft_tile_ct(C* a, C* b, const C* tw, int tid) {
   return (Pow2Plan<L>::NSTAGES % 2 == 0) ? a : b;
 }
 
+// ---- register-resident engine ------------------------------------------------------
+// One thread transforms one line of L points held in registers (the same Stockham
+// stages as above, every index a compile-time constant, so the stages are register
+// renamings); twiddles come from the block's shared table tw[t] = exp(-2 pi i t / L).
+// An output the caller never reads is not computed (dead code).
+template <int L, int S, int DIR, typename C>
+__device__ __forceinline__ void fft_reg_stages(C* v, const C* __restrict__ tw) {
+  using PL = Pow2Plan<L>;
+  if constexpr (S < PL::NSTAGES) {
+    constexpr int R = PL::radix(S), NS = PL::ns(S), NB = L / R, TSTEP = L / (NS * R);
+    C out[L];
+#pragma unroll
+    for (int j = 0; j < NB; ++j) {
+      const int kk = j % NS;
+      C u[R];
+#pragma unroll
+      for (int r = 0; r < R; ++r) u[r] = v[j + r * NB];
+      if (kk != 0) {
+#pragma unroll
+        for (int r = 1; r < R; ++r) {
+          C w = tw[r * kk * TSTEP];
+          if (DIR > 0) w.y = -w.y;
+          u[r] = u[r] * w;
+        }
+      }
+      Dft<R, DIR, C>::run(u);
+      const int idxD = (j - kk) * R + kk;
+#pragma unroll
+      for (int r = 0; r < R; ++r) out[idxD + r * NS] = u[r];
+    }
+#pragma unroll
+    for (int i = 0; i < L; ++i) v[i] = out[i];
+    fft_reg_stages<L, S + 1, DIR>(v, tw);
+  }
+}
+
+template <int L, int DIR, typename C>
+__device__ __forceinline__ void fft_reg(C* v, const C* __restrict__ tw) {
+  fft_reg_stages<L, 0, DIR>(v, tw);
+}
+
 }  // namespace msc

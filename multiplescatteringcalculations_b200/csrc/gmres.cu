@@ -99,7 +99,7 @@ static size_t hess_bytes(int m) {
 // ---- block reduction of NV complex partials; last block reduces over blocks -----------
 // sums[i] (i < nv) are this thread's partials. The final values land in out[i].
 template <int NV>
-__device__ void reduce_to(double2* sums, int nv, double2* __restrict__ part, int* counter, double2* out) {
+__device__ bool reduce_to(double2* sums, int nv, double2* __restrict__ part, int* counter, double2* out) {
   __shared__ double2 sh[NTH / 32][NV];
   __shared__ bool last;
   const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
@@ -124,7 +124,7 @@ __device__ void reduce_to(double2* sums, int nv, double2* __restrict__ part, int
   __syncthreads();
   if (threadIdx.x == 0) last = (atomicAdd(counter, 1) == (int)gridDim.x - 1);
   __syncthreads();
-  if (!last) return;
+  if (!last) return false;
   __threadfence();
   for (int i = w; i < nv; i += NTH / 32) {
     double2 v = make_double2(0, 0);
@@ -136,6 +136,7 @@ __device__ void reduce_to(double2* sums, int nv, double2* __restrict__ part, int
     if (l == 0) out[i] = v;
   }
   if (threadIdx.x == 0) *counter = 0;
+  return true;
 }
 
 // Chunked multi-vector kernels. A block of NTH threads covers chunks of NTH*EPT
@@ -222,121 +223,26 @@ __global__ void __launch_bounds__(NTH) k_mdot(const cx<T>* __restrict__ V, size_
   reduce_rows(mine[0], nv, part, counter, out);
 }
 
-// w -= sum_i coef_i s_i V_i (i < nv); optionally out_norm.x = ||w||^2
-template <typename T, bool NORM>
-__global__ void __launch_bounds__(NTH) k_maxpy(const cx<T>* __restrict__ V, size_t n, int nv, const double* scale,
-                                               const double2* coef, cx<T>* __restrict__ w, double2* part, int* counter,
-                                               double2* out_norm, const int* done) {
-  if (done && *done) return;
-  __shared__ cx<T> cf[32];
-  if (threadIdx.x < 32) {
-    const int i = threadIdx.x;
-    const double s = (scale && i < nv) ? scale[i] : 1.0;
-    cf[i] = i < nv ? mk<T>((T)(s * coef[i].x), (T)(s * coef[i].y)) : czero<cx<T>>();
-  }
-  __syncthreads();
-  const size_t chunk = (size_t)NTH * EPT;
-  double nrm = 0.0;
-  for (size_t base = (size_t)blockIdx.x * chunk; base < n; base += (size_t)gridDim.x * chunk) {
-    cx<T> wr[EPT];
-#pragma unroll
-    for (int u = 0; u < EPT; ++u) {
-      const size_t k = base + (size_t)u * NTH + threadIdx.x;
-      wr[u] = k < n ? w[k] : czero<cx<T>>();
-    }
-    for (int i = 0; i < nv; ++i) {
-      const cx<T>* Vi = V + (size_t)i * n;
-      const cx<T> c = cf[i];
-#pragma unroll
-      for (int u = 0; u < EPT; ++u) {
-        const size_t k = base + (size_t)u * NTH + threadIdx.x;
-        if (k < n) {
-          const cx<T> v = Vi[k];
-          wr[u].x -= c.x * v.x - c.y * v.y;
-          wr[u].y -= c.x * v.y + c.y * v.x;
-        }
-      }
-    }
-#pragma unroll
-    for (int u = 0; u < EPT; ++u) {
-      const size_t k = base + (size_t)u * NTH + threadIdx.x;
-      if (k < n) {
-        w[k] = wr[u];
-        if (NORM) nrm += (double)wr[u].x * wr[u].x + (double)wr[u].y * wr[u].y;
-      }
-    }
-  }
-  if (NORM) {
-    double2 a[1] = {make_double2(nrm, 0.0)};
-    reduce_to<1>(a, 1, part, counter, out_norm);
-  }
-}
-
-// ||v||^2 -> out.x ; optionally also r = b - ax written first (when b != null)
-template <typename T>
-__global__ void __launch_bounds__(NTH) k_resid_norm(const cx<T>* __restrict__ b, const cx<T>* __restrict__ ax,
-                                                    cx<T>* __restrict__ r, size_t n, double2* part, int* counter,
-                                                    double2* out) {
-  double2 nrm = make_double2(0, 0);
-  for (size_t k = (size_t)blockIdx.x * NTH + threadIdx.x; k < n; k += (size_t)gridDim.x * NTH) {
-    cx<T> v;
-    if (ax) {
-      v = b[k] - ax[k];
-      r[k] = v;
-    } else {
-      v = b[k];
-    }
-    const double2 d = to_d(v);
-    nrm.x += d.x * d.x + d.y * d.y;
-  }
-  double2 a[1] = {nrm};
-  reduce_to<1>(a, 1, part, counter, out);
-}
-
-// cycle start: beta = sqrt(nrm), scale[0] = 1/beta, g = (beta, 0, ...)
-__global__ void k_cycle_init(GState* st, HessPtr h, int m, double tol_abs) {
-  if (threadIdx.x != 0) return;
-  const double beta = sqrt(h.nrm[0].x);
-  st->beta = beta;
-  st->res = beta;
-  st->tol_abs = tol_abs;
-  st->k = 0;
-  st->steps = 0;
-  st->status = MSC_OK;
-  st->converged = 0;
-  st->done = 0;
-  for (int i = 0; i <= m; ++i) h.g[i] = make_double2(0, 0);
-  h.g[0] = make_double2(beta, 0);
-  h.scale[0] = beta > 0 ? 1.0 / beta : 0.0;
-  if (!(beta == beta) || isinf(beta)) {
-    st->status = MSC_ERR_NONFINITE;
-    st->done = 1;
-  } else if (beta <= tol_abs || beta == 0.0) {
-    st->converged = 1;
-    st->done = 1;
-  }
-}
-
+// Column j of H from the CGS passes (h1, plus h2 for CGS2), rotations, residual
+// estimate, and (when the cycle ends) the back substitution. Run by one warp (the
+// last block of the normalising k_maxpy) right after ||w|| is known; the warp stages
+// the data in shared memory and lane 0 runs the sequential FP64 recurrences.
 __device__ __forceinline__ double cabs_(double2 a) { return hypot(a.x, a.y); }
-
-// Column j of H from the two CGS passes, rotations, residual estimate, and (when the
-// cycle ends) the back substitution. One warp stages the data in shared memory;
-// lane 0 runs the sequential FP64 recurrences.
-__global__ void k_givens(GState* st, HessPtr h, int m, int j) {
+__device__ void givens_step(GState* st, HessPtr h, int m, int j, bool cgs2) {
   __shared__ double2 col[33], sn[32];
   __shared__ double cs[32];
   __shared__ int stop;
-  const int l = threadIdx.x;
+  const int l = threadIdx.x & 31;
   if (l == 0) stop = st->done;
-  __syncthreads();
+  __syncwarp();
   if (stop) return;
   double2* Hc = h.H + (size_t)j * (m + 1);
-  for (int i = l; i <= j; i += 32) col[i] = h.h1[i] + h.h2[i];
+  for (int i = l; i <= j; i += 32) col[i] = cgs2 ? h.h1[i] + h.h2[i] : h.h1[i];
   for (int i = l; i < j; i += 32) {
     cs[i] = h.cs[i];
     sn[i] = h.sn[i];
   }
-  __syncthreads();
+  __syncwarp();
   if (l == 0) {
     st->steps = j + 1;
     const double hn = sqrt(h.nrm[0].x);
@@ -401,10 +307,10 @@ __global__ void k_givens(GState* st, HessPtr h, int m, int j) {
     stop = end ? 1 : 0;
     }
   }
-  __syncthreads();
+  __syncwarp();
   for (int i = l; i <= j + 1; i += 32) Hc[i] = col[i];
   if (stop) {
-    __syncthreads();
+    __syncwarp();
     if (l == 0) {
       const int k = stop == 2 ? j : j + 1;
       st->k = k;
@@ -421,6 +327,108 @@ __global__ void k_givens(GState* st, HessPtr h, int m, int j) {
     }
   }
 }
+
+// w -= sum_i coef_i s_i V_i (i < nv); optionally out_norm.x = ||w||^2
+template <typename T, bool NORM>
+__global__ void __launch_bounds__(NTH) k_maxpy(const cx<T>* __restrict__ V, size_t n, int nv, const double* scale,
+                                               const double2* coef, cx<T>* __restrict__ w, double2* part, int* counter,
+                                               double2* out_norm, const int* done, GState* st, HessPtr hp, int m,
+                                               int j, int cgs2) {
+  if (done && *done) return;
+  __shared__ cx<T> cf[32];
+  if (threadIdx.x < 32) {
+    const int i = threadIdx.x;
+    const double s = (scale && i < nv) ? scale[i] : 1.0;
+    cf[i] = i < nv ? mk<T>((T)(s * coef[i].x), (T)(s * coef[i].y)) : czero<cx<T>>();
+  }
+  __syncthreads();
+  const size_t chunk = (size_t)NTH * EPT;
+  double nrm = 0.0;
+  for (size_t base = (size_t)blockIdx.x * chunk; base < n; base += (size_t)gridDim.x * chunk) {
+    cx<T> wr[EPT];
+#pragma unroll
+    for (int u = 0; u < EPT; ++u) {
+      const size_t k = base + (size_t)u * NTH + threadIdx.x;
+      wr[u] = k < n ? w[k] : czero<cx<T>>();
+    }
+    for (int i = 0; i < nv; ++i) {
+      const cx<T>* Vi = V + (size_t)i * n;
+      const cx<T> c = cf[i];
+#pragma unroll
+      for (int u = 0; u < EPT; ++u) {
+        const size_t k = base + (size_t)u * NTH + threadIdx.x;
+        if (k < n) {
+          const cx<T> v = Vi[k];
+          wr[u].x -= c.x * v.x - c.y * v.y;
+          wr[u].y -= c.x * v.y + c.y * v.x;
+        }
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < EPT; ++u) {
+      const size_t k = base + (size_t)u * NTH + threadIdx.x;
+      if (k < n) {
+        w[k] = wr[u];
+        if (NORM) nrm += (double)wr[u].x * wr[u].x + (double)wr[u].y * wr[u].y;
+      }
+    }
+  }
+  if (NORM) {
+    double2 a[1] = {make_double2(nrm, 0.0)};
+    const bool last = reduce_to<1>(a, 1, part, counter, out_norm);
+    // the last block holds the final ||w||^2: it runs the step's Givens update
+    if (last && st && threadIdx.x < 32) {
+      __syncwarp();
+      givens_step(st, hp, m, j, cgs2 != 0);
+    }
+  }
+}
+
+// ||v||^2 -> out.x ; optionally also r = b - ax written first (when b != null)
+template <typename T>
+__global__ void __launch_bounds__(NTH) k_resid_norm(const cx<T>* __restrict__ b, const cx<T>* __restrict__ ax,
+                                                    cx<T>* __restrict__ r, size_t n, double2* part, int* counter,
+                                                    double2* out) {
+  double2 nrm = make_double2(0, 0);
+  for (size_t k = (size_t)blockIdx.x * NTH + threadIdx.x; k < n; k += (size_t)gridDim.x * NTH) {
+    cx<T> v;
+    if (ax) {
+      v = b[k] - ax[k];
+      r[k] = v;
+    } else {
+      v = b[k];
+    }
+    const double2 d = to_d(v);
+    nrm.x += d.x * d.x + d.y * d.y;
+  }
+  double2 a[1] = {nrm};
+  reduce_to<1>(a, 1, part, counter, out);
+}
+
+// cycle start: beta = sqrt(nrm), scale[0] = 1/beta, g = (beta, 0, ...)
+__global__ void k_cycle_init(GState* st, HessPtr h, int m, double tol_abs) {
+  if (threadIdx.x != 0) return;
+  const double beta = sqrt(h.nrm[0].x);
+  st->beta = beta;
+  st->res = beta;
+  st->tol_abs = tol_abs;
+  st->k = 0;
+  st->steps = 0;
+  st->status = MSC_OK;
+  st->converged = 0;
+  st->done = 0;
+  for (int i = 0; i <= m; ++i) h.g[i] = make_double2(0, 0);
+  h.g[0] = make_double2(beta, 0);
+  h.scale[0] = beta > 0 ? 1.0 / beta : 0.0;
+  if (!(beta == beta) || isinf(beta)) {
+    st->status = MSC_ERR_NONFINITE;
+    st->done = 1;
+  } else if (beta <= tol_abs || beta == 0.0) {
+    st->converged = 1;
+    st->done = 1;
+  }
+}
+
 
 // x += sum_{i<k} y_i s_i V_i, with k from the state (s_i = 1 when scale is null)
 template <typename T, typename TX, int NV>
@@ -474,13 +482,16 @@ static int mdot(msc_plan* pl, GmresWork* gw, const cx<T>* V, int nv, const doubl
   return MSC_OK;
 }
 
+// With giv_j >= 0 (NORM only) the last block also runs the Givens update of step giv_j.
 template <typename T, bool NORM>
 static int maxpy(msc_plan* pl, GmresWork* gw, const cx<T>* V, int nv, const double* scale, const double2* coef,
-                 cx<T>* w, double2* out_norm, const int* done) {
+                 cx<T>* w, double2* out_norm, const int* done, int giv_j = -1, int m = 0, bool cgs2 = false) {
   GState* st = (GState*)gw->state.p;
   double2* part = (double2*)gw->part.p;
   const int nb = std::min<long long>(NB, ceil_div((long long)gw->n, (long long)NTH * EPT));
-  k_maxpy<T, NORM><<<nb, NTH, 0, pl->stream>>>(V, gw->n, nv, scale, coef, w, part, &st->counter[1], out_norm, done); ::msc::note_launch();
+  k_maxpy<T, NORM><<<nb, NTH, 0, pl->stream>>>(V, gw->n, nv, scale, coef, w, part, &st->counter[1], out_norm, done,
+                                               giv_j >= 0 ? st : nullptr, hess_ptrs(gw), m, giv_j, cgs2 ? 1 : 0);
+  ::msc::note_launch();
   MSC_CUDA(cudaGetLastError());
   return MSC_OK;
 }
@@ -593,15 +604,11 @@ static int gmres_core(msc_plan* pl, int m, const cx<T>* rhs, cx<T>* x, bool x_ze
       if (cgs2) {
         MSC_TRY((maxpy<T, false>(pl, gw, V, j + 1, h.scale, h.h1, w, nullptr, done)));
         MSC_TRY(mdot<T>(pl, gw, V, j + 1, h.scale, w, h.h2, done));
-        MSC_TRY((maxpy<T, true>(pl, gw, V, j + 1, h.scale, h.h2, w, &h.nrm[0], done)));
+        MSC_TRY((maxpy<T, true>(pl, gw, V, j + 1, h.scale, h.h2, w, &h.nrm[0], done, j, m, true)));
       } else {
-        // one projection; h2 = 0 so the Hessenberg column is h1
-        MSC_CUDA(cudaMemsetAsync(h.h2, 0, sizeof(double2) * (j + 1), pl->stream));
-        MSC_TRY((maxpy<T, true>(pl, gw, V, j + 1, h.scale, h.h1, w, &h.nrm[0], done)));
+        // one projection: the Hessenberg column is h1
+        MSC_TRY((maxpy<T, true>(pl, gw, V, j + 1, h.scale, h.h1, w, &h.nrm[0], done, j, m, false)));
       }
-      k_givens<<<1, 32, 0, pl->stream>>>(st, h, m, j);
-      ::msc::note_launch();
-      MSC_CUDA(cudaGetLastError());
       return MSC_OK;
     };
     GState cur;
