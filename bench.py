@@ -51,7 +51,7 @@ WORKLOADS = {
     "cfg3": dict(batch=256, tol=1e-8, periodic=False, mat=("iid", 0.20)),
     # held-out 64x64x16 GRF slabs of the learned-preconditioner distribution: correlation
     # length U[2,6] cells, std U[0.1,0.3], ka U[0.3,1], angle U[0,40 deg], P/SV; aperiodic
-    "cfg4": dict(precond_eval=8, M=64, N_z=16, tol=1e-8, periodic=False),
+    "cfg4": dict(precond_eval=8, precond_train=16, precond_val=4, M=64, N_z=16, tol=1e-8, periodic=False),
 }
 ALPHA, BETA, RHO, A = 3000.0, 1732.0, 2500.0, 1.0
 
@@ -471,20 +471,38 @@ def cfg4_problem(wl: dict, seed: int):
 
 
 def run_precond_eval(args, wl, rank, world, local_rank) -> int:
-    """cfg4: per held-out slab, the time to 1e-8 (FP64 true residual) of plain FP64
-    GMRES(30), mixed-precision GMRES(30) and mixed-precision flexible GMRES(30) with the
-    near-field preconditioner; each solve includes T0, G0, incident and R_PP. The line's
-    value is the preconditioned mixed solver's throughput over the slabs."""
+    """cfg4: the learned preconditioner is trained on the GPU on GRF slabs of the
+    workload (seeds 3000+, untimed; model selection on validation slabs, seeds 4000+),
+    then, per held-out slab (seeds 5000+), the time to 1e-8 (FP64 true residual) of plain
+    FP64 GMRES(30), mixed-precision GMRES(30), mixed-precision flexible GMRES(30) with
+    the near-field Neumann polynomial of degree 2 and of the learned network's degree,
+    and with the learned network; each solve includes T0, G0, incident and R_PP. The
+    line's value is the learned-preconditioned mixed solver's throughput."""
+    import time
+
     import torch
 
-    from multiplescatteringcalculations_b200 import SlabPlan, _native
+    from multiplescatteringcalculations_b200 import BatchProblem, NearFieldPreconditioner, SlabPlan, _native
+    from multiplescatteringcalculations_b200.learned import train_nearfield
 
     torch.cuda.set_device(local_rank)
     dev = torch.device("cuda", local_rank)
     lib = _native.load()
+
+    def problem(seed):
+        ref, g, mat, kh, om, wave, _ = cfg4_problem(wl, seed)
+        return BatchProblem(g, mat, om, kh, wave)
+
+    t_train = time.perf_counter()
+    net = train_nearfield([problem(3000 + i) for i in range(wl["precond_train"])],
+                          [problem(4000 + i) for i in range(wl["precond_val"])], max_iter=6000)
+    t_train = time.perf_counter() - t_train
+    physics = NearFieldPreconditioner(net.degree)
     variants = {"fp64": dict(precision="fp64", preconditioner=None),
                 "mixed": dict(precision="mixed", preconditioner=None),
-                "mixed_nearfield": dict(precision="mixed", preconditioner="nearfield")}
+                "mixed_nearfield": dict(precision="mixed", preconditioner="nearfield"),
+                f"mixed_nearfield_d{net.degree}": dict(precision="mixed", preconditioner=physics),
+                "mixed_learned": dict(precision="mixed", preconditioner=net)}
     stream = torch.cuda.current_stream(dev)
     rows = []
     n0 = lib.msc_launch_count()
@@ -500,10 +518,13 @@ def run_precond_eval(args, wl, rank, world, local_rank) -> int:
                     plan.build_t0(md, om)
                     plan.build_g0(om)
                     psi0 = plan.incident(om, kh, wave)
-                    if v["preconditioner"]:
+                    pc = v["preconditioner"]
+                    if pc == "nearfield":
                         plan.set_nearfield()
+                    elif pc is not None:
+                        pc.install(plan)
                     x, st = plan.solve(psi0, tol=wl["tol"], max_iter=6000, restart=30, precision=v["precision"],
-                                       preconditioner=v["preconditioner"])
+                                       preconditioner=None if pc is None else "nearfield")
                     plan.rpp_periodic(x, om)
                     return st
                 for _ in range(max(1, args.warmup)):
@@ -524,13 +545,17 @@ def run_precond_eval(args, wl, rank, world, local_rank) -> int:
     ok = all(r[n]["residual"] <= wl["tol"] for r in rows for n in variants)
     t = {n: float(np.sum([r[n]["ms"] for r in rows])) for n in variants}
     line = {
-        "metric": METRIC, "value": 1e3 * len(rows) / t["mixed_nearfield"], "unit": "solves/s", "n_gpus": 1,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": t["mixed_nearfield"] / len(rows),
+        "metric": METRIC, "value": 1e3 * len(rows) / t["mixed_learned"], "unit": "solves/s", "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": t["mixed_learned"] / len(rows),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "c64+c128", "data": "synthetic",
         "config": {"workload": "cfg4", "lattice": f"{wl['M']}x{wl['M']}x{wl['N_z']}", "slabs": len(rows),
                    "ell": "U[2,6]", "std": "U[0.1,0.3]", "ka": "U[0.3,1]", "incidence_deg": "U[0,40]",
                    "wave": "P/SV", "tol": wl["tol"], "periodic": False, "restart": 30,
-                   "precond": "near-field Neumann polynomial, degree 2 (no trained network)",
+                   "precond": (f"learned near-field network, degree {net.degree}, BF16 weights, trained on the GPU "
+                               f"on {wl['precond_train']} slabs ({len(net.history[0]['losses'])} Adam steps, "
+                               f"{t_train:.1f} s incl. residual generation and validation); selected: "
+                               f"{net.history[-1].get('selected', 'trained')}"),
+                   "validation_matvecs": net.history[1] if len(net.history) > 1 else None,
                    "l2": "inputs larger than L2 (G0 spectrum build per solve)"},
         "gpu_launches": int(launches), "all_converged": ok,
         "ms_per_solve": {n: t[n] / len(rows) for n in variants},

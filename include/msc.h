@@ -145,6 +145,35 @@ int msc_set_nearfield(msc_plan* plan, int degree, const double* coef, const doub
 int msc_nearfield_blocks(const msc_plan* plan, double* out);
 /* z = P x, fields (N_z, M, M, 9) on the device in the precision given. */
 int msc_precondition(msc_plan* plan, const void* x, void* z, int precision);
+/* Storage of the layer blocks G_nn + dG_l for the complex64 preconditioner:
+ * MSC_NF_WEIGHTS_FP32 (default) or MSC_NF_WEIGHTS_BF16 (rounded to bfloat16, FP32
+ * accumulation; the form the learned network is trained in). The complex128 path
+ * always uses FP64 blocks. */
+enum msc_nf_weights { MSC_NF_WEIGHTS_FP32 = 0, MSC_NF_WEIGHTS_BF16 = 1 };
+int msc_set_nearfield_weights(msc_plan* plan, int format);
+
+/* Learned near-field preconditioner: training on the GPU. The network is the
+ * polynomial above with learned coefficients c_l and block corrections
+ * dG_l = s w_l, s = msc_nearfield_scale(plan) = max |G_nn| (0 before build_g0); the
+ * weights w are dimensionless (L x 27 x 81 complex, re/im doubles) and carry over
+ * between frequencies. Objective per residual r, the residual of one GMRES step on
+ * the preconditioned operator: loss = min_alpha || alpha A P r^ - r^ ||^2
+ * = 1 - |<A P r^, r^>|^2 / ||A P r^||^2, r^ = r / ||r||, A = I - G0 T0. Needs the
+ * point-propagator kernel without a Bloch phase (MSC_ERR_UNSUPPORTED otherwise).
+ * No counterpart in the reference, which solves without a preconditioner. */
+double msc_nearfield_scale(const msc_plan* plan);
+/* Loss and gradients with respect to conj(c) (gcoef: 2(L+1) doubles) and conj(w)
+ * (gw: L x 27 x 81 complex) for one residual r (N_z, M, M, 9) on the device in the
+ * precision given; complex64 evaluates with BF16 layer weights. */
+int msc_nf_loss_grad(msc_plan* plan, const void* r, int precision, int degree, const double* coef,
+                     const double* w, double* loss, double* gcoef, double* gw);
+/* `steps` Adam steps (beta 0.9/0.999, eps 1e-8, FP32 master weights, BF16 layer
+ * weights) over n_res complex64 residuals r[n_res][N_z][M][M][9] on the device, one
+ * residual per step in turn. coef, w are updated in place; adam (2 n_par + 1 doubles,
+ * n_par = 2(L+1) + 2 L 27 81: first moments, second moments, step count; zeros to
+ * start) carries the optimiser state between calls; losses (steps doubles) may be NULL. */
+int msc_nf_train(msc_plan* plan, const void* r, int n_res, int degree, int steps, double lr, double* coef, double* w,
+                 double* adam, double* losses);
 
 /* Solve (I - G0 T0) x = b; b, x complex128 (N_z, M, M, 9). Restarted GMRES with
  * CGS2 Arnoldi and FP64 Givens/least squares; precision MIXED runs complex64

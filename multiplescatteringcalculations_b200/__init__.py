@@ -29,4 +29,6 @@ from .slab import (  # noqa: F401
     uniform_slab_material,
 )
 
+from .learned import NearFieldPreconditioner, fgmres_matvecs, solver_residuals, train_nearfield  # noqa: F401,E402
+
 __version__ = "0.1.0"

@@ -28,6 +28,8 @@ MSC_RPP_BLOCH = 1
 MSC_RPP_PLANE_WAVE_MOMENT = 2
 MSC_PC_NONE = 0
 MSC_PC_NEARFIELD = 1
+MSC_NF_WEIGHTS_FP32 = 0
+MSC_NF_WEIGHTS_BF16 = 1
 MSC_SOLVE_MIXED = 0
 MSC_SOLVE_FP64 = 1
 MSC_WAVE_P = 0
@@ -110,6 +112,12 @@ SIGNATURES = {
     "msc_batch_solve": (C.c_int, [C.POINTER(BatchItem), C.c_int, C.POINTER(SolveOpts), C.c_int,
                                   C.POINTER(C.c_int)]),
     "msc_nearfield_blocks": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "msc_set_nearfield_weights": (C.c_int, [C.c_void_p, C.c_int]),
+    "msc_nearfield_scale": (C.c_double, [C.c_void_p]),
+    "msc_nf_loss_grad": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p,
+                                   C.c_void_p, C.c_void_p]),
+    "msc_nf_train": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_double, C.c_void_p,
+                               C.c_void_p, C.c_void_p, C.c_void_p]),
     "msc_precondition": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int]),
     "msc_rpp_periodic": (C.c_int, [C.c_void_p, C.c_void_p, C.c_double, C.c_double, C.c_int, C.c_void_p]),
     "msc_reflected_field": (C.c_int, [C.c_void_p, C.c_void_p, C.c_double, C.c_void_p, C.c_void_p]),

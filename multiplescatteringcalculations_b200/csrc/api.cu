@@ -227,6 +227,7 @@ int msc_plan_destroy(msc_plan* pl) {
   if (pl->nf) {
     dfree(pl, pl->nf->g64_dev);
     dfree(pl, pl->nf->g32_dev);
+    dfree(pl, pl->nf->g16_dev);
     dfree(pl, pl->nf->tmp32);
     dfree(pl, pl->nf->tmp64);
     delete pl->nf;
@@ -358,6 +359,18 @@ int msc_set_nearfield(msc_plan* pl, int degree, const double* coef, const double
   }
   nf->dirty = true;
   ++pl->gen;
+  return MSC_OK;
+}
+
+int msc_set_nearfield_weights(msc_plan* pl, int format) {
+  if (!pl) { set_error("null plan"); return MSC_ERR_INVALID; }
+  if (format != MSC_NF_WEIGHTS_FP32 && format != MSC_NF_WEIGHTS_BF16) {
+    set_error("weight format must be 0 (FP32) or 1 (BF16), got %d", format);
+    return MSC_ERR_INVALID;
+  }
+  if (!pl->nf) pl->nf = new NearField();
+  pl->nf->wbf16 = format == MSC_NF_WEIGHTS_BF16;
+  ++pl->gen;  // the captured solver graphs bind the block pointer
   return MSC_OK;
 }
 

@@ -55,6 +55,7 @@ int nearfield_extract(msc_plan* pl, const double2* Ks, double scale) {
   NearField* nf = pl->nf;
   MSC_TRY(dalloc(pl, nf->g64_dev, sizeof(double2) * (size_t)(NF_MAXL + 1) * NF_OFFS * 81));
   MSC_TRY(dalloc(pl, nf->g32_dev, sizeof(float2) * (size_t)(NF_MAXL + 1) * NF_OFFS * 81));
+  MSC_TRY(dalloc(pl, nf->g16_dev, sizeof(__nv_bfloat162) * (size_t)(NF_MAXL + 1) * NF_OFFS * 81));
   double2* dst = (double2*)nf->g64_dev.p;
   k_nf_extract<<<ceil_div(NF_OFFS * 81, 256), 256, 0, pl->stream>>>(Ks, pl->g, pl->E, 1.0 / scale, dst);
   ::msc::note_launch();
@@ -78,7 +79,8 @@ template <typename T> struct NFTile {
 template <typename T>
 __device__ __forceinline__ void nf_body(const cx<T>* __restrict__ x, const double* scale, const cx<T>* __restrict__ t4,
                                         cx<T>* __restrict__ h, cx<T>* __restrict__ acc, cx<T> ch, cx<T> c0, int init,
-                                        const cx<T>* __restrict__ G, const Geo& g) {
+                                        const cx<T>* __restrict__ G, const __nv_bfloat162* __restrict__ G16,
+                                        const Geo& g) {
   using C = cx<T>;
   using TL = NFTile<T>;
   constexpr int TZ = TL::TZ, TX = TL::TX, TY = TL::TY, VPT = TL::VPT;
@@ -92,9 +94,12 @@ __device__ __forceinline__ void nf_body(const cx<T>* __restrict__ x, const doubl
   C* tau = reinterpret_cast<C*>(Gs + NF_OFFS * 81);          // [9][HALO]
   const int tid = threadIdx.x;
   for (int i = tid; i < NF_OFFS * 81; i += NT) {
-    const C v = __ldg(G + i);
-    if constexpr (sizeof(T) == 4) Gs[i] = make_float4(v.x, v.x, v.y, v.y);
-    else Gs[i] = v;
+    if constexpr (sizeof(T) == 4) {
+      const float2 v = G16 ? __bfloat1622float2(G16[i]) : __ldg(G + i);  // BF16 or FP32 weights
+      Gs[i] = make_float4(v.x, v.x, v.y, v.y);
+    } else {
+      Gs[i] = __ldg(G + i);
+    }
   }
   const int nxb = (g.M + TX - 1) / TX;
   const int y0 = blockIdx.x * TY, x0 = (blockIdx.y % nxb) * TX, z0 = (blockIdx.y / nxb) * TZ;
@@ -191,9 +196,10 @@ __device__ __forceinline__ void nf_body(const cx<T>* __restrict__ x, const doubl
 __global__ void __launch_bounds__(256, 2) k_nf32(const float2* __restrict__ x, const double* scale,
                                               const float2* __restrict__ t4, float2* __restrict__ h,
                                               float2* __restrict__ acc, float2 ch, float2 c0, int init,
-                                              const float2* __restrict__ G, Geo g, const int* done) {
+                                              const float2* __restrict__ G, const __nv_bfloat162* __restrict__ G16,
+                                              Geo g, const int* done) {
   if (done && *done) return;
-  nf_body<float>(x, scale, t4, h, acc, ch, c0, init, G, g);
+  nf_body<float>(x, scale, t4, h, acc, ch, c0, init, G, G16, g);
 }
 
 __global__ void __launch_bounds__(256) k_nf64(const double2* __restrict__ x, const double* scale,
@@ -201,7 +207,7 @@ __global__ void __launch_bounds__(256) k_nf64(const double2* __restrict__ x, con
                                               double2* __restrict__ acc, double2 ch, double2 c0, int init,
                                               const double2* __restrict__ G, Geo g, const int* done) {
   if (done && *done) return;
-  nf_body<double>(x, scale, t4, h, acc, ch, c0, init, G, g);
+  nf_body<double>(x, scale, t4, h, acc, ch, c0, init, G, nullptr, g);
 }
 
 // Upload the per-layer blocks g64 + dg[l] (complex128 and complex64) to the device.
@@ -212,15 +218,19 @@ int nearfield_refresh(msc_plan* pl) {
   const size_t nb = (size_t)L * NF_OFFS * 81;
   nf->h64.resize(nb);
   nf->h32.resize(nb);
+  nf->h16.resize(nb);
   for (int l = 0; l < L; ++l)
     for (int i = 0; i < NF_OFFS * 81; ++i) {
       double2 v = nf->g64[i];
       if (!nf->dg.empty()) v = v + nf->dg[(size_t)l * NF_OFFS * 81 + i];
       nf->h64[(size_t)l * NF_OFFS * 81 + i] = v;
       nf->h32[(size_t)l * NF_OFFS * 81 + i] = make_float2((float)v.x, (float)v.y);
+      nf->h16[(size_t)l * NF_OFFS * 81 + i] = __floats2bfloat162_rn((float)v.x, (float)v.y);
     }
   MSC_CUDA(cudaMemcpyAsync(nf->g64_dev.p, nf->h64.data(), sizeof(double2) * nb, cudaMemcpyHostToDevice, pl->stream));
   MSC_CUDA(cudaMemcpyAsync(nf->g32_dev.p, nf->h32.data(), sizeof(float2) * nb, cudaMemcpyHostToDevice, pl->stream));
+  MSC_CUDA(cudaMemcpyAsync(nf->g16_dev.p, nf->h16.data(), sizeof(__nv_bfloat162) * nb, cudaMemcpyHostToDevice,
+                           pl->stream));
   MSC_CUDA(cudaStreamSynchronize(pl->stream));
   nf->dirty = false;
   return MSC_OK;
@@ -259,7 +269,10 @@ int nearfield_apply(msc_plan* pl, const cx<T>* v, const double* scale, cx<T>* z,
       k_nf32<<<grid, TL::NT, sm, pl->stream>>>((const float2*)in, sc, (const float2*)t4, (float2*)h, (float2*)z,
                                              make_float2((float)ch.x, (float)ch.y),
                                              make_float2((float)c0.x, (float)c0.y), init,
-                                             (const float2*)nf->g32_dev.p + (size_t)(l - 1) * NF_OFFS * 81, g, done);
+                                             (const float2*)nf->g32_dev.p + (size_t)(l - 1) * NF_OFFS * 81,
+                                             nf->wbf16 ? (const __nv_bfloat162*)nf->g16_dev.p + (size_t)(l - 1) * NF_OFFS * 81
+                                                       : nullptr,
+                                             g, done);
     } else {
       k_nf64<<<grid, TL::NT, sm, pl->stream>>>((const double2*)in, sc, (const double2*)t4, (double2*)h, (double2*)z,
                                              make_double2((double)ch.x, (double)ch.y),

@@ -7,6 +7,8 @@
 // is c = (1, 1, ..., 1). A learned preconditioner sets the coefficients and adds
 // corrections to the stencil blocks of each layer (pc.cu).
 #pragma once
+#include <cuda_bf16.h>
+
 #include "plan.cuh"
 
 namespace msc {
@@ -27,9 +29,11 @@ struct NearField {
   // Per-layer blocks g64 + dg[l] on the device, [L][27][81], y_a(v) += g[o][a][b] tau_b(v - o).
   // The kernels read them through these pointers, so a captured solver graph stays valid
   // when the blocks change (a new frequency): only the buffers' contents are refreshed.
-  DBuf g64_dev, g32_dev;
+  DBuf g64_dev, g32_dev, g16_dev;
+  int wbf16 = 0;               // complex64 path: BF16 blocks (g16_dev) instead of FP32 (g32_dev)
   std::vector<double2> h64;    // host staging of the refresh
   std::vector<float2> h32;
+  std::vector<__nv_bfloat162> h16;
   DBuf tmp32, tmp64;           // two field-size work vectors per precision
   bool dirty = true;           // layer blocks to rebuild from g64, dg
 };

@@ -299,12 +299,15 @@ class SlabPlan:
                  "residual": st.residual, "n_precond": st.n_precond, "pc_fallback": bool(st.pc_fallback)}
         return xx, stats
 
-    def set_nearfield(self, degree: int = 2, coef=None, dblocks=None) -> None:
+    def set_nearfield(self, degree: int = 2, coef=None, dblocks=None, weights: str = "fp32") -> None:
         """Near-field polynomial preconditioner P = sum_l c_l S_l ... S_1 with
         S_l x = (G_nn + dG_l)(T0 x): ``coef`` (degree + 1 complex, default all ones:
         the truncated Neumann series), ``dblocks`` (degree x 27 x 9 x 9 complex block
         corrections, default none; entries outside the lattice's mirror-symmetry
-        pattern are not applied)."""
+        pattern are not applied), ``weights`` the storage of the layer blocks in the
+        complex64 preconditioner ("fp32" or "bf16")."""
+        if weights not in ("fp32", "bf16"):
+            raise ValueError(f"weights must be 'fp32' or 'bf16', got {weights!r}")
         c = None
         if coef is not None:
             cc = np.asarray(coef, dtype=np.complex128).ravel()
@@ -319,6 +322,57 @@ class SlabPlan:
             d = np.ascontiguousarray(np.stack([dd.real, dd.imag], -1).ravel())
         N.check(self.lib.msc_set_nearfield(self.handle, int(degree), None if c is None else c.ctypes.data,
                                            None if d is None else d.ctypes.data), "msc_set_nearfield")
+        N.check(self.lib.msc_set_nearfield_weights(
+            self.handle, N.MSC_NF_WEIGHTS_BF16 if weights == "bf16" else N.MSC_NF_WEIGHTS_FP32),
+            "msc_set_nearfield_weights")
+
+    def nearfield_scale(self) -> float:
+        """s = max |G_nn| of the last build_g0: the unit of the learned block weights."""
+        return float(self.lib.msc_nearfield_scale(self.handle))
+
+    def nf_loss_grad(self, r: torch.Tensor, coef, w, precision: str = "complex128"):
+        """Training objective of the learned near-field preconditioner for one residual
+        r (N_z, M, M, 9): loss = min_alpha ||alpha A P r^ - r^||^2, r^ = r / ||r|| (one
+        GMRES step on the preconditioned operator), with P of degree
+        len(coef) - 1, coefficients ``coef`` and block weights ``w`` (degree x 27 x 9 x 9,
+        dG_l = nearfield_scale() w_l). Returns (loss, dL/dconj(coef), dL/dconj(w)),
+        computed by the library's forward and backward kernels; "complex64" evaluates
+        with BF16 layer weights."""
+        cc = np.asarray(coef, dtype=np.complex128).ravel()
+        L = cc.size - 1
+        ww = np.ascontiguousarray(np.asarray(w, dtype=np.complex128).reshape(L, 27, 9, 9))
+        dt = torch.complex128 if precision == "complex128" else torch.complex64
+        rr = r.to(device=self.device, dtype=dt).contiguous()
+        loss = C.c_double()
+        gc = np.zeros(L + 1, dtype=np.complex128)
+        gw = np.zeros((L, 27, 9, 9), dtype=np.complex128)
+        cr = np.ascontiguousarray(cc)
+        N.check(self.lib.msc_nf_loss_grad(self.handle, _ptr(rr),
+                                          N.MSC_COMPLEX128 if dt == torch.complex128 else N.MSC_COMPLEX64, L,
+                                          cr.ctypes.data, ww.ctypes.data, C.byref(loss), gc.ctypes.data,
+                                          gw.ctypes.data), "msc_nf_loss_grad")
+        return float(loss.value), gc, gw
+
+    def nf_train(self, residuals: torch.Tensor, coef, w, adam, steps: int, lr: float):
+        """``steps`` Adam steps of the learned preconditioner over the complex64
+        residuals (n, N_z, M, M, 9) on the device, one per step in turn. Returns
+        (coef, w, adam, losses); ``adam`` is the optimiser state (None to start)."""
+        # copies: the library updates them in place
+        cc = np.array(coef, dtype=np.complex128).ravel()
+        L = cc.size - 1
+        ww = np.array(w, dtype=np.complex128).reshape(L, 27, 9, 9)
+        npar = 2 * (L + 1) + 2 * L * 27 * 81
+        st = np.zeros(2 * npar + 1) if adam is None else np.array(adam, dtype=np.float64)
+        if st.size != 2 * npar + 1:
+            raise ValueError(f"adam state needs {2 * npar + 1} entries, got {st.size}")
+        rr = residuals.to(device=self.device, dtype=torch.complex64).contiguous()
+        if rr.dim() != 5:
+            raise ValueError("residuals must have shape (n, N_z, M, M, 9)")
+        losses = np.zeros(max(int(steps), 1))
+        N.check(self.lib.msc_nf_train(self.handle, _ptr(rr), int(rr.shape[0]), L, int(steps), float(lr),
+                                      cc.ctypes.data, ww.ctypes.data, st.ctypes.data, losses.ctypes.data),
+                "msc_nf_train")
+        return cc, ww, st, losses[: int(steps)]
 
     def nearfield_blocks(self) -> NDArray:
         """The (27, 9, 9) near-field blocks G_nn of the last build_g0."""

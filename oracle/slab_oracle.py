@@ -830,3 +830,77 @@ def nearfield_precondition(x, t4, blocks, M, N_z, coef=(1, 1, 1), dblocks=None):
         h = nearfield_stencil(h, t4, b, M, N_z)
         out = out + coef[l] * h
     return out
+
+
+def nearfield_stencil_adjoint(y, t4, blocks, M, N_z):
+    """S^H y = T0^H (sum_o G_o^H y(. + o)): the adjoint of nearfield_stencil in the
+    Euclidean inner product (T0 is complex symmetric, so T0^H = conj(T0))."""
+    blocks = blocks * nearfield_symmetry_mask()
+    yp = np.zeros((N_z + 2, M + 2, M + 2, 9), dtype=complex)
+    yp[1:-1, 1:-1, 1:-1] = np.asarray(y).reshape(N_z, M, M, 9)
+    z = np.zeros((N_z, M, M, 9), dtype=complex)
+    for o in range(27):
+        dz, dx, dy = o // 9 - 1, (o // 3) % 3 - 1, o % 3 - 1
+        z += yp[1 + dz:1 + dz + N_z, 1 + dx:1 + dx + M, 1 + dy:1 + dy + M] @ blocks[o].conj()
+    return apply_t0(np.conj(t4), z).ravel()
+
+
+_ADJ_P = np.array([-1.0, -1.0, -1.0, 1.0, 1.0, 1.0, 1.0, 1.0, 1.0])  # displacements odd, strains even
+_ADJ_D = np.array([1.0, 1.0, 1.0, 1.0, 1.0, 1.0, 2.0, 2.0, 2.0])    # Voigt factors of the shear strains
+
+
+def slab_operator_adjoint(y, t4, kernel_hat, M, N_z, *, periodic=False):
+    """A^H y for A = I - G0 T0 (an addition of this build). Reciprocity makes K D
+    symmetric and the mirror symmetry gives K(-r) = P K(r) P, so G0^T = P D^-1 G0 D P and
+    A^H y = y - conj(T0) P D^-1 conj(G0 (D P conj(y))), G0 u = (u - A_tau u) / tau with
+    A_tau the operator at T0 = tau I, tau = 1 / max|K| (so G0 tau u does not cancel)."""
+    tau = 1.0 / np.abs(kernel_hat).max() * kernel_hat.shape[1] * kernel_hat.shape[2]
+    ident = np.zeros_like(t4)
+    ident[0] = ident[2] = ident[3] = tau
+    y = np.asarray(y, dtype=complex).reshape(-1, 9)
+    u = (_ADJ_D * _ADJ_P * np.conj(y)).ravel()
+    g0u = (u - slab_matvec(u, ident, kernel_hat, M, N_z, periodic=periodic)) / tau
+    w = (_ADJ_P / _ADJ_D * np.conj(g0u.reshape(-1, 9))).reshape(N_z, M, M, 9)
+    return y.ravel() - apply_t0(np.conj(t4), w).ravel()
+
+
+def nearfield_residual_loss_grad(r, t4, kernel_hat, blocks, M, N_z, coef, w=None, *, periodic=False):
+    """Training objective of the learned near-field preconditioner and its gradients
+    (an addition of this build). With P r = sum_l c_l h_l, h_0 = r, h_l = S_l h_{l-1},
+    S_l = (G_nn + s w_l) T0, s = max |G_nn|, the residual of one GMRES step:
+        loss = min_alpha || alpha A P r^ - r^ ||^2 = 1 - |<y, r^>|^2 / <y, y>,
+        y = A P r^,  r^ = r / ||r||.
+    Returns (loss, dL/dconj(c) (L+1,), dL/dconj(w) (L, 27, 9, 9)); the weight gradient
+    is zero outside the mirror-symmetry pattern."""
+    coef = np.asarray(coef, dtype=complex)
+    L = len(coef) - 1
+    s = np.abs(blocks).max()
+    w = np.zeros((L, 27, 9, 9), dtype=complex) if w is None else np.asarray(w, dtype=complex)
+    r = np.asarray(r, dtype=complex).ravel()
+    r = r / np.linalg.norm(r)
+    mask = nearfield_symmetry_mask()
+    lay = [blocks + s * w[l] for l in range(L)]
+    hs, taus = [r], []
+    for l in range(L):
+        taus.append(apply_t0(t4, hs[-1].reshape(N_z, M, M, 9)))
+        hs.append(nearfield_stencil(hs[-1], t4, lay[l], M, N_z))
+    z = sum(c * h for c, h in zip(coef, hs))
+    y = slab_matvec(z, t4, kernel_hat, M, N_z, periodic=periodic)
+    alpha = np.vdot(y, r) / np.vdot(y, y).real
+    q = alpha * y - r
+    loss = np.vdot(q, q).real
+    d = slab_operator_adjoint(np.conj(alpha) * q, t4, kernel_hat, M, N_z, periodic=periodic)
+    gc = np.array([np.vdot(h, d) for h in hs])
+    gw = np.zeros((L, 27, 9, 9), dtype=complex)
+    delta = np.conj(coef[L]) * d
+    for l in range(L, 0, -1):
+        tp = np.zeros((N_z + 2, M + 2, M + 2, 9), dtype=complex)
+        tp[1:-1, 1:-1, 1:-1] = taus[l - 1]
+        dv = delta.reshape(N_z, M, M, 9)
+        for o in range(27):
+            dz, dx, dy = o // 9 - 1, (o // 3) % 3 - 1, o % 3 - 1
+            src = tp[1 - dz:1 - dz + N_z, 1 - dx:1 - dx + M, 1 - dy:1 - dy + M]
+            gw[l - 1, o] = s * np.einsum("zxya,zxyb->ab", dv, np.conj(src)) * mask[o]
+        if l > 1:
+            delta = np.conj(coef[l - 1]) * d + nearfield_stencil_adjoint(delta, t4, lay[l - 1], M, N_z)
+    return loss, gc, gw
