@@ -96,6 +96,29 @@ static size_t hess_bytes(int m) {
   return sizeof(double2) * ((size_t)(m + 1) * m + m + (m + 1) + m + 2 * (m + 1) + 4) + sizeof(double) * (m + m + 1);
 }
 
+// Row i of the per-block partials summed over the nb blocks in a fixed order: lane l
+// takes blocks l, l + 32, ... and the warp adds the lanes by shuffles. All of a lane's
+// loads (through L2, ld.global.cg, which sees the other blocks' fenced stores) are in
+// flight before the first add, so the last block pays one L2 round trip per row instead
+// of one per partial.
+__device__ __forceinline__ double2 sum_partials(const double2* __restrict__ part, int i, int nb, int l) {
+  constexpr int MAXQ = (NB + 31) / 32;
+  double2 t[MAXQ];
+#pragma unroll
+  for (int q = 0; q < MAXQ; ++q) {
+    const int b = l + 32 * q;
+    t[q] = b < nb ? __ldcg(part + (size_t)b * PLD + i) : make_double2(0, 0);
+  }
+  double2 v = make_double2(0, 0);
+#pragma unroll
+  for (int q = 0; q < MAXQ; ++q) v += t[q];
+  for (int o = 16; o > 0; o >>= 1) {
+    v.x += __shfl_xor_sync(0xffffffffu, v.x, o);
+    v.y += __shfl_xor_sync(0xffffffffu, v.y, o);
+  }
+  return v;
+}
+
 // ---- block reduction of NV complex partials; last block reduces over blocks -----------
 // sums[i] (i < nv) are this thread's partials. The final values land in out[i].
 template <int NV>
@@ -127,12 +150,7 @@ __device__ bool reduce_to(double2* sums, int nv, double2* __restrict__ part, int
   if (!last) return false;
   __threadfence();
   for (int i = w; i < nv; i += NTH / 32) {
-    double2 v = make_double2(0, 0);
-    for (int b = l; b < (int)gridDim.x; b += 32) v += ((volatile double2*)part)[(size_t)b * PLD + i];
-    for (int o = 16; o > 0; o >>= 1) {
-      v.x += __shfl_xor_sync(0xffffffffu, v.x, o);
-      v.y += __shfl_xor_sync(0xffffffffu, v.y, o);
-    }
+    const double2 v = sum_partials(part, i, (int)gridDim.x, l);
     if (l == 0) out[i] = v;
   }
   if (threadIdx.x == 0) *counter = 0;
@@ -143,6 +161,9 @@ __device__ bool reduce_to(double2* sums, int nv, double2* __restrict__ part, int
 // consecutive elements (thread t holds elements t, t + NTH, ..., so each warp
 // access is coalesced); blocks stride over the chunks.
 constexpr int EPT = 8;
+// vectors per load group in k_mdot / k_maxpy (memory-level parallelism: VG x EPT
+// independent loads per thread)
+constexpr int VG = 4;
 
 // Thread i < nv of every block holds the block's total of row i; the last block
 // to finish sums the rows over blocks in a fixed order into out[i].
@@ -157,12 +178,7 @@ __device__ void reduce_rows(double2 mine, int nv, double2* __restrict__ part, in
   __threadfence();
   const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
   for (int i = w; i < nv; i += NTH / 32) {
-    double2 v = make_double2(0, 0);
-    for (int b = l; b < (int)gridDim.x; b += 32) v += ((volatile double2*)part)[(size_t)b * PLD + i];
-    for (int o = 16; o > 0; o >>= 1) {
-      v.x += __shfl_xor_sync(0xffffffffu, v.x, o);
-      v.y += __shfl_xor_sync(0xffffffffu, v.y, o);
-    }
+    const double2 v = sum_partials(part, i, (int)gridDim.x, l);
     if (l == 0) out[i] = v;
   }
   if (threadIdx.x == 0) *counter = 0;
@@ -188,7 +204,43 @@ __global__ void __launch_bounds__(NTH) k_mdot(const cx<T>* __restrict__ V, size_
       const size_t k = base + (size_t)u * NTH + threadIdx.x;
       wr[u] = k < n ? w[k] : czero<cx<T>>();
     }
-    for (int i = 0; i < nv; ++i) {
+    int i = 0;
+    // groups of VG vectors: all VG x EPT loads are in flight before the first product
+    for (; i + VG <= nv; i += VG) {
+      cx<T> v[VG][EPT];
+#pragma unroll
+      for (int q = 0; q < VG; ++q)
+#pragma unroll
+        for (int u = 0; u < EPT; ++u) {
+          const size_t k = base + (size_t)u * NTH + threadIdx.x;
+          v[q][u] = k < n ? V[(size_t)(i + q) * n + k] : czero<cx<T>>();
+        }
+      double ax[VG], ay[VG];
+#pragma unroll
+      for (int q = 0; q < VG; ++q) {
+        cx<T> a = czero<cx<T>>();
+#pragma unroll
+        for (int u = 0; u < EPT; ++u) {
+          a.x += v[q][u].x * wr[u].x + v[q][u].y * wr[u].y;
+          a.y += v[q][u].x * wr[u].y - v[q][u].y * wr[u].x;
+        }
+        ax[q] = a.x;
+        ay[q] = a.y;
+      }
+      for (int o = 16; o > 0; o >>= 1)
+#pragma unroll
+        for (int q = 0; q < VG; ++q) {
+          ax[q] += __shfl_xor_sync(0xffffffffu, ax[q], o);
+          ay[q] += __shfl_xor_sync(0xffffffffu, ay[q], o);
+        }
+      if (lane == 0)
+#pragma unroll
+        for (int q = 0; q < VG; ++q) {
+          sh[wp][i + q].x += ax[q];
+          sh[wp][i + q].y += ay[q];
+        }
+    }
+    for (; i < nv; ++i) {
       const cx<T>* Vi = V + (size_t)i * n;
       cx<T> a = czero<cx<T>>();
 #pragma unroll
@@ -351,7 +403,27 @@ __global__ void __launch_bounds__(NTH) k_maxpy(const cx<T>* __restrict__ V, size
       const size_t k = base + (size_t)u * NTH + threadIdx.x;
       wr[u] = k < n ? w[k] : czero<cx<T>>();
     }
-    for (int i = 0; i < nv; ++i) {
+    int i = 0;
+    for (; i + VG <= nv; i += VG) {
+      cx<T> v[VG][EPT];
+#pragma unroll
+      for (int q = 0; q < VG; ++q)
+#pragma unroll
+        for (int u = 0; u < EPT; ++u) {
+          const size_t k = base + (size_t)u * NTH + threadIdx.x;
+          v[q][u] = k < n ? V[(size_t)(i + q) * n + k] : czero<cx<T>>();
+        }
+#pragma unroll
+      for (int q = 0; q < VG; ++q) {
+        const cx<T> c = cf[i + q];
+#pragma unroll
+        for (int u = 0; u < EPT; ++u) {
+          wr[u].x -= c.x * v[q][u].x - c.y * v[q][u].y;
+          wr[u].y -= c.x * v[q][u].y + c.y * v[q][u].x;
+        }
+      }
+    }
+    for (; i < nv; ++i) {
       const cx<T>* Vi = V + (size_t)i * n;
       const cx<T> c = cf[i];
 #pragma unroll
