@@ -301,7 +301,7 @@ __device__ __forceinline__ C* fft_tile_ct(C* a, C* b, const C* tw, int tid) {
 // stages as above, every index a compile-time constant, so the stages are register
 // renamings); twiddles come from the block's shared table tw[t] = exp(-2 pi i t / L).
 // An output the caller never reads is not computed (dead code).
-template <int L, int S, int DIR, typename C>
+template <int L, int S, int DIR, int TS = 1, typename C>
 __device__ __forceinline__ void fft_reg_stages(C* v, const C* __restrict__ tw) {
   using PL = Pow2Plan<L>;
   if constexpr (S < PL::NSTAGES) {
@@ -316,7 +316,7 @@ __device__ __forceinline__ void fft_reg_stages(C* v, const C* __restrict__ tw) {
       if (kk != 0) {
 #pragma unroll
         for (int r = 1; r < R; ++r) {
-          C w = tw[r * kk * TSTEP];
+          C w = tw[r * kk * TSTEP * TS];
           if (DIR > 0) w.y = -w.y;
           u[r] = u[r] * w;
         }
@@ -328,13 +328,15 @@ __device__ __forceinline__ void fft_reg_stages(C* v, const C* __restrict__ tw) {
     }
 #pragma unroll
     for (int i = 0; i < L; ++i) v[i] = out[i];
-    fft_reg_stages<L, S + 1, DIR>(v, tw);
+    fft_reg_stages<L, S + 1, DIR, TS>(v, tw);
   }
 }
 
-template <int L, int DIR, typename C>
+// TS: the table's entries are TS apart (tw[t TS] = exp(-2 pi i t / L)), so a table of
+// a longer length L TS serves.
+template <int L, int DIR, int TS = 1, typename C>
 __device__ __forceinline__ void fft_reg(C* v, const C* __restrict__ tw) {
-  fft_reg_stages<L, 0, DIR>(v, tw);
+  fft_reg_stages<L, 0, DIR, TS>(v, tw);
 }
 
 }  // namespace msc

@@ -191,6 +191,8 @@ template <typename T>
 __global__ void __launch_bounds__(NTH) k_mdot(const cx<T>* __restrict__ V, size_t n, int nv, const double* scale,
                                               const cx<T>* __restrict__ w, double2* part, int* counter, double2* out,
                                               const int* done) {
+  pdl_wait();
+  pdl_trigger();
   if (done && *done) return;
   __shared__ double2 sh[NTH / 32][33];
   const int lane = threadIdx.x & 31, wp = threadIdx.x >> 5;
@@ -386,6 +388,8 @@ __global__ void __launch_bounds__(NTH) k_maxpy(const cx<T>* __restrict__ V, size
                                                const double2* coef, cx<T>* __restrict__ w, double2* part, int* counter,
                                                double2* out_norm, const int* done, GState* st, HessPtr hp, int m,
                                                int j, int cgs2) {
+  pdl_wait();
+  pdl_trigger();
   if (done && *done) return;
   __shared__ cx<T> cf[32];
   if (threadIdx.x < 32) {
@@ -549,8 +553,14 @@ static int mdot(msc_plan* pl, GmresWork* gw, const cx<T>* V, int nv, const doubl
   GState* st = (GState*)gw->state.p;
   double2* part = (double2*)gw->part.p;
   const int nb = std::min<long long>(NB, ceil_div((long long)gw->n, (long long)NTH * EPT));
-  k_mdot<T><<<nb, NTH, 0, pl->stream>>>(V, gw->n, nv, scale, w, part, &st->counter[0], out, done); ::msc::note_launch();
-  MSC_CUDA(cudaGetLastError());
+  size_t n = gw->n;
+  int* counter = &st->counter[0];
+  void* args[] = {(void*)&V, (void*)&n, (void*)&nv, (void*)&scale, (void*)&w, (void*)&part, (void*)&counter,
+                  (void*)&out, (void*)&done};
+  // an ordinary launch: with programmatic dependent launch the Arnoldi kernels made the
+  // cfg2 solve 8% slower (the matvec kernels, which gain from it, keep it)
+  MSC_CUDA(cudaLaunchKernel((const void*)k_mdot<T>, dim3(nb), dim3(NTH), args, 0, pl->stream));
+  ::msc::note_launch();
   return MSC_OK;
 }
 
@@ -561,10 +571,16 @@ static int maxpy(msc_plan* pl, GmresWork* gw, const cx<T>* V, int nv, const doub
   GState* st = (GState*)gw->state.p;
   double2* part = (double2*)gw->part.p;
   const int nb = std::min<long long>(NB, ceil_div((long long)gw->n, (long long)NTH * EPT));
-  k_maxpy<T, NORM><<<nb, NTH, 0, pl->stream>>>(V, gw->n, nv, scale, coef, w, part, &st->counter[1], out_norm, done,
-                                               giv_j >= 0 ? st : nullptr, hess_ptrs(gw), m, giv_j, cgs2 ? 1 : 0);
+  size_t n = gw->n;
+  int* counter = &st->counter[1];
+  GState* gst = giv_j >= 0 ? st : nullptr;
+  HessPtr hp = hess_ptrs(gw);
+  int c2 = cgs2 ? 1 : 0;
+  void* args[] = {(void*)&V, (void*)&n, (void*)&nv, (void*)&scale, (void*)&coef, (void*)&w, (void*)&part,
+                  (void*)&counter, (void*)&out_norm, (void*)&done, (void*)&gst, (void*)&hp, (void*)&m,
+                  (void*)&giv_j, (void*)&c2};
+  MSC_CUDA(cudaLaunchKernel((const void*)k_maxpy<T, NORM>, dim3(nb), dim3(NTH), args, 0, pl->stream));
   ::msc::note_launch();
-  MSC_CUDA(cudaGetLastError());
   return MSC_OK;
 }
 

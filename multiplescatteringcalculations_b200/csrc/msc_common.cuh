@@ -70,6 +70,29 @@ template <typename C> __device__ __forceinline__ C from_d(double2 a) { return to
 __device__ __forceinline__ float2 ld_stream(const float2* p) { return __ldcs(p); }
 __device__ __forceinline__ double2 ld_stream(const double2* p) { return __ldcs(p); }
 
+// Programmatic dependent launch. A kernel launched by launch_pdl may be scheduled while
+// its predecessor in the stream is still draining; it calls pdl_wait() (griddepcontrol.
+// wait: blocks until the predecessor grid has completed and its writes are visible; a
+// no-op for an ordinary launch) before it reads anything, and pdl_trigger() to let its
+// own successor's blocks be scheduled once every block of this grid has issued it. The
+// successor's blocks then wait in hardware, not in a spin loop.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;\n" ::: "memory"); }
+__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;\n" ::: "memory"); }
+
+inline cudaError_t launch_pdl(const void* f, dim3 grid, dim3 block, void** args, size_t smem, cudaStream_t st) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelExC(&cfg, f, args);
+}
+
 // Asynchronous global -> shared copies (cp.async): one complex element per call,
 // zero-filled without a read when ok is false (src must still be a valid address).
 // Many copies stay in flight per thread; cp_async_wait_all() then a barrier

@@ -1,4 +1,6 @@
 // Line FFT along the contiguous axis (the x passes of the matvec and of the G0 build).
+#include <cstdint>
+
 #include "mv_common.cuh"
 
 namespace msc {
@@ -15,6 +17,8 @@ template <typename T, int DIR, bool POW2, int LC, bool PR>
 __global__ void __launch_bounds__(256, 4) k_fft_contig(const cx<T>* in, cx<T>* out, long long nlines, long long G,
                                                        long long GS, long long stride, int n_in, int n_out,
                                                        FftPlan1D pl, const cx<T>* __restrict__ twg, const int* done) {
+  pdl_wait();
+  pdl_trigger();
   if (done && *done) return;
   using C = cx<T>;
   constexpr int TL = Tile<T>::W;
@@ -82,6 +86,81 @@ __global__ void __launch_bounds__(256, 4) k_fft_contig(const cx<T>* in, cx<T>* o
   }
 }
 
+// ---- register four-step engine (complex64, L = 64, 128, 256) -------------------------
+// A line of L = R1 * NTL points is held by NTL consecutive threads of a warp, R1 points
+// each: thread t holds x[t + NTL m], m < R1. Four steps: an R1-point DFT over m in
+// registers, the twiddle W_L^(t k1), a transpose through shared memory within the warp
+// (__syncwarp only; no block barrier), an NTL-point DFT over t in registers. Thread t
+// then holds X[k1 + R1 k2] for its KPT = R1 / NTL values of k1 and every k2. Shared
+// memory per line: R1 rows of NTL + 1 entries (the odd row pitch spreads a reader's
+// rows over the banks), lines padded to alternate bank halves.
+template <int L> struct RowReg {
+  static constexpr int NTL = L >= 256 ? 16 : 8;
+  static constexpr int R1 = L / NTL;
+  static constexpr int KPT = R1 / NTL;
+  static constexpr int LPB = 256 / NTL;  // lines per block
+  static constexpr int RS = NTL + 1;     // row pitch
+  static constexpr int LS0 = R1 * RS;
+  static constexpr int LS = ((LS0 * 8 / 4) % 32 == 16) ? LS0 : LS0 + 8;  // line pitch (complex)
+};
+
+template <int DIR, int L>
+__global__ void __launch_bounds__(256) k_fft_rows_reg(const float2* __restrict__ in, float2* __restrict__ out,
+                                                      long long nlines, long long G, long long GS, long long stride,
+                                                      int n_in, int n_out, const float2* __restrict__ twg,
+                                                      const int* done) {
+  pdl_wait();
+  pdl_trigger();
+  if (done && *done) return;
+  using RR = RowReg<L>;
+  constexpr int NTL = RR::NTL, R1 = RR::R1, KPT = RR::KPT, LPB = RR::LPB, RS = RR::RS, LS = RR::LS;
+  static_assert(R1 % NTL == 0, "R1 a multiple of NTL");
+  __shared__ __align__(16) float2 sm[LPB * LS];
+  const int q = threadIdx.x / NTL, t = threadIdx.x % NTL;
+  const long long line = (long long)blockIdx.x * LPB + q;
+  const long long off = line < nlines ? (line / G) * GS + (line % G) * stride : -1;
+  float2 v[R1];
+#pragma unroll
+  for (int m = 0; m < R1; ++m) {
+    const int n = t + NTL * m;
+    v[m] = (off >= 0 && n < n_in) ? in[off + n] : make_float2(0.f, 0.f);
+  }
+  fft_reg<R1, DIR, L / R1>(v, twg);
+#pragma unroll
+  for (int k1 = 1; k1 < R1; ++k1) {
+    float2 w = __ldg(twg + ((t * k1) & (L - 1)));
+    if (DIR > 0) w.y = -w.y;
+    v[k1] = v[k1] * w;
+  }
+  float2* ls = sm + q * LS;
+#pragma unroll
+  for (int k1 = 0; k1 < R1; ++k1) ls[k1 * RS + t] = v[k1];
+  __syncwarp();
+  float2 u[KPT][NTL];
+#pragma unroll
+  for (int c = 0; c < KPT; ++c)
+#pragma unroll
+    for (int s = 0; s < NTL; ++s) u[c][s] = ls[(t * KPT + c) * RS + s];
+#pragma unroll
+  for (int c = 0; c < KPT; ++c) fft_reg<NTL, DIR, L / NTL>(u[c], twg);
+  if (off < 0) return;
+  float2* o = out + off;
+#pragma unroll
+  for (int k2 = 0; k2 < NTL; ++k2) {
+    const int k = t * KPT + R1 * k2;
+    if constexpr (KPT == 2) {
+      if (k + 1 < n_out)
+        *reinterpret_cast<float4*>(o + k) = make_float4(u[0][k2].x, u[0][k2].y, u[1][k2].x, u[1][k2].y);
+      else if (k < n_out)
+        o[k] = u[0][k2];
+    } else {
+#pragma unroll
+      for (int c = 0; c < KPT; ++c)
+        if (k + c < n_out) o[k + c] = u[c][k2];
+    }
+  }
+}
+
 template <typename T>
 int launch_fft_contig(msc_plan* pl, const cx<T>* in, cx<T>* out, long long nlines, long long G, long long GS,
                       long long stride, int n_in, int n_out, const FftPlan1D& f, const cx<T>* tw, int dir,
@@ -107,11 +186,34 @@ int launch_fft_contig(msc_plan* pl, const cx<T>* in, cx<T>* out, long long nline
   if (dir < 0) { PICK(-1) } else { PICK(+1) }
 #undef PICK
 #undef LEN
+  if constexpr (sizeof(T) == 4) {
+    // register four-step engine: complex64, L = 64, 128, 256, even line offsets (16-byte stores)
+    const bool even = (GS % 2 == 0) && (stride % 2 == 0) && ((reinterpret_cast<uintptr_t>(out) & 15) == 0);
+    const void* rk = nullptr;
+    int lpb = 0;
+#define RR(D, LL) rk = (const void*)k_fft_rows_reg<D, LL>; lpb = RowReg<LL>::LPB;
+    if (even && f.pow2) {
+      if (dir < 0) {
+        if (f.L == 64) { RR(-1, 64) } else if (f.L == 128) { RR(-1, 128) } else if (f.L == 256) { RR(-1, 256) }
+      } else {
+        if (f.L == 64) { RR(+1, 64) } else if (f.L == 128) { RR(+1, 128) } else if (f.L == 256) { RR(+1, 256) }
+      }
+    }
+#undef RR
+    if (rk) {
+      const unsigned nbr = (unsigned)((nlines + lpb - 1) / lpb);
+      void* args[] = {(void*)&in, (void*)&out, (void*)&nlines, (void*)&G, (void*)&GS, (void*)&stride,
+                      (void*)&n_in, (void*)&n_out, (void*)&tw, (void*)&done};
+      MSC_CUDA(launch_pdl(rk, dim3(nbr), dim3(256), args, 0, pl->stream));
+      ::msc::note_launch();
+      return MSC_OK;
+    }
+  }
   MSC_CUDA(prep_kernel(kern));
   FftPlan1D ff = f;
   void* args[] = {(void*)&in, (void*)&out, (void*)&nlines, (void*)&G, (void*)&GS, (void*)&stride,
                   (void*)&n_in, (void*)&n_out, (void*)&ff, (void*)&tw, (void*)&done};
-  MSC_CUDA(cudaLaunchKernel(kern, dim3(nb), dim3(nthr), args, sm, pl->stream));
+  MSC_CUDA(launch_pdl(kern, dim3(nb), dim3(nthr), args, sm, pl->stream));
   ::msc::note_launch();
   return MSC_OK;
 }

@@ -22,6 +22,8 @@ template <typename T, bool POW2, int LC, bool PR>
 __global__ void __launch_bounds__(256, 4) k_t0_fft_y(const cx<T>* __restrict__ x, const double* scale,
                                                      const cx<T>* __restrict__ t4, cx<T>* __restrict__ W, Geo g,
                                                      FftPlan1D pl, const cx<T>* __restrict__ twg, const int* done) {
+  pdl_wait();
+  pdl_trigger();
   if (done && *done) return;
   using C = cx<T>;
   constexpr int TR = Tile<T>::W;
@@ -98,7 +100,7 @@ int launch_t0_fft_y(msc_plan* pl, const cx<T>* x, const double* scale, cx<T>* W,
   Geo gg = g;
   FftPlan1D ff = pl->fxy;
   void* args[] = {(void*)&x, (void*)&scale, (void*)&t4, (void*)&W, (void*)&gg, (void*)&ff, (void*)&tw, (void*)&done};
-  MSC_CUDA(cudaLaunchKernel(kern, grid, dim3(nthr), args, sm, pl->stream));
+  MSC_CUDA(launch_pdl(kern, grid, dim3(nthr), args, sm, pl->stream));
   ::msc::note_launch();
   return MSC_OK;
 }

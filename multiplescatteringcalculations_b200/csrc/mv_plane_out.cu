@@ -11,6 +11,8 @@ template <typename T, bool POW2, int LC, bool PR>
 __global__ void __launch_bounds__(256, 4) k_fft_y_out(const cx<T>* __restrict__ W, const cx<T>* __restrict__ x,
                                                       const double* scale, cx<T>* __restrict__ y, Geo g,
                                                       FftPlan1D pl, const cx<T>* __restrict__ twg, const int* done) {
+  pdl_wait();
+  pdl_trigger();
   if (done && *done) return;
   using C = cx<T>;
   constexpr int TR = Tile<T>::W;
@@ -80,7 +82,7 @@ int launch_fft_y_out(msc_plan* pl, const cx<T>* W, const cx<T>* x, const double*
   Geo gg = g;
   FftPlan1D ff = pl->fxy;
   void* args[] = {(void*)&W, (void*)&x, (void*)&scale, (void*)&y, (void*)&gg, (void*)&ff, (void*)&tw, (void*)&done};
-  MSC_CUDA(cudaLaunchKernel(kern, grid, dim3(nthr), args, sm, pl->stream));
+  MSC_CUDA(launch_pdl(kern, grid, dim3(nthr), args, sm, pl->stream));
   ::msc::note_launch();
   return MSC_OK;
 }

@@ -16,6 +16,8 @@ __global__ void __launch_bounds__(256, 3) k_fft_strided(const cx<T>* in, long lo
                                                         cx<T>* out, long long eo, long long O1, long long O2,
                                                         float2* out32, int ncol, int TC, int n_in, int n_out,
                                                         FftPlan1D pl, const cx<T>* __restrict__ twg, const int* done) {
+  pdl_wait();
+  pdl_trigger();
   if (done && *done) return;
   using C = cx<T>;
   extern __shared__ __align__(16) unsigned char smem_raw[];

@@ -114,6 +114,8 @@ template <typename T, int LC, int KXC, bool SYM, bool OCT, bool POW2>
 __global__ void __launch_bounds__(ZBZ_THREADS, 2) k_zbz(cx<T>* __restrict__ W, const kent<T>* __restrict__ khat, Geo g,
                                                         ZbzLayout lay, FftPlan1D pl, const cx<T>* __restrict__ twg,
                                                         const int* done) {
+  pdl_wait();
+  pdl_trigger();
   if (done && *done) return;
   using C = cx<T>;
   using KE = kent<T>;
@@ -259,6 +261,8 @@ template <typename T, int LC, int KXC, bool SYM>
 __global__ void __launch_bounds__(zbz_reg_threads<KXC>(), 3)
     k_zbz_reg(cx<T>* __restrict__ W, const kent<T>* __restrict__ khat, Geo g, ZbzLayout lay,
               const cx<T>* __restrict__ twg, const int* done) {
+  pdl_wait();
+  pdl_trigger();
   if (done && *done) return;
   using C = cx<T>;
   using KE = kent<T>;
@@ -408,7 +412,7 @@ int launch_zbz(msc_plan* pl, cx<T>* W, const int* done) {
         Geo gg = g;
         ZbzLayout ll = lay;
         void* args[] = {(void*)&W, (void*)&kh, (void*)&gg, (void*)&ll, (void*)&tw, (void*)&done};
-        MSC_CUDA(cudaLaunchKernel(rk, grid, dim3(nt), args, sm, pl->stream));
+        MSC_CUDA(launch_pdl(rk, grid, dim3(nt), args, sm, pl->stream));
         ::msc::note_launch();
         return MSC_OK;
       }
@@ -426,7 +430,7 @@ int launch_zbz(msc_plan* pl, cx<T>* W, const int* done) {
   ZbzLayout ll = lay;
   FftPlan1D ff = pl->fz;
   void* args[] = {(void*)&W, (void*)&kh, (void*)&gg, (void*)&ll, (void*)&ff, (void*)&tw, (void*)&done};
-  MSC_CUDA(cudaLaunchKernel(kern, grid, dim3(ZBZ_THREADS), args, lay.smem, pl->stream));
+  MSC_CUDA(launch_pdl(kern, grid, dim3(ZBZ_THREADS), args, lay.smem, pl->stream));
   ::msc::note_launch();
   return MSC_OK;
 }

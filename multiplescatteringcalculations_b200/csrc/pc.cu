@@ -198,6 +198,8 @@ __global__ void __launch_bounds__(256, 2) k_nf32(const float2* __restrict__ x, c
                                               float2* __restrict__ acc, float2 ch, float2 c0, int init,
                                               const float2* __restrict__ G, const __nv_bfloat162* __restrict__ G16,
                                               Geo g, const int* done) {
+  pdl_wait();
+  pdl_trigger();
   if (done && *done) return;
   nf_body<float>(x, scale, t4, h, acc, ch, c0, init, G, G16, g);
 }
@@ -206,6 +208,8 @@ __global__ void __launch_bounds__(256) k_nf64(const double2* __restrict__ x, con
                                               const double2* __restrict__ t4, double2* __restrict__ h,
                                               double2* __restrict__ acc, double2 ch, double2 c0, int init,
                                               const double2* __restrict__ G, Geo g, const int* done) {
+  pdl_wait();
+  pdl_trigger();
   if (done && *done) return;
   nf_body<double>(x, scale, t4, h, acc, ch, c0, init, G, nullptr, g);
 }
