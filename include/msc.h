@@ -203,7 +203,7 @@ typedef struct msc_batch_item {
 /* Solve n independent slabs (uneven sizes, frequencies and incidences) on the
  * current device: T0 and G0 builds, incident field, solve with opts, R_PP and the
  * field, per item. `workers` host threads with a stream and a plan cache each run
- * items concurrently (0 = choose by timing the first items at 2, 4 and 8 workers;
+ * items concurrently (0 = choose by timing the first items at 1, 2 and 4 workers;
  * the count used is written to *workers_used when not NULL). Returns MSC_OK when
  * every item converged, MSC_NOT_CONVERGED when any item failed or did not converge
  * (its own status and message say which), negative only for errors of the call

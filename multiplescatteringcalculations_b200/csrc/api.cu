@@ -1,6 +1,8 @@
 // C-ABI entry points of libmsc_b200.so (declared in include/msc.h).
+#include <algorithm>
 #include <atomic>
 #include <cstdarg>
+#include <mutex>
 #include <cstdio>
 #include <cstring>
 
@@ -25,6 +27,49 @@ void set_error(const char* fmt, ...) {
 // allocation or a release never synchronises the device, so plans on different
 // streams (the batch workers) build and solve concurrently. A reallocation bumps
 // the plan's generation, which invalidates its captured solver graphs.
+//
+// The allocations draw on one memory pool of the library per device whose release
+// threshold is 1/8 of the device memory, at most 16 GiB: memory freed by a plan stays
+// reserved up to that amount and the next plan (a batch over slabs of many shapes
+// creates and destroys plans all the time) reuses it without mapping it again, which
+// the default pool (threshold 0) does at every synchronisation. Above the threshold the
+// pool returns memory to the driver at synchronisation.
+namespace {
+std::mutex g_pool_mu;
+cudaMemPool_t g_pools[64] = {};
+}  // namespace
+
+cudaMemPool_t device_pool(int device) {
+  if (device < 0 || device >= 64) return nullptr;
+  std::lock_guard<std::mutex> lk(g_pool_mu);
+  if (!g_pools[device]) {
+    cudaMemPoolProps props = {};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = device;
+    cudaMemPool_t pool = nullptr;
+    if (cudaMemPoolCreate(&pool, &props) != cudaSuccess) {
+      cudaGetLastError();
+      return nullptr;
+    }
+    size_t fr = 0, total = 0;
+    if (cudaMemGetInfo(&fr, &total) != cudaSuccess) {
+      cudaGetLastError();
+      total = 0;
+    }
+    uint64_t thr = std::min<uint64_t>(16ull << 30, total / 8);
+    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
+    g_pools[device] = pool;
+  }
+  return g_pools[device];
+}
+
+cudaError_t pool_alloc(void** p, size_t bytes, int device, cudaStream_t st) {
+  cudaMemPool_t pool = device_pool(device);
+  if (!pool) return cudaMallocAsync(p, bytes, st);
+  return cudaMallocFromPoolAsync(p, bytes, pool, st);
+}
+
 int dalloc(msc_plan* pl, DBuf& b, size_t bytes) {
   if (b.p && b.bytes >= bytes) return MSC_OK;
   cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
@@ -35,10 +80,10 @@ int dalloc(msc_plan* pl, DBuf& b, size_t bytes) {
   if (b.p) dfree(pl, b);
   if (bytes == 0) bytes = 16;
   void* p = nullptr;
-  cudaError_t e = cudaMallocAsync(&p, bytes, pl->stream);
+  cudaError_t e = pool_alloc(&p, bytes, pl->device, pl->stream);
   if (e != cudaSuccess) {
     cudaGetLastError();
-    set_error("cudaMallocAsync of %zu bytes failed: %s", bytes, cudaGetErrorString(e));
+    set_error("device allocation of %zu bytes failed: %s", bytes, cudaGetErrorString(e));
     return MSC_ERR_NOMEM;
   }
   b.p = p;

@@ -5,9 +5,11 @@
 // slab is a few microseconds of launches on a few dozen SMs), so the batch runs
 // several solves at once: `workers` host threads each own a stream, a small cache
 // of plans (LRU, keyed by geometry and background) and pinned staging buffers, and
-// take items from a shared counter. Every plan's work runs on its own stream with
-// graph-captured GMRES cycles, so the solves of different workers overlap on the
-// device. With workers = 0 an online autotuner times the first items at 2, 4 and 8
+// take items from a shared counter. Every plan's work runs on its own stream, so the
+// solves of different workers overlap on the device; their GMRES cycles run
+// uncaptured (a graph capture per new plan costs more than a short solve saves).
+// Plan memory comes from the library's memory pool, so the plan churn of a batch over
+// many shapes reuses device memory instead of mapping it again. With workers = 0 an online autotuner times the first items at 1, 2 and 4
 // workers and finishes the batch with the fastest. Items are independent: a failed
 // item records its status and the others continue.
 #include <algorithm>
@@ -34,6 +36,7 @@ struct CachedPlan {
 
 struct Worker {
   cudaStream_t stream = nullptr;
+  int device = 0;
   std::vector<CachedPlan> plans;
   long long tick = 0;
   // device staging: contrasts (3 N float64), psi0 and x (9 N complex128 each)
@@ -74,6 +77,9 @@ struct Worker {
     msc_plan* p = nullptr;
     const int s = msc_plan_create(&d, stream, &p);
     if (s != MSC_OK) return s;
+    // a batch item is one short solve on a plan that is rarely reused: capturing and
+    // instantiating its GMRES cycles costs more than it saves
+    p->graphs = false;
     CachedPlan c;
     std::memcpy(&c.key, &d, sizeof(d));
     c.plan = p;
@@ -88,7 +94,7 @@ struct Worker {
       if (dev) cudaFreeAsync(dev, stream);
       dev = nullptr;
       dev_bytes = 0;
-      if (cudaMallocAsync(&dev, dbytes, stream) != cudaSuccess) {
+      if (pool_alloc(&dev, dbytes, device, stream) != cudaSuccess) {
         cudaGetLastError();
         set_error("batch: device staging of %zu bytes failed", dbytes);
         return MSC_ERR_NOMEM;
@@ -211,26 +217,30 @@ extern "C" int msc_batch_solve(msc_batch_item* items, int n, const msc_solve_opt
   }
   int device = 0;
   MSC_CUDA(cudaGetDevice(&device));
-  const int maxw = workers > 0 ? workers : 8;
+  const int maxw = workers > 0 ? workers : 4;
   std::vector<Worker> pool(maxw);
-  for (auto& w : pool) MSC_CUDA(cudaStreamCreateWithFlags(&w.stream, cudaStreamNonBlocking));
+  for (auto& w : pool) {
+    w.device = device;
+    MSC_CUDA(cudaStreamCreateWithFlags(&w.stream, cudaStreamNonBlocking));
+  }
   std::atomic<int> next{0};
   int chosen = workers;
   if (workers == 0) {
-    // online autotune: a chunk of items at 2, 4 and 8 workers, time per item compared
+    // online autotune: chunks of items at 1, 2 and 4 workers, time per item compared;
+    // the search stops at the first count that is slower than the best so far (more
+    // threads contend for the driver as well as the device)
     const int chunk = std::max(2, std::min(16, n / 8));
     double best = 1e300;
-    chosen = 2;
-    for (int w : {2, 4, 8}) {
+    chosen = 1;
+    for (int w : {1, 2, 4}) {
       const int start = next.load();
       if (start >= n) break;
-      const int end = std::min(n, start + chunk * w / 2);
+      const int end = std::min(n, start + std::max(1, chunk * w / 2));
       const double t = run_workers(pool, w, items, next, end, *opts, device);
       const double per = t / std::max(1, end - start);
-      if (per < best) {
-        best = per;
-        chosen = w;
-      }
+      if (per >= best) break;
+      best = per;
+      chosen = w;
     }
   }
   if (next.load() < n) run_workers(pool, chosen, items, next, n, *opts, device);

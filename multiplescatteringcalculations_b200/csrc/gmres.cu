@@ -57,7 +57,7 @@ struct GmresWork {
     int m = 0;
     bool cgs2 = false;
     uint64_t gen = 0;
-    bool warm = false;  // a cycle of this kind ran uncaptured: kernel attributes set, buffers allocated
+    int warm = 0;  // cycles of this kind run uncaptured (kernel attributes set, buffers allocated)
   } graph[2][2];
 };
 
@@ -702,11 +702,13 @@ static int gmres_core(msc_plan* pl, int m, const cx<T>* rhs, cx<T>* x, bool x_ze
     GState cur;
     auto& gr = gw->graph[sizeof(T) == 8 ? 1 : 0][use_pc ? 1 : 0];
     // A whole cycle as one captured graph: m steps whose kernels return at once
-    // after the device flag `done` is set. Used from the second cycle of a plan
-    // generation on (buffers allocated, kernel attributes set) and when the budget
-    // covers m steps.
+    // after the device flag `done` is set. Captured after two uncaptured cycles of the
+    // kind (buffers allocated, kernel attributes set; a solve of one or two cycles on a
+    // short-lived plan does not repay the capture and instantiation) when the budget
+    // covers m steps, and replayed while the plan generation holds. Plans with graphs
+    // off (the batch's) always run uncaptured.
     const bool graph_ok = gr.exec && gr.m == m && gr.cgs2 == cgs2 && gr.gen == pl->gen;
-    if ((graph_ok || gr.warm) && used + m <= max_mv) {
+    if (pl->graphs && (graph_ok || gr.warm >= 2) && used + m <= max_mv) {
       if (!graph_ok) {
         if (use_pc) MSC_TRY(nearfield_refresh(pl));
         if (gr.exec) cudaGraphExecDestroy(gr.exec);
@@ -765,7 +767,7 @@ static int gmres_core(msc_plan* pl, int m, const cx<T>* rhs, cx<T>* x, bool x_ze
       MSC_CUDA(cudaMemcpyAsync(&gw->hstate[0], st, sizeof(GState), cudaMemcpyDeviceToHost, pl->stream));
       MSC_CUDA(cudaStreamSynchronize(pl->stream));
       cur = gw->hstate[0];
-      gr.warm = true;
+      gr.warm += 1;
     }
     // x += V y (k columns), or Z y with the preconditioner
     if (cur.k > 0) {

@@ -96,6 +96,8 @@ struct msc_plan {
   // bumped by every (re)allocation, spectrum build and preconditioner change: the
   // captured solver graphs of an older generation are stale
   uint64_t gen = 1;
+  // capture GMRES cycles into graphs (off for the batch's short-lived plans)
+  bool graphs = true;
 };
 
 namespace msc {
@@ -120,6 +122,8 @@ struct StreamFence {
 
 int dalloc(msc_plan* pl, DBuf& b, size_t bytes);
 void dfree(msc_plan* pl, DBuf& b);
+// stream-ordered allocation from the library's memory pool of `device`
+cudaError_t pool_alloc(void** p, size_t bytes, int device, cudaStream_t st);
 
 // ---- launches (all enqueue on pl->stream) ------------------------------------
 int build_twiddles(msc_plan* pl);
