@@ -42,7 +42,7 @@ struct Worker {
   // device staging: contrasts (3 N float64), psi0 and x (9 N complex128 each)
   void* dev = nullptr;
   size_t dev_bytes = 0;
-  // pinned host staging for the contrasts and the solution
+  // pinned host staging for the contrasts
   void* host = nullptr;
   size_t host_bytes = 0;
 
@@ -122,7 +122,7 @@ struct Worker {
     MSC_TRY(plan_for(it.desc, &pl));
     const size_t ns = (size_t)it.desc.N_z * it.desc.M * it.desc.M;
     const size_t fb = sizeof(double2) * 9 * ns;
-    MSC_TRY(staging(3 * sizeof(double) * ns + 2 * fb, std::max(3 * sizeof(double) * ns, fb)));
+    MSC_TRY(staging(3 * sizeof(double) * ns + 2 * fb, 3 * sizeof(double) * ns));
     double* dc = (double*)dev;
     double2* psi0 = (double2*)(dc + 3 * ns);
     double2* x = psi0 + 9 * ns;
@@ -151,9 +151,10 @@ struct Worker {
     const double p = it.bloch ? std::sqrt(it.k_hat[1] * it.k_hat[1] + it.k_hat[2] * it.k_hat[2]) / nk / speed : 0.0;
     MSC_TRY(msc_rpp_periodic(pl, x, it.omega, p, it.bloch ? MSC_RPP_BLOCH : 0, it.rpp));
     if (it.psi) {
-      MSC_CUDA(cudaMemcpyAsync(host, x, fb, cudaMemcpyDeviceToHost, stream));
+      // straight into the caller's array: a second copy through the pinned staging
+      // buffer costs a host memcpy at single-thread bandwidth
+      MSC_CUDA(cudaMemcpyAsync(it.psi, x, fb, cudaMemcpyDeviceToHost, stream));
       MSC_CUDA(cudaStreamSynchronize(stream));
-      std::memcpy(it.psi, host, fb);
     }
     return s;
   }
