@@ -24,6 +24,15 @@ int launch_matvec_ws(msc_plan* pl, const cx<T>* x, const double* scale, cx<T>* y
     set_error("matvec needs build_t0 and build_g0 first");
     return MSC_ERR_STATE;
   }
+  if constexpr (sizeof(T) == 4) {
+    // aperiodic, Lx = Ly in {64, 128}: the y and x passes of each direction fused per plane
+    if (plane_fused_ok(pl)) {
+      MSC_TRY(launch_plane_fwd(pl, x, scale, W, done));    // A + X
+      MSC_TRY(launch_zbz<T>(pl, W, done));                 // ZBZ'
+      MSC_TRY(launch_plane_inv(pl, W, x, scale, y, done)); // X' + C
+      return MSC_OK;
+    }
+  }
   const cx<T>* twxy = (const cx<T>*)(sizeof(T) == 8 ? pl->tw64_xy.p : pl->tw32_xy.p);
   const long long G = (long long)9 * g.Nz * g.Ly;  // x lines, contiguous rows of W
   MSC_TRY(launch_t0_fft_y<T>(pl, x, scale, W, twxy, done));                                       // A

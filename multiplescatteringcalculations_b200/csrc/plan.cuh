@@ -139,6 +139,11 @@ int launch_soa_to_ref(msc_plan* pl, const cx<Tin>* in, cx<Tout>* out);
 // y = x - G0 T0 (scale * x), SoA; scale may be null (1). done may be null.
 template <typename T>
 int launch_matvec(msc_plan* pl, const cx<T>* x, const double* scale, cx<T>* y, const int* done);
+// complex64 plane passes with the y and x transforms fused (mv_plane_fused.cu)
+bool plane_fused_ok(const msc_plan* pl);
+int launch_plane_fwd(msc_plan* pl, const float2* x, const double* scale, float2* W, const int* done);
+int launch_plane_inv(msc_plan* pl, const float2* W, const float2* x, const double* scale, float2* y,
+                     const int* done);
 // the same on a caller-provided workspace of ws_elems(g) elements
 template <typename T>
 int launch_matvec_ws(msc_plan* pl, const cx<T>* x, const double* scale, cx<T>* y, cx<T>* W, const int* done);
