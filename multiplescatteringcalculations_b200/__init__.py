@@ -30,5 +30,6 @@ from .slab import (  # noqa: F401
 )
 
 from .learned import NearFieldPreconditioner, fgmres_matvecs, solver_residuals, train_nearfield  # noqa: F401,E402
+from .sphere import SphereDecompositionResult, compute_sphere_foldy_lax_fft_gpu, sphere_grid  # noqa: F401,E402
 
 __version__ = "0.1.0"

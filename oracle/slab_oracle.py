@@ -904,3 +904,77 @@ def nearfield_residual_loss_grad(r, t4, kernel_hat, blocks, M, N_z, coef, w=None
         if l > 1:
             delta = np.conj(coef[l - 1]) * d + nearfield_stencil_adjoint(delta, t4, lay[l - 1], M, N_z)
     return loss, gc, gw
+
+
+# ---------------------------------------------------------------------------
+# 10. Sphere FFT Foldy-Lax (sphere_scattering_fft.py:42-330) on the slab operator
+# ---------------------------------------------------------------------------
+
+
+def sphere_grid(radius, n_sub):
+    """Cells of the n_sub^3 cube grid inside the sphere (sphere_scattering_fft.py:42-80):
+    centre coordinates (-n/2 + 1/2 + i) d per axis, d = 2 a_sub, a_sub = radius / n_sub,
+    kept when |centre| < radius. Returns (grid_idx (N, 3), centres (N, 3), a_sub)."""
+    a_sub = radius / n_sub
+    d = 2.0 * a_sub
+    c1 = (-n_sub / 2.0 + 0.5 + np.arange(n_sub)) * d
+    g = np.stack(np.meshgrid(c1, c1, c1, indexing="ij"), -1).reshape(-1, 3)
+    idx = np.stack(np.meshgrid(*(np.arange(n_sub),) * 3, indexing="ij"), -1).reshape(-1, 3)
+    keep = np.linalg.norm(g, axis=1) < radius
+    return idx[keep], g[keep], a_sub
+
+
+_VOIGT_PAIRS = ((0, 0), (1, 1), (2, 2), (1, 2), (0, 2), (0, 1))
+
+
+def sphere_incident(centres, omega, alpha, beta, k_hat=None, wave_type="S"):
+    """The 9 incident patterns (9N, 9) of the coupled system
+    (resonance_tmatrix.py:526-586): columns 0-2 a uniform displacement e_p, columns 3-8
+    the displacement eps(e_alpha) (x - x_mean) with the Voigt strain e_alpha (engineering
+    shear: off-diagonal tensor entries 1/2), all times exp(i k k_hat . x)."""
+    k_hat = np.array([0.0, 0.0, 1.0]) if k_hat is None else np.asarray(k_hat, dtype=float)
+    k_hat = k_hat / np.linalg.norm(k_hat)
+    k = omega / (beta if wave_type == "S" else alpha)
+    ph = np.exp(1j * k * (centres @ k_hat))
+    dx = centres - centres.mean(axis=0)
+    N = len(centres)
+    U = np.zeros((N, 9, 9), dtype=complex)
+    for p in range(3):
+        U[:, p, p] = ph
+    for al, (p, q) in enumerate(_VOIGT_PAIRS):
+        e = np.zeros((3, 3))
+        if p == q:
+            e[p, p] = 1.0
+        else:
+            e[p, q] = e[q, p] = 0.5
+        U[:, :3, 3 + al] = (dx @ e.T) * ph[:, None]
+        U[:, 3 + al, 3 + al] = ph
+    return U.reshape(9 * N, 9)
+
+
+def sphere_foldy_lax(omega, radius, alpha, beta, rho, dlam, dmu, drho, n_sub, k_hat=None, wave_type="S",
+                     gmres_tol=1e-12):
+    """T_comp (9, 9) and psi_exc (9N, 9) of the sphere: the slab operator on the
+    n_sub^3 lattice (cube half-width a_sub, aperiodic) with the contrast inside the
+    sphere and none outside, so the outside cells carry no source and the inside block
+    is the reference's (I - P T) (sphere_scattering_fft.py:83-125, 184-225); scipy GMRES
+    per column from the Born guess; T_comp = sum over cells of T x."""
+    grid_idx, centres, a_sub = sphere_grid(radius, n_sub)
+    n = n_sub
+    mask = np.zeros((n, n, n), dtype=bool)
+    mask[tuple(grid_idx.T)] = True
+    t4 = t0_scalars(omega, a_sub, alpha, beta, rho, dlam * mask, dmu * mask, drho * mask)
+    kh = build_slab_kernels(n, n, a_sub, omega, alpha, beta, rho)
+    U = sphere_incident(centres, omega, alpha, beta, k_hat, wave_type)
+    N = len(centres)
+    A = LinearOperator((9 * n ** 3,) * 2, matvec=lambda v: slab_matvec(v, t4, kh, n, n), dtype=complex)
+    psi = np.zeros((9 * N, 9), dtype=complex)
+    Tc = np.zeros((9, 9), dtype=complex)
+    for col in range(9):
+        b = np.zeros((n, n, n, 9), dtype=complex)
+        b[tuple(grid_idx.T)] = U[:, col].reshape(N, 9)
+        x, _ = gmres(A, b.ravel(), x0=b.ravel().copy(), rtol=gmres_tol, maxiter=500, restart=30)
+        xf = x.reshape(n, n, n, 9)
+        psi[:, col] = xf[tuple(grid_idx.T)].ravel()
+        Tc[:, col] = apply_t0(t4, xf).reshape(-1, 9).sum(axis=0)
+    return Tc, psi, centres, a_sub

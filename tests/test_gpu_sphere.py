@@ -1,0 +1,64 @@
+"""Sphere FFT Foldy-Lax on the GPU (compute_sphere_foldy_lax_fft_gpu, on the slab plan
+and its CUDA kernels) against fixtures of the reference's CPU solver
+(tests/golden/make_sphere_golden.py: sphere_scattering_fft.py at scipy rtol 1e-12)."""
+
+from pathlib import Path
+
+import numpy as np
+import pytest
+import torch
+
+pytestmark = pytest.mark.gpu
+
+if not torch.cuda.is_available():  # pragma: no cover
+    pytest.skip("needs a CUDA device", allow_module_level=True)
+
+from multiplescatteringcalculations_b200 import (  # noqa: E402
+    MaterialContrast,
+    ReferenceMedium,
+    compute_sphere_foldy_lax_fft_gpu,
+)
+
+GOLD = np.load(Path(__file__).parent / "golden" / "sphere.npz")
+REF = ReferenceMedium(float(GOLD["alpha"]), float(GOLD["beta"]), float(GOLD["rho"]))
+CON = MaterialContrast(float(GOLD["Dlambda"]), float(GOLD["Dmu"]), float(GOLD["Drho"]))
+
+
+def _rel(a, b):
+    return np.linalg.norm(np.asarray(a) - np.asarray(b)) / np.linalg.norm(np.asarray(b))
+
+
+def _run(k, **kw):
+    kh = GOLD[f"c{k}_k_hat"]
+    return compute_sphere_foldy_lax_fft_gpu(float(GOLD[f"c{k}_omega"]), float(GOLD[f"c{k}_radius"]), REF, CON,
+                                            int(GOLD[f"c{k}_n_sub"]), None if kh.size == 0 else kh,
+                                            str(GOLD[f"c{k}_wave"]), **kw)
+
+
+@pytest.mark.parametrize("k", range(int(GOLD["n_cases"])))
+def test_sphere_fp64_matches_reference(k):
+    r = _run(k, gmres_tol=1e-12, gmres_maxiter=2000, precision="fp64")
+    assert r.n_cells == len(GOLD[f"c{k}_centres"])
+    assert np.array_equal(r.centres, GOLD[f"c{k}_centres"])
+    assert _rel(r.T_comp_9x9, GOLD[f"c{k}_T_comp"]) < 1e-10
+    assert _rel(r.psi_exc, GOLD[f"c{k}_psi_exc"]) < 1e-10
+    assert np.array_equal(r.T3x3, r.T_comp_9x9[:3, :3])
+    assert all(st["residual"] <= 1e-12 for st in r.stats)
+
+
+@pytest.mark.parametrize("k", range(int(GOLD["n_cases"])))
+def test_sphere_mixed_precision(k):
+    """complex64 GMRES inside FP64 refinement reaches the FP64 answer to the tolerance."""
+    r = _run(k, gmres_tol=1e-10, gmres_maxiter=2000, precision="mixed")
+    assert _rel(r.T_comp_9x9, GOLD[f"c{k}_T_comp"]) < 1e-8
+    assert _rel(r.psi_exc, GOLD[f"c{k}_psi_exc"]) < 1e-8
+
+
+def test_sphere_zero_contrast_and_errors():
+    zero = MaterialContrast(0.0, 0.0, 0.0)
+    r = compute_sphere_foldy_lax_fft_gpu(500.0, 0.5, REF, zero, 4, wave_type="P")
+    assert np.all(r.T_comp_9x9 == 0)
+    with pytest.raises(ValueError):
+        compute_sphere_foldy_lax_fft_gpu(500.0, 0.5, REF, CON, 4, wave_type="X")
+    with pytest.raises(ValueError):
+        compute_sphere_foldy_lax_fft_gpu(500.0, -1.0, REF, CON, 4)
