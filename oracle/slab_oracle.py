@@ -952,6 +952,24 @@ def sphere_incident(centres, omega, alpha, beta, k_hat=None, wave_type="S"):
     return U.reshape(9 * N, 9)
 
 
+def sphere_foldy_lax_column(omega, radius, alpha, beta, rho, dlam, dmu, drho, n_sub, k_hat, wave_type, col,
+                            gmres_tol=1e-12):
+    """Column ``col`` of the sphere system alone (the unit of the CPU baseline):
+    returns the exciting field on the inside cells (N, 9)."""
+    grid_idx, centres, a_sub = sphere_grid(radius, n_sub)
+    n = n_sub
+    mask = np.zeros((n, n, n), dtype=bool)
+    mask[tuple(grid_idx.T)] = True
+    t4 = t0_scalars(omega, a_sub, alpha, beta, rho, dlam * mask, dmu * mask, drho * mask)
+    kh = build_slab_kernels(n, n, a_sub, omega, alpha, beta, rho)
+    U = sphere_incident(centres, omega, alpha, beta, k_hat, wave_type)
+    A = LinearOperator((9 * n ** 3,) * 2, matvec=lambda v: slab_matvec(v, t4, kh, n, n), dtype=complex)
+    b = np.zeros((n, n, n, 9), dtype=complex)
+    b[tuple(grid_idx.T)] = U[:, col].reshape(len(centres), 9)
+    x, _ = gmres(A, b.ravel(), x0=b.ravel().copy(), rtol=gmres_tol, maxiter=500, restart=30)
+    return x.reshape(n, n, n, 9)[tuple(grid_idx.T)]
+
+
 def sphere_foldy_lax(omega, radius, alpha, beta, rho, dlam, dmu, drho, n_sub, k_hat=None, wave_type="S",
                      gmres_tol=1e-12):
     """T_comp (9, 9) and psi_exc (9N, 9) of the sphere: the slab operator on the
