@@ -16,6 +16,7 @@ from __future__ import annotations
 
 import ctypes as C
 import warnings
+from pathlib import Path
 from dataclasses import dataclass, field
 from typing import Callable
 
@@ -458,6 +459,19 @@ _PLAN_CACHE: dict = {}
 _PLAN_CACHE_SIZE = 2
 
 
+_NETWORK = None
+
+
+def _packaged_network():
+    """The packaged learned near-field preconditioner (data/nearfield_grf.npz), loaded once."""
+    global _NETWORK
+    if _NETWORK is None:
+        from .learned import NearFieldPreconditioner
+
+        _NETWORK = NearFieldPreconditioner.load(Path(__file__).resolve().parent / "data" / "nearfield_grf.npz")
+    return _NETWORK
+
+
 def _cached_plan(geometry: SlabGeometry, ref: ReferenceMedium, periodic: bool, device) -> SlabPlan:
     """Plans are reused across calls with the same geometry, medium, periodicity
     and device (allocations and FFT set-up happen once); the two most recent
@@ -523,19 +537,23 @@ def compute_slab_scattering_gpu(
     (complex64 or complex128); the arithmetic is set by ``precision`` and the
     returned field is always complex128 with its FP64 true residual.
     ``preconditioner``: None (plain GMRES), "nearfield" (flexible GMRES with the
-    near-field Neumann polynomial of the plan's settings), or a
-    ``NearFieldPreconditioner`` (its degree, coefficients and learned block
-    corrections); plain GMRES finishes the solve if a preconditioned cycle stalls.
+    near-field Neumann polynomial of the plan's settings), "learned" (the packaged
+    network, trained on the GPU on Gaussian-random-field slabs:
+    ``data/make_nearfield_weights.py``), or a ``NearFieldPreconditioner`` (its degree,
+    coefficients and learned block corrections); plain GMRES finishes the solve if a
+    preconditioned cycle stalls.
     """
     if wave_type not in ("P", "S"):
         raise ValueError(f"wave_type must be 'P' or 'S', got '{wave_type}'")
     if dtype is not None and dtype not in (torch.complex64, torch.complex128):
         raise ValueError(f"dtype must be torch.complex64 or torch.complex128, got {dtype}")
     pc_mode = None
+    if isinstance(preconditioner, str) and preconditioner == "learned":
+        preconditioner = _packaged_network()
     if preconditioner is not None:
         if isinstance(preconditioner, str):
             if preconditioner not in ("nearfield", "none"):
-                raise ValueError(f"preconditioner must be None, 'nearfield' or a NearFieldPreconditioner, "
+                raise ValueError(f"preconditioner must be None, 'nearfield', 'learned' or a NearFieldPreconditioner, "
                                  f"got {preconditioner!r}")
             pc_mode = None if preconditioner == "none" else "nearfield"
         elif hasattr(preconditioner, "install"):

@@ -164,3 +164,20 @@ def test_learned_preconditioner_ablation(capsys):
     else:
         assert np.array_equal(net.coef, np.ones(net.degree + 1)) and not net.w.any()
     assert sum(learned) < sum(plain)
+
+
+def test_packaged_network_as_drop_in_option():
+    """preconditioner="learned" loads the packaged network (trained on the GPU on GRF
+    slabs, data/make_nearfield_weights.py) and solves a hard held-out slab to the same
+    field as plain GMRES in fewer operator applications."""
+    from multiplescatteringcalculations_b200 import compute_slab_scattering_gpu
+
+    p = _grf(124)
+    plain = compute_slab_scattering_gpu(p.geometry, p.material, p.omega, p.k_hat, p.wave_type, gmres_tol=1e-8,
+                                        max_iter=3000)
+    lrn = compute_slab_scattering_gpu(p.geometry, p.material, p.omega, p.k_hat, p.wave_type, gmres_tol=1e-8,
+                                      max_iter=3000, preconditioner="learned")
+    assert plain.gmres_residual < 1e-8 and lrn.gmres_residual < 1e-8
+    assert lrn.stats["n_precond"] > 0 and not lrn.stats["pc_fallback"]
+    assert lrn.n_gmres_iter < plain.n_gmres_iter
+    assert _rel(lrn.psi, plain.psi) < 1e-6
