@@ -4,9 +4,11 @@ Mirrors ``cubic_scattering/solver_config.py`` (tmnestor/MultipleScatteringCalcul
 ``:35-475``): the same dataclasses, YAML keys (``configs/example_slab.yml``) and
 validation messages, dispatching slab problems to the B200 solver. Added keys:
 ``solver.restart``, ``solver.precision`` ("mixed" | "fp64"), ``solver.ortho``,
-``solver.inner_tol``, ``problem.incident.bloch``, ``problem.geometry.periodic``,
-and the slab material types ``grf`` (``correlation_length``, ``std``, ``seed``) and
-``iid`` (``fraction``, ``seed``). Sphere problems are not part of this package.
+``solver.inner_tol``, ``solver.preconditioner`` (none | nearfield | learned),
+``problem.incident.bloch``, ``problem.geometry.periodic``, and the slab material types
+``grf`` (``correlation_length``, ``std``, ``seed``) and ``iid`` (``fraction``, ``seed``).
+Sphere problems (``problem.sphere``: ``radius``, ``n_sub``) go to the sphere FFT
+Foldy-Lax solver on the GPU, as the reference's GPU branch does (solver_config.py:440-458).
 """
 
 from __future__ import annotations
@@ -70,6 +72,7 @@ class SolverConfig:
     precision: str = "mixed"
     ortho: str = "auto"
     inner_tol: float = 0.0
+    preconditioner: str = "none"
 
 
 @dataclass
@@ -128,6 +131,7 @@ def load_config(path) -> ScatteringConfig:
         precision=sol.get("precision", "mixed"),
         ortho=sol.get("ortho", "auto"),
         inner_tol=float(sol.get("inner_tol", 0.0)),
+        preconditioner=str(sol.get("preconditioner", "none")),
     )
     prob = raw.get("problem")
     if prob is None:
@@ -187,6 +191,9 @@ def validate_config(config: ScatteringConfig) -> None:
     valid_dtypes = ("auto", "complex64", "complex128")
     if config.device.dtype not in valid_dtypes:
         raise ValueError(f"Invalid dtype '{config.device.dtype}'. Valid options: {', '.join(valid_dtypes)}.")
+    if config.solver.preconditioner not in ("none", "nearfield", "learned"):
+        raise ValueError(f"Invalid preconditioner '{config.solver.preconditioner}'. "
+                         f"Must be 'none', 'nearfield' or 'learned'.")
     if p.type == "sphere":
         sp = p.sphere
         if sp is None:
@@ -220,18 +227,26 @@ def build_material(config: ScatteringConfig):
     return uniform_slab_material(geometry, ref, p.to_material_contrast())
 
 
-def run_from_config(config: ScatteringConfig) -> SlabResult:
-    """Solve the configured slab on the GPU (solver_config.py:375-438).
+def run_from_config(config: ScatteringConfig):
+    """Solve the configured problem on the GPU (solver_config.py:375-475): a slab
+    (SlabResult) or a sphere (SphereDecompositionResult).
 
     The reference sends CPU configs to its numpy path; this package has no CPU
-    path and raises for them. Sphere problems are outside this package.
+    path and raises for them.
     """
-    if config.problem.type != "slab":
-        raise ValueError("this package solves slab problems; sphere problems stay with the reference")
     device = config.device.resolve_device()
     dtype = config.device.resolve_dtype(device)
     p = config.problem
     s = config.solver
+    if p.type == "sphere":
+        from .sphere import compute_sphere_foldy_lax_fft_gpu
+
+        sp = p.sphere or {}
+        return compute_sphere_foldy_lax_fft_gpu(
+            float(p.frequency["omega"]), float(sp["radius"]), p.to_reference_medium(), p.to_material_contrast(),
+            int(sp["n_sub"]), k_hat=np.array(p.incident["k_hat"], dtype=float), wave_type=p.incident["wave_type"],
+            gmres_tol=s.gmres_tol, gmres_maxiter=s.max_iter, initial_guess=s.initial_guess, device=device,
+            dtype=dtype, precision=s.precision, restart=s.restart)
     geometry = p.to_slab_geometry()
     material = build_material(config)
     return compute_slab_scattering_gpu(
@@ -239,4 +254,5 @@ def run_from_config(config: ScatteringConfig) -> SlabResult:
         p.incident["wave_type"], gmres_tol=s.gmres_tol, max_iter=s.max_iter, initial_guess=s.initial_guess,
         device=device, dtype=dtype, periodic=bool(p.geometry.get("periodic", False)), restart=s.restart,
         precision=s.precision, bloch=bool(p.incident.get("bloch", False)), ortho=s.ortho, inner_tol=s.inner_tol,
+        preconditioner=None if s.preconditioner == "none" else s.preconditioner,
     )

@@ -47,6 +47,8 @@ def test_load_config_reference_schema():
     (lambda d: d["solver"].update(precision="half"), "Invalid precision"),
     (lambda d: d["device"].update(backend="tpu"), "Invalid backend"),
     (lambda d: d["problem"]["slab"].update(material_type="grf"), "correlation_length"),
+    (lambda d: d["solver"].update(preconditioner="magic"), "Invalid preconditioner"),
+    (lambda d: d["problem"].update(type="sphere"), "requires a 'sphere' section"),
 ])
 def test_validation_messages(tmp_path, patch, match):
     d = yaml.safe_load((HERE / "configs" / "slab_small.yml").read_text())
