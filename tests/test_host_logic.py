@@ -120,3 +120,19 @@ def test_dataclass_validation():
         SlabMaterial(np.zeros((2, 2)), np.zeros((2, 2)), np.zeros((2, 2)), REF)
     mat = uniform_slab_material(SlabGeometry(2, 3, 1.0), REF, MaterialContrast(1.0, 2.0, 3.0))
     assert mat.Dmu.shape == (3, 2, 2) and np.all(mat.Dmu == 2.0)
+
+
+def test_result_arrays_are_recycled_only_when_unreferenced():
+    from multiplescatteringcalculations_b200 import slab as S
+
+    a = S._host_array((3, 7))
+    ida = id(a)
+    b = S._host_array((3, 7))
+    assert a is not b
+    del a
+    c = S._host_array((3, 7))
+    assert id(c) == ida  # dropped by the caller: filled again
+    v = c[1:]
+    del c
+    d = S._host_array((3, 7))
+    assert d is not v.base  # a view keeps it alive
