@@ -142,6 +142,31 @@ def test_matvec_compiled_lengths_vs_oracle(M, Nz, per, va):
     assert _rel(got32, want) < 1e-5
 
 
+@pytest.mark.parametrize("M,Nz,Lxy,va", [
+    (32, 5, 64, 0),    # M = L/2
+    (30, 4, 64, 0),    # M < L/2, not a multiple of 4 (warps holding rows inside and outside the lattice)
+    (64, 3, 128, 0),   # the cfg2 shape
+    (45, 6, 128, 1),   # odd M, volume averaged
+])
+def test_matvec_fused_plane_passes_vs_oracle(M, Nz, Lxy, va):
+    """The complex64 matvec's fused plane kernels (aperiodic, Lx = Ly in {64, 128}):
+    T0 + y + x per plane and x' + y' + output per plane."""
+    rng = np.random.default_rng(M * 100 + Nz)
+    g = SlabGeometry(M, Nz, 1.0)
+    mat = random_slab_material(g, REF, CONTRAST, 0.5, seed=M + 3 * Nz)
+    t4 = O.t0_scalars(OMEGA, 1.0, REF.alpha, REF.beta, REF.rho, mat.Dlambda, mat.Dmu, mat.Drho)
+    kh = O.build_slab_kernels(M, Nz, 1.0, OMEGA, REF.alpha, REF.beta, REF.rho, volume_averaged=bool(va))
+    x = rng.standard_normal(Nz * M * M * 9) + 1j * rng.standard_normal(Nz * M * M * 9)
+    want = O.slab_matvec(x, t4, kh, M, Nz)
+    plan = SlabPlan(g, REF, Lxy=Lxy)
+    assert plan.fft_sizes()[1:] == (Lxy, Lxy)
+    plan.build_t0(mat, OMEGA)
+    plan.build_g0(OMEGA, volume_averaged=bool(va))
+    xt = torch.from_numpy(x.reshape(Nz, M, M, 9))
+    assert _rel(plan.matvec(xt, "complex64").cpu().numpy().ravel(), want) < 1e-5
+    assert _rel(plan.matvec(xt, "complex128").cpu().numpy().ravel(), want) < 1e-12
+
+
 def test_bloch_matvec_compiled_lengths_vs_oracle():
     """Full (non-octant) spectrum with Lxy 16 periodic and Lz 16."""
     M, Nz = 16, 8
