@@ -465,22 +465,34 @@ _PLAN_CACHE_SIZE = 2
 # list (the caller dropped the result and holds no view of it) is unobserved and is
 # filled again instead of a fresh one: new host memory costs its first-touch page
 # faults on every call (several milliseconds for the 23 MB of a 64 x 64 x 16 result).
-_HOST_POOL: list = []
+#
+# The first _PINNED_MAX arrays of the pool are page-locked (views of pinned torch
+# tensors), so a recycled result is filled by an asynchronous DMA copy; later ones are
+# pageable, so callers that keep every result never pay more than those few
+# page-locked allocations (each a cudaHostAlloc of ~16 ms for 23 MB).
+_HOST_POOL: list = []   # entries [ndarray, pinned tensor or None]
 _HOST_POOL_SIZE = 8
+_PINNED_MAX = 6
 _HOST_POOL_LOCK = threading.Lock()
 
 
-def _host_array(shape: tuple) -> np.ndarray:
+def _host_array(shape: tuple):
+    """(array, pinned tensor or None) for a complex128 result of ``shape``."""
     with _HOST_POOL_LOCK:  # the returned value holds a reference before the lock is released
-        for a in _HOST_POOL:
-            # references: the list, the loop variable and getrefcount's argument
-            if a.shape == shape and sys.getrefcount(a) <= 3:
-                return a
-        a = np.empty(shape, dtype=np.complex128)
-        _HOST_POOL.append(a)
+        for e in _HOST_POOL:
+            # references to the array: the entry, getrefcount's argument
+            if e[0].shape == shape and sys.getrefcount(e[0]) <= 2:
+                return e[0], e[1]
+        pinned = sum(1 for e in _HOST_POOL if e[1] is not None)
+        if pinned < _PINNED_MAX and torch.cuda.is_available():
+            t = torch.empty(shape, dtype=torch.complex128, pin_memory=True)
+            e = [t.numpy(), t]
+        else:
+            e = [np.empty(shape, dtype=np.complex128), None]
+        _HOST_POOL.append(e)
         if len(_HOST_POOL) > _HOST_POOL_SIZE:
             _HOST_POOL.pop(0)
-        return a
+        return e[0], e[1]
 
 
 _NETWORK = None
@@ -613,9 +625,13 @@ def compute_slab_scattering_gpu(
     # torch.empty). Pinned buffers copy faster but results kept alive by the caller
     # would each hold one, and every new block is a cudaHostAlloc of ~16 ms.
     host = [_host_array(tuple(t.shape)) for t in (x, psi0, t4)]
-    for h, t in zip(host, (x, psi0, t4)):
-        torch.from_numpy(h).copy_(t)
-    psi_h, psi0_h, t4_h = host
+    for (h, ht), t in zip(host, (x, psi0, t4)):
+        if ht is not None:
+            ht.copy_(t, non_blocking=True)
+        else:
+            torch.from_numpy(h).copy_(t)
+    torch.cuda.current_stream(plan.device).synchronize()
+    psi_h, psi0_h, t4_h = (h for h, _ in host)
     res = SlabResult(
         psi=psi_h,
         psi0=psi0_h,

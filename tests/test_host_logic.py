@@ -125,14 +125,14 @@ def test_dataclass_validation():
 def test_result_arrays_are_recycled_only_when_unreferenced():
     from multiplescatteringcalculations_b200 import slab as S
 
-    a = S._host_array((3, 7))
+    a = S._host_array((3, 7))[0]
     ida = id(a)
-    b = S._host_array((3, 7))
+    b = S._host_array((3, 7))[0]
     assert a is not b
     del a
-    c = S._host_array((3, 7))
+    c = S._host_array((3, 7))[0]
     assert id(c) == ida  # dropped by the caller: filled again
     v = c[1:]
     del c
-    d = S._host_array((3, 7))
+    d = S._host_array((3, 7))[0]
     assert d is not v.base  # a view keeps it alive
