@@ -38,6 +38,7 @@
 // path (FP64 weights) serves the gradient check against the oracle.
 #include <cuda_bf16.h>
 
+#include <algorithm>
 #include <cmath>
 #include <vector>
 
@@ -129,35 +130,100 @@ __device__ double2 block_sum(double2 v) {
   return r;
 }
 
-// gG[o][a][b] += scale sum_v delta_a(v) conj(tau_b(v - o)); one block per entry
+// Weight gradient, tiled: a block stages delta on its tile of 2 x 8 x 16 sites and tau on
+// the tile with a one-voxel halo (zero outside the slab) in shared memory, and each thread
+// accumulates sum_v delta_a(v) conj(tau_b(v - o)) over the tile for its entries (o, a, b)
+// of the mirror-symmetry pattern; part[block][entry] holds the block's sums, which
+// k_tr_wgrad_reduce adds over the blocks in a fixed order. Row pitches 257 and 721 put
+// the rows of different components in different banks.
+constexpr int WG_TZ = 2, WG_TX = 8, WG_TY = 16, WG_NT = WG_TZ * WG_TX * WG_TY;
+constexpr int WG_HZ = WG_TZ + 2, WG_HX = WG_TX + 2, WG_HY = WG_TY + 2, WG_HALO = WG_HZ * WG_HX * WG_HY;
+constexpr int WG_DP = WG_NT + 1, WG_TP = WG_HALO + 1;
+
 template <typename T>
-__global__ void k_tr_wgrad(const cx<T>* __restrict__ delta, const cx<T>* __restrict__ tau, double2* gG, Geo g,
-                           double scale) {
-  const int e = blockIdx.x;
-  const int o = e / 81, a = (e / 9) % 9, b = e % 9;
-  if (!nf_allowed(o, a, b)) return;  // uniform over the block
-  const int dz = o / 9 - 1, dx = (o / 3) % 3 - 1, dy = o % 3 - 1;
-  cx<T> sum = czero<cx<T>>();
-  for (int s = threadIdx.x; s < g.nsite; s += blockDim.x) {
-    const int j = s % g.M, i = (s / g.M) % g.M, n = s / (g.M * g.M);
-    const int zn = n - dz, xi = i - dx, yj = j - dy;
-    if (zn < 0 || zn >= g.Nz || xi < 0 || xi >= g.M || yj < 0 || yj >= g.M) continue;
-    const cx<T> dv = delta[(size_t)a * g.nsite + s];
-    const cx<T> tv = tau[(size_t)b * g.nsite + (zn * g.M + xi) * g.M + yj];
-    sum += mul_conj(dv, tv);
+__global__ void __launch_bounds__(WG_NT) k_tr_wgrad_tile(const cx<T>* __restrict__ delta, const cx<T>* __restrict__ tau,
+                                                         double2* __restrict__ part, Geo g) {
+  using C = cx<T>;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* dl = reinterpret_cast<C*>(smem_raw);  // [9][WG_DP]
+  C* tu = dl + 9 * WG_DP;                   // [9][WG_TP]
+  const int nby = (g.M + WG_TY - 1) / WG_TY, nbx = (g.M + WG_TX - 1) / WG_TX;
+  const int by = blockIdx.x % nby, bx = (blockIdx.x / nby) % nbx, bz = blockIdx.x / (nby * nbx);
+  const int y0 = by * WG_TY, x0 = bx * WG_TX, z0 = bz * WG_TZ;
+  const int tid = threadIdx.x;
+  {
+    const int vy = tid % WG_TY, vx = (tid / WG_TY) % WG_TX, vz = tid / (WG_TY * WG_TX);
+    const int z = z0 + vz, x = x0 + vx, y = y0 + vy;
+    const bool in = z < g.Nz && x < g.M && y < g.M;
+    const int site = (z * g.M + x) * g.M + y;
+#pragma unroll
+    for (int c = 0; c < 9; ++c) dl[c * WG_DP + tid] = in ? delta[(size_t)c * g.nsite + site] : czero<C>();
   }
-  const double2 r = block_sum(to_d(sum));
-  if (threadIdx.x == 0) gG[e] = gG[e] + scale * r;
+  for (int i = tid; i < WG_HALO; i += WG_NT) {
+    const int hy = i % WG_HY, hx = (i / WG_HY) % WG_HX, hz = i / (WG_HY * WG_HX);
+    const int z = z0 + hz - 1, x = x0 + hx - 1, y = y0 + hy - 1;
+    const bool in = z >= 0 && z < g.Nz && x >= 0 && x < g.M && y >= 0 && y < g.M;
+    const int site = (z * g.M + x) * g.M + y;
+#pragma unroll
+    for (int c = 0; c < 9; ++c) tu[c * WG_TP + i] = in ? tau[(size_t)c * g.nsite + site] : czero<C>();
+  }
+  __syncthreads();
+  double2* pb = part + (size_t)blockIdx.x * NF_OFFS * 81;
+  for (int e = tid; e < NF_OFFS * 81; e += WG_NT) {
+    const int o = e / 81, a = (e / 9) % 9, b = e % 9;
+    C sum = czero<C>();
+    if (nf_allowed(o, a, b)) {
+      const int dz = o / 9 - 1, dx = (o / 3) % 3 - 1, dy = o % 3 - 1;
+      const C* da = dl + a * WG_DP;
+      const C* tb = tu + b * WG_TP;
+      for (int vz = 0; vz < WG_TZ; ++vz)
+        for (int vx = 0; vx < WG_TX; ++vx) {
+          const int v0 = (vz * WG_TX + vx) * WG_TY;
+          const int h0 = ((vz + 1 - dz) * WG_HX + (vx + 1 - dx)) * WG_HY + 1 - dy;
+#pragma unroll
+          for (int vy = 0; vy < WG_TY; ++vy) sum += mul_conj(da[v0 + vy], tb[h0 + vy]);
+        }
+    }
+    pb[e] = to_d(sum);
+  }
 }
 
-// out[k] = sum conj(a_k) b over n elements for the vectors a_k = A + k n (one block each)
+// gG[e] += scale sum over blocks of part[block][e] (fixed order)
+__global__ void k_tr_wgrad_reduce(const double2* __restrict__ part, int nblocks, double2* gG, double scale) {
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= NF_OFFS * 81) return;
+  double2 s = make_double2(0, 0);
+  for (int b = 0; b < nblocks; ++b) s = s + part[(size_t)b * NF_OFFS * 81 + e];
+  gG[e] = gG[e] + scale * s;
+}
+
+inline int wgrad_blocks(const Geo& g) {
+  return ((g.M + WG_TY - 1) / WG_TY) * ((g.M + WG_TX - 1) / WG_TX) * ((g.Nz + WG_TZ - 1) / WG_TZ);
+}
+
+// out[k] += sum conj(a_k) b over n elements for the vectors a_k = A + k n: blockIdx.y = k,
+// the blocks along x split the elements; each adds its FP64 block sum atomically (out
+// zeroed by the caller)
 template <typename T>
 __global__ void k_tr_dots(const cx<T>* __restrict__ A, size_t n, const cx<T>* __restrict__ b, double2* out) {
-  const cx<T>* a = A + (size_t)blockIdx.x * n;
+  const cx<T>* a = A + (size_t)blockIdx.y * n;
   double2 sum = make_double2(0, 0);
-  for (size_t k = threadIdx.x; k < n; k += blockDim.x) sum = sum + to_d(conj_mul(a[k], b[k]));
+  for (size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x)
+    sum = sum + to_d(conj_mul(a[k], b[k]));
   const double2 r = block_sum(sum);
-  if (threadIdx.x == 0) out[blockIdx.x] = r;
+  if (threadIdx.x == 0) {
+    atomicAdd(&out[blockIdx.y].x, r.x);
+    atomicAdd(&out[blockIdx.y].y, r.y);
+  }
+}
+
+// out[k] = sum conj(a_k) b, k < nv
+template <typename T>
+int tr_dots(cudaStream_t st, const cx<T>* A, size_t n, const cx<T>* b, double2* out, int nv) {
+  MSC_CUDA(cudaMemsetAsync(out, 0, sizeof(double2) * nv, st));
+  const unsigned nbx = (unsigned)std::min<size_t>(592, (n + 255) / 256);
+  k_tr_dots<T><<<dim3(nbx, (unsigned)nv), 256, 0, st>>>(A, n, b, out);
+  return MSC_OK;
 }
 
 // z = sum_l c_l H_l (nv vectors)
@@ -321,11 +387,12 @@ struct Trainer {
   template <typename T>
   int loss_grad(const cx<T>* r, const double2* coef_dev, const std::vector<double2>& coef,
                 const typename WType<T>::type* Gl, const cx<T>* t4id, double* loss, double2* gw, double2* gc_dev,
-                cx<T>* H, cx<T>* tau, cx<T>* z, cx<T>* q, cx<T>* u, cx<T>* y, cx<T>* d, cx<T>* del, double2* red) {
+                cx<T>* H, cx<T>* tau, cx<T>* z, cx<T>* q, cx<T>* u, cx<T>* y, cx<T>* d, cx<T>* del, double2* red,
+                double2* part) {
     const Geo& g = pl->g;
     cudaStream_t st = pl->stream;
     const cx<T>* t4 = (const cx<T>*)(sizeof(T) == 8 ? pl->t4_64.p : pl->t4_32.p);
-    k_tr_dots<T><<<1, 256, 0, st>>>(r, n, r, red);
+    MSC_TRY(tr_dots<T>(st, r, n, r, red, 1));
     double2 rn2;
     MSC_CUDA(cudaMemcpyAsync(&rn2, red, sizeof(rn2), cudaMemcpyDeviceToHost, st));
     MSC_CUDA(cudaStreamSynchronize(st));
@@ -343,8 +410,8 @@ struct Trainer {
     k_tr_combine<T><<<nblk(n), 256, 0, st>>>(H, L + 1, coef_dev, n, z);
     MSC_TRY(launch_matvec<T>(pl, z, nullptr, q, nullptr));  // y = A z (in q)
     // the optimal scale alpha = <y, r^> / <y, y>
-    k_tr_dots<T><<<1, 256, 0, st>>>(q, n, H, red + 2);
-    k_tr_dots<T><<<1, 256, 0, st>>>(q, n, q, red + 3);
+    MSC_TRY(tr_dots<T>(st, q, n, H, red + 2, 1));
+    MSC_TRY(tr_dots<T>(st, q, n, q, red + 3, 1));
     double2 ab[2];
     MSC_CUDA(cudaMemcpyAsync(ab, red + 2, sizeof(ab), cudaMemcpyDeviceToHost, st));
     MSC_CUDA(cudaStreamSynchronize(st));
@@ -354,19 +421,26 @@ struct Trainer {
     }
     const double2 alpha = make_double2(ab[0].x / ab[1].x, ab[0].y / ab[1].x);
     k_tr_axpby<T><<<nblk(n), 256, 0, st>>>(H, make_double2(-1, 0), alpha, q, n);  // q = alpha y - r^
-    k_tr_dots<T><<<1, 256, 0, st>>>(q, n, q, red + 1);
+    MSC_TRY(tr_dots<T>(st, q, n, q, red + 1, 1));
     k_tr_axpby<T><<<nblk(n), 256, 0, st>>>(q, conj_(alpha), make_double2(0, 0), q, n);  // q *= conj(alpha)
     // d = A^H q
     k_tr_adj_pre<T><<<nblk(n), 256, 0, st>>>(q, u, g.nsite);
     MSC_TRY(matvec_identity<T>(u, y, t4id));
     k_tr_adj_post<T><<<nblk(g.nsite), 256, 0, st>>>(q, u, y, t4, d, g.nsite, s);
     // coefficient gradients
-    k_tr_dots<T><<<L + 1, 256, 0, st>>>(H, n, d, gc_dev);
+    MSC_TRY(tr_dots<T>(st, H, n, d, gc_dev, L + 1));
     // backward through the layers
     MSC_CUDA(cudaMemsetAsync(del, 0, sizeof(cx<T>) * n, st));
     k_tr_axpby<T><<<nblk(n), 256, 0, st>>>(d, conj_(coef[L]), make_double2(0, 0), del, n);
     for (int l = L; l >= 1; --l) {
-      k_tr_wgrad<T><<<NF_OFFS * 81, 256, 0, st>>>(del, tau + (l - 1) * n, gw + (size_t)(l - 1) * NF_OFFS * 81, g, s);
+      {
+        const int nbw = wgrad_blocks(g);
+        const size_t smw = sizeof(cx<T>) * 9 * (size_t)(WG_DP + WG_TP);
+        MSC_CUDA(prep_kernel((const void*)k_tr_wgrad_tile<T>));
+        k_tr_wgrad_tile<T><<<nbw, WG_NT, smw, st>>>(del, tau + (l - 1) * n, part, g);
+        k_tr_wgrad_reduce<<<(NF_OFFS * 81 + 255) / 256, 256, 0, st>>>(part, nbw,
+                                                                      gw + (size_t)(l - 1) * NF_OFFS * 81, s);
+      }
       if (l > 1) {
         k_tr_stencil<T><<<nblk(g.nsite, 128), 128, 0, st>>>(del, Gl + (size_t)(l - 1) * NF_OFFS * 81, u, g, 1);
         k_tr_tapply<T><<<nblk(g.nsite), 256, 0, st>>>(u, t4, del, g.nsite, 1);
@@ -403,7 +477,7 @@ int check_plan(msc_plan* pl, int degree) {
 template <typename T>
 struct Fields {
   cx<T> *r, *H, *tau, *z, *q, *u, *y, *d, *del, *t4id;
-  double2 *gw, *gc, *cd, *red;
+  double2 *gw, *gc, *cd, *red, *part;
   typename WType<T>::type* Gl;
   int alloc(Trainer& tr) {
     const size_t n = tr.n;
@@ -422,6 +496,7 @@ struct Fields {
     MSC_TRY(tr.get(&gc, L + 1));
     MSC_TRY(tr.get(&cd, L + 1));
     MSC_TRY(tr.get(&red, 4));
+    MSC_TRY(tr.get(&part, (size_t)wgrad_blocks(tr.pl->g) * NF_OFFS * 81));
     MSC_TRY(tr.get(&Gl, nb));
     k_tr_ident_t4<T><<<nblk(tr.pl->g.nsite), 256, 0, tr.pl->stream>>>(t4id, tr.pl->g.nsite, 1.0 / tr.s);
     ::msc::note_launch();
@@ -431,7 +506,7 @@ struct Fields {
   int run(Trainer& tr, const std::vector<double2>& c, double* loss) {
     MSC_CUDA(cudaMemcpyAsync(cd, c.data(), sizeof(double2) * c.size(), cudaMemcpyHostToDevice, tr.pl->stream));
     MSC_CUDA(cudaMemsetAsync(gw, 0, sizeof(double2) * (size_t)tr.L * NF_OFFS * 81, tr.pl->stream));
-    return tr.loss_grad<T>(r, cd, c, Gl, t4id, loss, gw, gc, H, tau, z, q, u, y, d, del, red);
+    return tr.loss_grad<T>(r, cd, c, Gl, t4id, loss, gw, gc, H, tau, z, q, u, y, d, del, red, part);
   }
 };
 
