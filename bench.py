@@ -575,6 +575,32 @@ def run_precond_eval(args, wl, rank, world, local_rank) -> int:
     return 0
 
 
+def run_train_steps(n: int) -> int:
+    """One 64 x 64 x 16 GRF slab of the learned-preconditioner workload (seed 3000), its
+    solver residuals after 2, 5, 10, 20, 40 FP64 GMRES matvecs, 2 untimed and n timed Adam
+    steps of a degree-4 network through msc_nf_train. Prints the time per step."""
+    import torch
+
+    from multiplescatteringcalculations_b200 import NearFieldPreconditioner, SlabPlan
+    from multiplescatteringcalculations_b200.data.make_nearfield_weights import grf_problem
+    from multiplescatteringcalculations_b200.learned import solver_residuals
+
+    p = grf_problem(3000)
+    plan = SlabPlan(p.geometry, p.material.ref)
+    plan.build_t0(p.material, p.omega)
+    plan.build_g0(p.omega)
+    res = solver_residuals(plan, plan.incident(p.omega, p.k_hat, p.wave_type), (2, 5, 10, 20, 40))
+    net = NearFieldPreconditioner(4)
+    plan.nf_train(res, net.coef, net.w, None, 2, 1e-4)
+    torch.cuda.synchronize()
+    t = time.perf_counter()
+    plan.nf_train(res, net.coef, net.w, None, n, 1e-4)
+    torch.cuda.synchronize()
+    print(json.dumps({"adam_steps": n, "ms_per_step": (time.perf_counter() - t) / n * 1e3,
+                      "lattice": "64x64x16", "degree": 4}))
+    return 0
+
+
 def run_matvecs(wl: dict, n: int) -> int:
     """Plan + T0 + G0 of the workload, then 3 untimed and n timed complex64 operator
     applications through msc_matvec (each: 2 layout transposes and the matvec
@@ -681,6 +707,8 @@ def main(argv=None) -> int:
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--solve-only", action="store_true", help="timed solves only (for profiler launch lists)")
+    ap.add_argument("--train-only", type=int, default=0, metavar="N",
+                    help="N Adam steps of the learned preconditioner on one 64x64x16 GRF slab (for kernel profiles)")
     ap.add_argument("--matvec-only", type=int, default=0, metavar="N",
                     help="build the plan and run N complex64 matvecs through msc_matvec (for kernel profiles)")
     args = ap.parse_args(argv)
@@ -692,6 +720,8 @@ def main(argv=None) -> int:
         return run_reference(args, wl, rank, world)
     if args.matvec_only:
         return run_matvecs(wl, args.matvec_only)
+    if args.train_only:
+        return run_train_steps(args.train_only)
     if "precond_eval" in wl:
         return run_precond_eval(args, wl, rank, world, local_rank)
     if "sphere" in wl:
