@@ -145,6 +145,24 @@ def cpu_baseline(wl: dict, threads: int, seed: int = 0):
     return dt, r, tm
 
 
+def max_over_ranks(value: float, world: int, device) -> float:
+    """The maximum of a per-rank value over the job (the job takes as long as its slowest
+    rank); one all-reduce when world > 1, the value itself otherwise."""
+    if world <= 1:
+        return float(value)
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([float(value)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def rank_seed(base: int, rank: int) -> int:
+    """Seed of a rank's workload: replicas solve disjoint inputs (weak scaling)."""
+    return base + rank
+
+
 def run_reference(args, wl, rank, world):
     if rank != 0:
         return 0
@@ -189,7 +207,7 @@ def run_ours(args, wl, rank, world, local_rank):
     torch.cuda.set_device(local_rank)
     dev = torch.device("cuda", local_rank)
     lib = _native.load()
-    ref, geom, mat, k_hat, omega = make_problem(wl, seed=1000 + rank)
+    ref, geom, mat, k_hat, omega = make_problem(wl, seed=rank_seed(1000, rank))
     plan = SlabPlan(geom, ref, periodic=wl["periodic"], device=dev)
     mat_dev = type(mat)(torch.from_numpy(mat.Dlambda).to(dev), torch.from_numpy(mat.Dmu).to(dev),
                         torch.from_numpy(mat.Drho).to(dev), ref)
@@ -226,11 +244,7 @@ def run_ours(args, wl, rank, world, local_rank):
     if world > 1:
         dist.barrier()
     torch.cuda.synchronize()
-    ms = ev0.elapsed_time(ev1)
-    t = torch.tensor([ms], dtype=torch.float64, device=dev)
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    ms_max = float(t.item())
+    ms_max = max_over_ranks(ev0.elapsed_time(ev1), world, dev)
     value = world * args.steps / (ms_max / 1e3)
     if stats.get("residual", 1.0) > wl["tol"]:
         raise RuntimeError(f"solve did not reach tol: {stats}")
@@ -406,7 +420,7 @@ def run_batch(args, wl, rank, world, local_rank) -> int:
     torch.cuda.set_device(local_rank)
     dev = torch.device("cuda", local_rank)
     lib = _native.load()
-    probs = batch_problems(wl, seed=1000 + rank)
+    probs = batch_problems(wl, seed=rank_seed(1000, rank))
     kw = dict(gmres_tol=wl["tol"], max_iter=2000, precision="mixed",
               preconditioner=None if args.precond == "none" else args.precond)
     warm = batch_problems(dict(wl, batch=16), seed=7)
@@ -423,10 +437,7 @@ def run_batch(args, wl, rank, world, local_rank) -> int:
         torch.cuda.synchronize()
         dt = time.perf_counter() - t0
     launches = lib.msc_launch_count() - n0
-    t = torch.tensor([dt], dtype=torch.float64, device=dev)
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    dt = float(t.item())
+    dt = max_over_ranks(dt, world, dev)
     value = world * args.steps * len(probs) / dt
     bad = [i for i, s in enumerate(sols) if s.status != 0]
     if bad:
