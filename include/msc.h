@@ -146,10 +146,11 @@ int msc_nearfield_blocks(const msc_plan* plan, double* out);
 /* z = P x, fields (N_z, M, M, 9) on the device in the precision given. */
 int msc_precondition(msc_plan* plan, const void* x, void* z, int precision);
 /* Storage of the layer blocks G_nn + dG_l for the complex64 preconditioner:
- * MSC_NF_WEIGHTS_FP32 (default) or MSC_NF_WEIGHTS_BF16 (rounded to bfloat16, FP32
- * accumulation; the form the learned network is trained in). The complex128 path
- * always uses FP64 blocks. */
-enum msc_nf_weights { MSC_NF_WEIGHTS_FP32 = 0, MSC_NF_WEIGHTS_BF16 = 1 };
+ * MSC_NF_WEIGHTS_FP32 (default), MSC_NF_WEIGHTS_BF16 (rounded to bfloat16, FP32
+ * accumulation; the form the learned network is trained in) or MSC_NF_WEIGHTS_BF16_TC
+ * (BF16 blocks and BF16 activations on the tensor cores, FP32 accumulation in tensor
+ * memory). The complex128 path always uses FP64 blocks. */
+enum msc_nf_weights { MSC_NF_WEIGHTS_FP32 = 0, MSC_NF_WEIGHTS_BF16 = 1, MSC_NF_WEIGHTS_BF16_TC = 2 };
 int msc_set_nearfield_weights(msc_plan* plan, int format);
 
 /* Learned near-field preconditioner: training on the GPU. The network is the

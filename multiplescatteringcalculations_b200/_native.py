@@ -30,6 +30,7 @@ MSC_PC_NONE = 0
 MSC_PC_NEARFIELD = 1
 MSC_NF_WEIGHTS_FP32 = 0
 MSC_NF_WEIGHTS_BF16 = 1
+MSC_NF_WEIGHTS_BF16_TC = 2
 MSC_SOLVE_MIXED = 0
 MSC_SOLVE_FP64 = 1
 MSC_WAVE_P = 0

@@ -409,12 +409,12 @@ int msc_set_nearfield(msc_plan* pl, int degree, const double* coef, const double
 
 int msc_set_nearfield_weights(msc_plan* pl, int format) {
   if (!pl) { set_error("null plan"); return MSC_ERR_INVALID; }
-  if (format != MSC_NF_WEIGHTS_FP32 && format != MSC_NF_WEIGHTS_BF16) {
-    set_error("weight format must be 0 (FP32) or 1 (BF16), got %d", format);
+  if (format != MSC_NF_WEIGHTS_FP32 && format != MSC_NF_WEIGHTS_BF16 && format != MSC_NF_WEIGHTS_BF16_TC) {
+    set_error("weight format must be 0 (FP32), 1 (BF16) or 2 (BF16 on the tensor cores), got %d", format);
     return MSC_ERR_INVALID;
   }
   if (!pl->nf) pl->nf = new NearField();
-  pl->nf->wbf16 = format == MSC_NF_WEIGHTS_BF16;
+  pl->nf->wbf16 = format;
   ++pl->gen;  // the captured solver graphs bind the block pointer
   return MSC_OK;
 }

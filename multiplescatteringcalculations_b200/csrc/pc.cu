@@ -270,6 +270,15 @@ int nearfield_apply(msc_plan* pl, const cx<T>* v, const double* scale, cx<T>* z,
     const cx<T> ch = mk<T>((T)nf->coef[l].x, (T)nf->coef[l].y);
     const int init = l == 1 ? 1 : 0;
     if constexpr (sizeof(T) == 4) {
+      if (nf->wbf16 == MSC_NF_WEIGHTS_BF16_TC) {
+        // the layer on the tensor cores
+        MSC_TRY(launch_nf_tc(pl, (const float2*)in, sc, (const float2*)t4, (float2*)h, (float2*)z,
+                             make_float2((float)ch.x, (float)ch.y), make_float2((float)c0.x, (float)c0.y), init,
+                             (const __nv_bfloat162*)nf->g16_dev.p + (size_t)(l - 1) * NF_OFFS * 81, done));
+        in = h;
+        sc = nullptr;
+        continue;
+      }
       k_nf32<<<grid, TL::NT, sm, pl->stream>>>((const float2*)in, sc, (const float2*)t4, (float2*)h, (float2*)z,
                                              make_float2((float)ch.x, (float)ch.y),
                                              make_float2((float)c0.x, (float)c0.y), init,

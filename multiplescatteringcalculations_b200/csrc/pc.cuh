@@ -30,7 +30,7 @@ struct NearField {
   // The kernels read them through these pointers, so a captured solver graph stays valid
   // when the blocks change (a new frequency): only the buffers' contents are refreshed.
   DBuf g64_dev, g32_dev, g16_dev;
-  int wbf16 = 0;               // complex64 path: BF16 blocks (g16_dev) instead of FP32 (g32_dev)
+  int wbf16 = 0;               // complex64 path: msc_nf_weights (1, 2: BF16 blocks g16_dev; 2: tensor cores)
   std::vector<double2> h64;    // host staging of the refresh
   std::vector<float2> h32;
   std::vector<__nv_bfloat162> h16;
@@ -44,6 +44,10 @@ int nearfield_extract(msc_plan* pl, const double2* Ks_spatial, double scale);
 // Upload the per-layer blocks after a change (synchronises the plan's stream; must not
 // run while a graph is being captured).
 int nearfield_refresh(msc_plan* pl);
+// One complex64 stencil layer with BF16 weights on the tensor cores (pc_tc.cu); the
+// arguments as the CUDA-core layer kernel of pc.cu.
+int launch_nf_tc(msc_plan* pl, const float2* x, const double* scale, const float2* t4, float2* h, float2* acc,
+                 float2 ch, float2 c0, int init, const __nv_bfloat162* G16, const int* done);
 // z = P(s v), s = *scale (1 when null); `done` as in the matvec.
 template <typename T>
 int nearfield_apply(msc_plan* pl, const cx<T>* v, const double* scale, cx<T>* z, const int* done);

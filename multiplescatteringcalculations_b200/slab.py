@@ -308,9 +308,11 @@ class SlabPlan:
         the truncated Neumann series), ``dblocks`` (degree x 27 x 9 x 9 complex block
         corrections, default none; entries outside the lattice's mirror-symmetry
         pattern are not applied), ``weights`` the storage of the layer blocks in the
-        complex64 preconditioner ("fp32" or "bf16")."""
-        if weights not in ("fp32", "bf16"):
-            raise ValueError(f"weights must be 'fp32' or 'bf16', got {weights!r}")
+        complex64 preconditioner ("fp32", "bf16", or "bf16_tc": BF16 blocks and
+        activations on the tensor cores)."""
+        modes = {"fp32": N.MSC_NF_WEIGHTS_FP32, "bf16": N.MSC_NF_WEIGHTS_BF16, "bf16_tc": N.MSC_NF_WEIGHTS_BF16_TC}
+        if weights not in modes:
+            raise ValueError(f"weights must be 'fp32', 'bf16' or 'bf16_tc', got {weights!r}")
         c = None
         if coef is not None:
             cc = np.asarray(coef, dtype=np.complex128).ravel()
@@ -325,9 +327,7 @@ class SlabPlan:
             d = np.ascontiguousarray(np.stack([dd.real, dd.imag], -1).ravel())
         N.check(self.lib.msc_set_nearfield(self.handle, int(degree), None if c is None else c.ctypes.data,
                                            None if d is None else d.ctypes.data), "msc_set_nearfield")
-        N.check(self.lib.msc_set_nearfield_weights(
-            self.handle, N.MSC_NF_WEIGHTS_BF16 if weights == "bf16" else N.MSC_NF_WEIGHTS_FP32),
-            "msc_set_nearfield_weights")
+        N.check(self.lib.msc_set_nearfield_weights(self.handle, modes[weights]), "msc_set_nearfield_weights")
 
     def nearfield_scale(self) -> float:
         """s = max |G_nn| of the last build_g0: the unit of the learned block weights."""

@@ -118,3 +118,30 @@ def test_fgmres_falls_back_to_plain_gmres():
     assert _rel(x.cpu().numpy(), ref.cpu().numpy()) < 1e-6
     with pytest.raises(ValueError):
         plan.solve(psi0, tol=1e-8, max_iter=10, preconditioner="bogus")
+
+
+@pytest.mark.parametrize("M,Nz", [(16, 8), (7, 5), (33, 2)])
+def test_precondition_bf16_tensor_cores_match_oracle(M, Nz):
+    """Weights "bf16_tc" run each stencil layer on the tensor cores (tcgen05: BF16
+    operands, FP32 accumulation in tensor memory). Against the oracle in FP64 the
+    difference is the BF16 rounding of weights and activations."""
+    om = 0.7 * REF.beta
+    g = SlabGeometry(M, Nz, 1.0)
+    mat = random_slab_material(g, REF, MaterialContrast(2e9, 1e9, 300.0), 0.5, seed=M + 2 * Nz)
+    plan = SlabPlan(g, REF)
+    plan.build_t0(mat, om)
+    plan.build_g0(om)
+    t4 = O.t0_scalars(om, 1.0, REF.alpha, REF.beta, REF.rho, mat.Dlambda, mat.Dmu, mat.Drho)
+    blocks = O.nearfield_blocks(M, Nz, 1.0, om, REF.alpha, REF.beta, REF.rho)
+    rng = np.random.default_rng(1)
+    x = rng.standard_normal(Nz * M * M * 9) + 1j * rng.standard_normal(Nz * M * M * 9)
+    xt = torch.from_numpy(x.reshape(Nz, M, M, 9))
+    coef = np.array([1.0, 0.8 + 0.1j, 0.5 - 0.2j, 0.1j])
+    dbl = (rng.standard_normal((3, 27, 9, 9)) + 1j * rng.standard_normal((3, 27, 9, 9))) * 0.1 * np.abs(blocks).max()
+    for deg, c, d in ((2, None, None), (3, coef, dbl)):
+        plan.set_nearfield(deg, c, d, weights="bf16_tc")
+        want = O.nearfield_precondition(x, t4, blocks, M, Nz, *(() if c is None else (c, d)))
+        got = plan.precondition(xt, "complex64").cpu().numpy().ravel()
+        assert _rel(got, want) < 2e-2
+        # the complex128 path keeps FP64 weights
+        assert _rel(plan.precondition(xt).cpu().numpy().ravel(), want) < 1e-12
