@@ -56,6 +56,7 @@ int nearfield_extract(msc_plan* pl, const double2* Ks, double scale) {
   MSC_TRY(dalloc(pl, nf->g64_dev, sizeof(double2) * (size_t)(NF_MAXL + 1) * NF_OFFS * 81));
   MSC_TRY(dalloc(pl, nf->g32_dev, sizeof(float2) * (size_t)(NF_MAXL + 1) * NF_OFFS * 81));
   MSC_TRY(dalloc(pl, nf->g16_dev, sizeof(__nv_bfloat162) * (size_t)(NF_MAXL + 1) * NF_OFFS * 81));
+  MSC_TRY(dalloc(pl, nf->gtc_dev, (size_t)NF_MAXL * NF_TC_LAYER_BYTES));
   double2* dst = (double2*)nf->g64_dev.p;
   k_nf_extract<<<ceil_div(NF_OFFS * 81, 256), 256, 0, pl->stream>>>(Ks, pl->g, pl->E, 1.0 / scale, dst);
   ::msc::note_launch();
@@ -235,6 +236,11 @@ int nearfield_refresh(msc_plan* pl) {
   MSC_CUDA(cudaMemcpyAsync(nf->g32_dev.p, nf->h32.data(), sizeof(float2) * nb, cudaMemcpyHostToDevice, pl->stream));
   MSC_CUDA(cudaMemcpyAsync(nf->g16_dev.p, nf->h16.data(), sizeof(__nv_bfloat162) * nb, cudaMemcpyHostToDevice,
                            pl->stream));
+  nf->htc.resize((size_t)L * NF_TC_LAYER_BYTES / 2);
+  for (int l = 0; l < L; ++l)
+    nf_tc_pack_layer(nf->h16.data() + (size_t)l * NF_OFFS * 81, nf->htc.data() + (size_t)l * NF_TC_LAYER_BYTES / 2);
+  MSC_CUDA(cudaMemcpyAsync(nf->gtc_dev.p, nf->htc.data(), (size_t)L * NF_TC_LAYER_BYTES, cudaMemcpyHostToDevice,
+                           pl->stream));
   MSC_CUDA(cudaStreamSynchronize(pl->stream));
   nf->dirty = false;
   return MSC_OK;
@@ -274,7 +280,7 @@ int nearfield_apply(msc_plan* pl, const cx<T>* v, const double* scale, cx<T>* z,
         // the layer on the tensor cores
         MSC_TRY(launch_nf_tc(pl, (const float2*)in, sc, (const float2*)t4, (float2*)h, (float2*)z,
                              make_float2((float)ch.x, (float)ch.y), make_float2((float)c0.x, (float)c0.y), init,
-                             (const __nv_bfloat162*)nf->g16_dev.p + (size_t)(l - 1) * NF_OFFS * 81, done));
+                             (const unsigned char*)nf->gtc_dev.p + (size_t)(l - 1) * NF_TC_LAYER_BYTES, done));
         in = h;
         sc = nullptr;
         continue;

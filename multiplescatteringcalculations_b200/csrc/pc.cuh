@@ -15,6 +15,9 @@ namespace msc {
 
 constexpr int NF_OFFS = 27;   // stencil offsets, o = ((dz + 1) * 3 + dx + 1) * 3 + dy + 1
 constexpr int NF_MAXL = 6;    // polynomial degree limit
+// One layer's blocks packed as the tensor-core operand (pc_tc.cu): 33 tiles of 32 rows x
+// 16 BF16 (27 offsets for DOFs 0-7, 6 for DOF 8).
+constexpr int NF_TC_LAYER_BYTES = (NF_OFFS + 6) * 1024;
 
 // Per-plan state of the preconditioner.
 struct NearField {
@@ -29,11 +32,12 @@ struct NearField {
   // Per-layer blocks g64 + dg[l] on the device, [L][27][81], y_a(v) += g[o][a][b] tau_b(v - o).
   // The kernels read them through these pointers, so a captured solver graph stays valid
   // when the blocks change (a new frequency): only the buffers' contents are refreshed.
-  DBuf g64_dev, g32_dev, g16_dev;
+  DBuf g64_dev, g32_dev, g16_dev, gtc_dev;
   int wbf16 = 0;               // complex64 path: msc_nf_weights (1, 2: BF16 blocks g16_dev; 2: tensor cores)
   std::vector<double2> h64;    // host staging of the refresh
   std::vector<float2> h32;
   std::vector<__nv_bfloat162> h16;
+  std::vector<uint16_t> htc;
   DBuf tmp32, tmp64;           // two field-size work vectors per precision
   bool dirty = true;           // layer blocks to rebuild from g64, dg
 };
@@ -44,10 +48,13 @@ int nearfield_extract(msc_plan* pl, const double2* Ks_spatial, double scale);
 // Upload the per-layer blocks after a change (synchronises the plan's stream; must not
 // run while a graph is being captured).
 int nearfield_refresh(msc_plan* pl);
-// One complex64 stencil layer with BF16 weights on the tensor cores (pc_tc.cu); the
-// arguments as the CUDA-core layer kernel of pc.cu.
+// Pack one layer's BF16 blocks [27][9][9] into the tensor-core operand layout
+// (NF_TC_LAYER_BYTES bytes at out).
+void nf_tc_pack_layer(const __nv_bfloat162* G16, uint16_t* out);
+// One complex64 stencil layer on the tensor cores (pc_tc.cu): the arguments as the
+// CUDA-core layer kernel of pc.cu, with the layer's packed blocks on the device.
 int launch_nf_tc(msc_plan* pl, const float2* x, const double* scale, const float2* t4, float2* h, float2* acc,
-                 float2 ch, float2 c0, int init, const __nv_bfloat162* G16, const int* done);
+                 float2 ch, float2 c0, int init, const void* Bpacked, const int* done);
 // z = P(s v), s = *scale (1 when null); `done` as in the matvec.
 template <typename T>
 int nearfield_apply(msc_plan* pl, const cx<T>* v, const double* scale, cx<T>* z, const int* done);

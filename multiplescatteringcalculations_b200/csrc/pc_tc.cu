@@ -1,27 +1,44 @@
 // Near-field stencil on the 5th-generation tensor cores (tcgen05): the complex64
-// preconditioner layer with BF16 weights (the form the learned network is trained in).
+// preconditioner layer with BF16 weights and activations, FP32 accumulation.
 //
-// One layer y_a(v) = sum_o sum_b G[o][a][b] tau_b(v - o), tau = T0 (s x), is a dense
-// contraction once written as a real GEMM over a tile of 128 voxels:
-//   Y (128 x 32) = A (128 x 496) B^T (496 x 32),
-//   A[v][k]  = tau_b(v - o).re / .im            k = 2 (9 o + b) + {0, 1}   (486 used, 496 padded)
-//   B[n][k]  rows n = 2 a + {0: re, 1: im} of the complex product   (18 used, 32 padded)
-//            (re, re) = G.re, (re, im) = -G.im, (im, re) = G.im, (im, im) = G.re,
-// with the entries the lattice's mirror symmetry sets to zero masked out of B. The block
-// stages tau on the tile plus a one-voxel halo in shared memory (FP32), writes A and B
-// as BF16 in the K-major no-swizzle layout of the tensor core (core matrices of 8 rows x
-// 16 bytes; 8-row groups 128 bytes apart; the two 8-element K chunks of one MMA step
-// LBO bytes apart), and one thread issues the 31 MMA steps (M 128, N 32, K 16) into a
-// 32-column FP32 accumulator in tensor memory. A commit to an mbarrier signals their
-// completion; every thread then reads its voxel's row from tensor memory (tcgen05.ld)
-// and applies the layer's epilogue (h = y; acc = c0 s x + ch y or acc += ch y), as the
-// CUDA-core kernel (pc.cu) does. Accumulation is FP32; tau enters as BF16.
+// One layer y_a(v) = sum_o sum_b G[o][a][b] tau_b(v - o), tau = T0 (s x), is computed
+// per tile of 128 voxels as real GEMMs accumulated in tensor memory, Y (128 x 32) +=
+// A B^T, with the complex products in real form: B rows n = 2 a + {0: re, 1: im},
+// (re, re) = G.re, (re, im) = -G.im, (im, re) = G.im, (im, im) = G.re, and the entries
+// the mirror symmetry of the lattice sets to zero left at zero (18 of 32 rows used).
 //
-// The wait on the mbarrier is bounded: when it runs out the kernel records a timeout
-// in the plan's status word, waits once more (bounded) and frees its tensor memory.
+// The operands are not materialised per offset. The tile is 16 x-lines of 8 voxels along
+// y in one layer z; tau of a halo plane (18 x 10 voxels) is stored in shared memory as
+// BF16 in the K-major no-swizzle layout (core matrices of 8 rows x 16 bytes, row = halo
+// voxel, y fastest, 160 bytes = one halo line between 8-row groups), so an operand that
+// reads the tile's voxels shifted by (dx, dy) is the plane's descriptor started
+// (1 - dx) 10 + (1 - dy) rows later. Each row holds 4 K chunks of 8 BF16:
+//   chunks 0-1: tau_0..tau_7 of the row                (one MMA per offset: 27 MMAs)
+//   chunk 2:    tau_8 of the rows r, r + 1, r + 2       (y neighbours)
+//   chunk 3:    tau_8 of the rows r + 10, r + 11, r + 12 (the next x-line)
+// so two MMAs per dz (started at shifts 0 and 20 rows) cover the 9 (dx, dy) taps of
+// DOF 8: 33 MMAs (M 128, N 32, K 16) per layer instead of 54.
+//
+// A block walks a column of tiles through zc consecutive layers; its halo planes live in
+// a ring of 4 slots, each plane staged once and read by three layers. Warp 8 allocates
+// the tensor memory, copies the layer's packed weights (33 tiles of 1 KB, built on the
+// host when the blocks change) into shared memory with one bulk copy, and issues the MMAs
+// of layer j into accumulator j & 1 once the plane j + 1 is staged and the epilogue of
+// layer j - 2 has drained that accumulator (mbarrier staged[j & 1], 256 arrivals). Warps
+// 0-7 stage planes and run the epilogue: for layer j - 1 they prefetch acc (or x), wait
+// for its MMAs (mbarrier done[(j - 1) & 1], committed by the MMA warp), read the
+// accumulator (tcgen05.ld; warps w and w + 4 share the lane quadrant w & 3 and split the
+// 9 DOFs) and write h = y and acc = c0 s x + ch y or acc += ch y; then they stage plane
+// j + 2 into the slot the MMAs of layer j - 1 released.
+//
+// Every wait on an mbarrier is bounded: when one runs out the kernel records a timeout in
+// the plan's status word and sets the block's abort flag, after which no warp issues or
+// waits for further work, and the tensor memory is freed.
 #include <cuda_bf16.h>
 
+#include <algorithm>
 #include <cstdint>
+#include <cstring>
 
 #include "mv_common.cuh"
 #include "pc.cuh"
@@ -30,31 +47,25 @@ namespace msc {
 
 namespace {
 
-constexpr int TC_TZ = 2, TC_TX = 4, TC_TY = 16, TC_M = TC_TZ * TC_TX * TC_TY;  // 128 voxels
-constexpr int TC_HZ = TC_TZ + 2, TC_HX = TC_TX + 2, TC_HY = TC_TY + 2, TC_HALO = TC_HZ * TC_HX * TC_HY;
-constexpr int TC_K = 496, TC_KC = TC_K / 8, TC_KUSED = 2 * NF_OFFS * 9;  // 486
-constexpr int TC_N = 32, TC_NUSED = 18;
-constexpr int TC_STEPS = TC_K / 16;
-constexpr int TC_A_BYTES = TC_M * TC_K * 2;   // 126976
-constexpr int TC_B_BYTES = TC_N * TC_K * 2;   // 31744
-constexpr int TC_LBO_A = (TC_M / 8) * 128;    // bytes between K chunks of A
-constexpr int TC_LBO_B = (TC_N / 8) * 128;
-constexpr size_t TC_TAU_BYTES = sizeof(float2) * 9 * TC_HALO;
-constexpr size_t TC_ALIGN = 1024;  // operand base alignment in the shared window
-constexpr size_t TC_SMEM = TC_ALIGN + (size_t)TC_A_BYTES + TC_B_BYTES + TC_TAU_BYTES + 16;
-constexpr long long TC_WAIT_LIMIT = 1ll << 22;  // mbarrier polls before a timeout is recorded
-
-__device__ __forceinline__ bool tc_allowed(int o, int a, int b) {
-  const int dz = o / 9 - 1, dx = (o / 3) % 3 - 1, dy = o % 3 - 1;
-  const int zm = (dx == 0 ? 1 : 0) | (dy == 0 ? 2 : 0) | (dz == 0 ? 4 : 0);
-  return ((dof_parity(a) ^ dof_parity(b)) & zm) == 0;
-}
-
-// byte offset of element (row r, k) in a K-major no-swizzle operand with R rows
-template <int R>
-__device__ __forceinline__ uint32_t umma_off(int r, int kc) {
-  return (uint32_t)((kc * (R / 8) + r / 8) * 8 + r % 8) * 16u;
-}
+constexpr int TV_TX = 16, TV_TY = 8, TV_M = TV_TX * TV_TY;                  // 128 voxel rows
+constexpr int TV_HX = TV_TX + 2, TV_HY = TV_TY + 2, TV_PROWS = TV_HX * TV_HY;  // 180 halo rows
+constexpr int TV_STAGE = 256;                 // warps 0-7: staging and epilogue
+constexpr int TV_THREADS = TV_STAGE + 32;     // warp 8: tensor memory, weights, MMA issue
+constexpr int TV_LBO_A = TV_PROWS * 16;       // bytes between the K chunks of a plane
+constexpr int TV_SBO_A = TV_HY * 16;          // bytes between 8-row groups (x-lines)
+constexpr int TV_PLANE = 4 * TV_LBO_A;        // one staged plane: 4 K chunks of 8 BF16
+constexpr int TV_RING = 4;
+constexpr int TV_N = 32;
+constexpr int TV_BTILE = TV_N * 16 * 2;       // one weight tile: 32 rows x 16 BF16
+constexpr int TV_LBO_B = (TV_N / 8) * 128;
+constexpr int TV_TILES = NF_OFFS + 6;         // 27 offsets (DOF 0-7) + 2 per dz (DOF 8)
+constexpr int TV_B_BYTES = TV_TILES * TV_BTILE;
+static_assert(TV_B_BYTES == NF_TC_LAYER_BYTES, "packed layer size");
+static_assert(TV_M == 128, "one accumulator lane per voxel row");
+constexpr int TV_ALIGN = 1024;                // operand base alignment in the shared window
+constexpr int TV_T8_BYTES = TV_RING * TV_PROWS * 8;
+constexpr size_t TV_SMEM = TV_ALIGN + (size_t)TV_B_BYTES + (size_t)TV_RING * TV_PLANE + TV_T8_BYTES + 64;
+constexpr long long TV_WAIT_LIMIT = 1ll << 22;  // mbarrier polls before a timeout is recorded
 
 // shared-memory matrix descriptor (K-major, no swizzle): start >> 4 in bits 0-13, LBO >> 4
 // in bits 16-29, SBO >> 4 in bits 32-45, version 1 in bits 46-47, layout type 0
@@ -69,8 +80,8 @@ __device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, uint32_t lbo, uint
 
 // instruction descriptor: D F32 (bits 4-5 = 1), A and B BF16 (bits 7-9, 10-12 = 1),
 // both K-major, N >> 3 in bits 17-22, M >> 4 in bits 24-28
-constexpr uint32_t TC_IDESC = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(TC_N >> 3) << 17) |
-                              ((uint32_t)(TC_M >> 4) << 24);
+constexpr uint32_t TV_IDESC = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(TV_N >> 3) << 17) |
+                              ((uint32_t)(TV_M >> 4) << 24);
 
 __device__ __forceinline__ uint32_t pack_bf16(float lo, float hi) {
   const __nv_bfloat162 v = __floats2bfloat162_rn(lo, hi);
@@ -89,185 +100,361 @@ __device__ __forceinline__ bool mbar_try_wait(uint32_t addr, uint32_t phase) {
   return ok != 0;
 }
 
-__global__ void __launch_bounds__(TC_M, 1)
+// bounded wait; on a timeout the status word is set and the wait is tried once more
+__device__ __forceinline__ bool mbar_wait_bounded(uint32_t addr, uint32_t phase, int* status) {
+  bool ok = false;
+  for (long long it = 0; it < TV_WAIT_LIMIT && !ok; ++it) ok = mbar_try_wait(addr, phase);
+  if (!ok) {
+    if (status) atomicExch(status, 1);
+    for (long long it = 0; it < TV_WAIT_LIMIT && !ok; ++it) ok = mbar_try_wait(addr, phase);
+  }
+  return ok;
+}
+
+struct TvTile {
+  int x0, y0, z0, zc;
+};
+
+// One halo row of a plane: the 9 components of x and the 4 T0 scalars at its voxel.
+struct HaloRow {
+  float2 xv[9], t[4];
+  bool in;
+};
+
+__device__ __forceinline__ void load_row(HaloRow& hr, int r, int z, const TvTile& tl, const float2* __restrict__ x,
+                                         const float2* __restrict__ t4, const Geo& g) {
+  const int hy = r % TV_HY, hx = r / TV_HY;
+  const int xx = tl.x0 + hx - 1, y = tl.y0 + hy - 1;
+  hr.in = z >= 0 && z < g.Nz && xx >= 0 && xx < g.M && y >= 0 && y < g.M;
+  if (hr.in) {
+    const int site = (z * g.M + xx) * g.M + y;
+#pragma unroll
+    for (int c = 0; c < 9; ++c) hr.xv[c] = x[(size_t)c * g.nsite + site];
+#pragma unroll
+    for (int c = 0; c < 4; ++c) hr.t[c] = t4[(size_t)c * g.nsite + site];
+  }
+}
+
+// tau = T0 (s x) of the row: tau_0..tau_7 as BF16 into chunks 0-1 of its slot, tau_8
+// into the slot's tau_8 line t8
+__device__ __forceinline__ void store_row01(const HaloRow& hr, unsigned char* ring, int slot, int r, float s,
+                                            float2* t8) {
+  float2 v[9];
+  if (hr.in) {
+    const float2 tr = hr.xv[3] + hr.xv[4] + hr.xv[5];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) v[c] = s * (hr.t[0] * hr.xv[c]);
+#pragma unroll
+    for (int c = 3; c < 6; ++c) v[c] = s * (hr.t[1] * tr + hr.t[2] * hr.xv[c]);
+#pragma unroll
+    for (int c = 6; c < 9; ++c) v[c] = s * (hr.t[3] * hr.xv[c]);
+  } else {
+#pragma unroll
+    for (int c = 0; c < 9; ++c) v[c] = make_float2(0.f, 0.f);
+  }
+  uint4* q = reinterpret_cast<uint4*>(ring + slot * TV_PLANE + r * 16);
+  q[0] = make_uint4(pack_bf16(v[0].x, v[0].y), pack_bf16(v[1].x, v[1].y), pack_bf16(v[2].x, v[2].y),
+                    pack_bf16(v[3].x, v[3].y));
+  q[TV_LBO_A / 16] = make_uint4(pack_bf16(v[4].x, v[4].y), pack_bf16(v[5].x, v[5].y), pack_bf16(v[6].x, v[6].y),
+                                pack_bf16(v[7].x, v[7].y));
+  t8[r] = v[8];
+}
+
+__device__ __forceinline__ uint32_t t8_at(const float2* t8, int r) {
+  const float2 v = r < TV_PROWS ? t8[r] : make_float2(0.f, 0.f);
+  return pack_bf16(v.x, v.y);
+}
+
+// chunks 2-3 of row r: tau_8 of the rows r, r + 1, r + 2 and r + 10, r + 11, r + 12
+__device__ __forceinline__ void store_row23(unsigned char* ring, int slot, int r, const float2* t8) {
+  uint4* q = reinterpret_cast<uint4*>(ring + slot * TV_PLANE + r * 16);
+  q[2 * TV_LBO_A / 16] = make_uint4(t8_at(t8, r), t8_at(t8, r + 1), t8_at(t8, r + 2), 0u);
+  q[3 * TV_LBO_A / 16] = make_uint4(t8_at(t8, r + TV_HY), t8_at(t8, r + TV_HY + 1), t8_at(t8, r + TV_HY + 2), 0u);
+}
+
+// barrier of the 8 staging warps only (the MMA warp does not take part)
+__device__ __forceinline__ void stage_bar() { asm volatile("bar.sync 1, %0;\n" ::"n"(TV_STAGE) : "memory"); }
+
+__device__ __forceinline__ void mma_bf16(uint32_t d, uint64_t ad, uint64_t bd, uint32_t accum) {
+  const uint32_t zm = 0;  // disable-output-lane mask: all lanes written
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(d),
+      "l"(ad), "l"(bd), "r"(TV_IDESC), "r"(accum), "r"(zm), "r"(zm), "r"(zm), "r"(zm)
+      : "memory");
+}
+
+// The 33 MMAs of one layer into accumulator d. dA[dz + 1]: descriptor of chunk 0 of the
+// plane of layer z - dz. The start address field is the low 14 bits of a descriptor
+// (address >> 4) and stays below 2^14 here, so byte offsets >> 4 are added to it.
+__device__ __forceinline__ void issue_layer(uint32_t d, const uint64_t (&dA)[3], uint64_t dB) {
+#pragma unroll
+  for (int o = 0; o < NF_OFFS; ++o) {
+    const int dz = o / 9 - 1, dx = (o / 3) % 3 - 1, dy = o % 3 - 1;
+    mma_bf16(d, dA[dz + 1] + (uint64_t)((((1 - dx) * TV_HY + (1 - dy)) * 16) >> 4),
+             dB + (uint64_t)((o * TV_BTILE) >> 4), o > 0 ? 1u : 0u);
+  }
+#pragma unroll
+  for (int dz = -1; dz <= 1; ++dz)
+#pragma unroll
+    for (int part = 0; part < 2; ++part)
+      mma_bf16(d, dA[dz + 1] + (uint64_t)(((part ? 2 * TV_HY * 16 : 0) + 2 * TV_LBO_A) >> 4),
+               dB + (uint64_t)(((NF_OFFS + 2 * (dz + 1) + part) * TV_BTILE) >> 4), 1u);
+}
+
+__device__ __forceinline__ void mbar_arrive(uint32_t addr) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(addr) : "memory");
+}
+
+__global__ void __launch_bounds__(TV_THREADS, 2)
     k_nf_tc(const float2* __restrict__ x, const double* scale, const float2* __restrict__ t4, float2* __restrict__ h,
-            float2* __restrict__ acc, float2 ch, float2 c0, int init, const __nv_bfloat162* __restrict__ G16, Geo g,
+            float2* __restrict__ acc, float2 ch, float2 c0, int init, const uint4* __restrict__ Bg, Geo g, int zc,
             const int* done, int* status) {
   pdl_wait();
   pdl_trigger();
   if (done && *done) return;
   // The operands start on a 1024-byte boundary of the shared address space (with a 128-byte
-  // static block ahead of the dynamic window, the MMA read both operands 16 bytes before
-  // their start), and the mbarrier and the tensor-memory slot follow tau.
+  // static block ahead of the dynamic window, the MMA read its operands 16 bytes before
+  // their start).
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const uint32_t raw_a = (uint32_t)__cvta_generic_to_shared(smem_raw);
-  unsigned char* As = smem_raw + (((raw_a + (uint32_t)TC_ALIGN - 1) & ~((uint32_t)TC_ALIGN - 1)) - raw_a);
-  unsigned char* Bs = As + TC_A_BYTES;
-  float2* tau = reinterpret_cast<float2*>(Bs + TC_B_BYTES);  // [9][TC_HALO]
-  uint64_t& mbar = *reinterpret_cast<uint64_t*>(Bs + TC_B_BYTES + TC_TAU_BYTES);
-  uint32_t& tmem_slot = *reinterpret_cast<uint32_t*>(Bs + TC_B_BYTES + TC_TAU_BYTES + 8);
-  const int tid = threadIdx.x, warp = tid >> 5;
-  const uint32_t mbar_a = (uint32_t)__cvta_generic_to_shared(&mbar);
+  unsigned char* Bs = smem_raw + (((raw_a + (uint32_t)TV_ALIGN - 1) & ~((uint32_t)TV_ALIGN - 1)) - raw_a);
+  unsigned char* ring = Bs + TV_B_BYTES;
+  float2* t8 = reinterpret_cast<float2*>(ring + TV_RING * TV_PLANE);  // [4][180]
+  // mbarriers: done[2] (MMAs of a layer), weights, staged[2] (256 arrivals)
+  uint64_t* mbar = reinterpret_cast<uint64_t*>(ring + TV_RING * TV_PLANE + TV_T8_BYTES);
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(mbar + 5);
+  volatile int* abort_flag = reinterpret_cast<volatile int*>(mbar + 5) + 1;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const uint32_t mb = (uint32_t)__cvta_generic_to_shared(mbar);
+  const uint32_t mb_done = mb, mb_w = mb + 16u, mb_staged = mb + 24u;
   if (tid == 0) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(mbar_a) : "memory");
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(mb_done) : "memory");
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(mb_done + 8u) : "memory");
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(mb_w) : "memory");
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(mb_staged), "n"(TV_STAGE) : "memory");
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(mb_staged + 8u), "n"(TV_STAGE) : "memory");
+    *abort_flag = 0;
     asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
   }
-  if (warp == 0) {
-    const uint32_t slot = (uint32_t)__cvta_generic_to_shared(&tmem_slot);
-    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(slot), "r"(TC_N)
+  if (warp == 8) {
+    const uint32_t slot = (uint32_t)__cvta_generic_to_shared(tmem_slot);
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(slot), "r"(2 * TV_N)
                  : "memory");
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::: "memory");
   }
-  // tile origin
-  const int nby = (g.M + TC_TY - 1) / TC_TY, nbx = (g.M + TC_TX - 1) / TC_TX;
-  const int by = blockIdx.x % nby, bx = (blockIdx.x / nby) % nbx, bz = blockIdx.x / (nby * nbx);
-  const int y0 = by * TC_TY, x0 = bx * TC_TX, z0 = bz * TC_TZ;
+  __syncthreads();
+  const uint32_t b_a = (uint32_t)__cvta_generic_to_shared(Bs), ring_a = (uint32_t)__cvta_generic_to_shared(ring);
+  // tile column and chunk of layers
+  const int nty = (g.M + TV_TY - 1) / TV_TY, ntx = (g.M + TV_TX - 1) / TV_TX;
+  const int col = blockIdx.x % (nty * ntx), chunk = blockIdx.x / (nty * ntx);
+  TvTile tl;
+  tl.y0 = (col % nty) * TV_TY;
+  tl.x0 = (col / nty) * TV_TX;
+  tl.z0 = chunk * zc;
+  tl.zc = min(zc, g.Nz - tl.z0);
   const float s = scale ? (float)(*scale) : 1.f;
-  // tau = T0 (s x) on the tile and its halo (zero outside the slab)
-  for (int i = tid; i < TC_HALO; i += TC_M) {
-    const int hy = i % TC_HY, hx = (i / TC_HY) % TC_HX, hz = i / (TC_HY * TC_HX);
-    const int z = z0 + hz - 1, xx = x0 + hx - 1, y = y0 + hy - 1;
-    float2 v[9];
-    if (z >= 0 && z < g.Nz && xx >= 0 && xx < g.M && y >= 0 && y < g.M) {
-      const int site = (z * g.M + xx) * g.M + y;
-      float2 xv[9];
-#pragma unroll
-      for (int c = 0; c < 9; ++c) xv[c] = x[(size_t)c * g.nsite + site];
-      const float2 tu = t4[site], tl = t4[(size_t)g.nsite + site], td = t4[(size_t)2 * g.nsite + site],
-                   ts = t4[(size_t)3 * g.nsite + site];
-      const float2 tr = xv[3] + xv[4] + xv[5];
-#pragma unroll
-      for (int c = 0; c < 3; ++c) v[c] = s * (tu * xv[c]);
-#pragma unroll
-      for (int c = 3; c < 6; ++c) v[c] = s * (tl * tr + td * xv[c]);
-#pragma unroll
-      for (int c = 6; c < 9; ++c) v[c] = s * (ts * xv[c]);
-    } else {
-#pragma unroll
-      for (int c = 0; c < 9; ++c) v[c] = make_float2(0.f, 0.f);
-    }
-#pragma unroll
-    for (int c = 0; c < 9; ++c) tau[c * TC_HALO + i] = v[c];
-  }
-  // B (weights): TC_N rows x TC_KC chunks of 8
-  for (int u = tid; u < TC_N * TC_KC; u += TC_M) {
-    const int n = u % TC_N, kc = u / TC_N;
-    const int a = n >> 1, rout = n & 1;
-    uint32_t w[4];
-#pragma unroll
-    for (int p = 0; p < 4; ++p) {
-      float f[2];
-#pragma unroll
-      for (int q = 0; q < 2; ++q) {
-        const int k = kc * 8 + 2 * p + q;  // q = rin (k even: re input, odd: im input)
-        float val = 0.f;
-        if (n < TC_NUSED && k < TC_KUSED) {
-          const int pair = k >> 1, o = pair / 9, b = pair % 9;
-          if (tc_allowed(o, a, b)) {
-            const float2 gv = __bfloat1622float2(G16[o * 81 + a * 9 + b]);
-            val = rout == 0 ? (q == 0 ? gv.x : -gv.y) : (q == 0 ? gv.y : gv.x);
-          }
-        }
-        f[q] = val;
-      }
-      w[p] = pack_bf16(f[0], f[1]);
-    }
-    *reinterpret_cast<uint4*>(Bs + umma_off<TC_N>(n, kc)) = make_uint4(w[0], w[1], w[2], w[3]);
-  }
-  __syncthreads();
-  // A (activations): row m = voxel of the tile, TC_KC chunks of 8
-  for (int u = tid; u < TC_M * TC_KC; u += TC_M) {
-    const int m = u % TC_M, kc = u / TC_M;
-    const int vy = m % TC_TY, vx = (m / TC_TY) % TC_TX, vz = m / (TC_TY * TC_TX);
-    uint32_t w[4];
-#pragma unroll
-    for (int p = 0; p < 4; ++p) {
-      const int pair = kc * 4 + p;  // (o, b): one complex value = two consecutive k
-      float2 tv = make_float2(0.f, 0.f);
-      if (pair < NF_OFFS * 9) {
-        const int o = pair / 9, b = pair % 9;
-        const int dz = o / 9 - 1, dx = (o / 3) % 3 - 1, dy = o % 3 - 1;
-        const int hi = ((vz + 1 - dz) * TC_HX + (vx + 1 - dx)) * TC_HY + (vy + 1 - dy);
-        tv = tau[b * TC_HALO + hi];
-      }
-      w[p] = pack_bf16(tv.x, tv.y);
-    }
-    *reinterpret_cast<uint4*>(As + umma_off<TC_M>(m, kc)) = make_uint4(w[0], w[1], w[2], w[3]);
-  }
-  // the generic-proxy writes of A and B become visible to the tensor core's async proxy
-  asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
-  __syncthreads();
-  asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
-  const uint32_t tmem = tmem_slot;
-  if (tid == 0) {
-    const uint32_t a0 = (uint32_t)__cvta_generic_to_shared(As), b0 = (uint32_t)__cvta_generic_to_shared(Bs);
-    for (int st = 0; st < TC_STEPS; ++st) {
-      const uint64_t ad = umma_desc(a0 + (uint32_t)st * 2u * TC_LBO_A, TC_LBO_A, 128);
-      const uint64_t bd = umma_desc(b0 + (uint32_t)st * 2u * TC_LBO_B, TC_LBO_B, 128);
-      const uint32_t accum = st > 0 ? 1u : 0u;
-      const uint32_t z = 0;  // disable-output-lane mask: all lanes written
+  if (warp == 8) {
+    if (lane == 0) {
+      // the layer's packed weights: one bulk copy into shared memory, completed on mb_w
+      asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(mb_w), "r"(TV_B_BYTES)
+                   : "memory");
       asm volatile(
-          "{\n\t.reg .pred p;\n\t"
-          "setp.ne.b32 p, %4, 0;\n\t"
-          "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(tmem),
-          "l"(ad), "l"(bd), "r"(TC_IDESC), "r"(accum), "r"(z), "r"(z), "r"(z), "r"(z)
+          "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(b_a),
+          "l"(Bg), "r"(TV_B_BYTES), "r"(mb_w)
           : "memory");
     }
-    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(mbar_a)
-                 : "memory");
-  }
-  // bounded wait for the MMAs
-  bool ok = false;
-  for (long long it = 0; it < TC_WAIT_LIMIT && !ok; ++it) ok = mbar_try_wait(mbar_a, 0);
-  if (!ok) {
-    if (status) atomicExch(status, 1);
-    for (long long it = 0; it < TC_WAIT_LIMIT && !ok; ++it) ok = mbar_try_wait(mbar_a, 0);
-  }
-  ok = __syncthreads_and(ok) != 0;  // one decision for the block: the loads below are warp-collective
-  asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
-  uint32_t r[32];
-  if (ok) {
-    const uint32_t ta = tmem + ((uint32_t)(warp * 32) << 16);
-    asm volatile(
-        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];\n"
-        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
-          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
-        : "r"(ta));
-    asm volatile(
-        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];\n"
-        : "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
-          "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
-        : "r"(ta + 16u));
-    asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
-  }
-  asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
-  __syncthreads();
-  if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(TC_N) : "memory");
-  if (!ok) return;
-  // epilogue: row m = tid is voxel (vz, vx, vy) of the tile
-  const int vy = tid % TC_TY, vx = (tid / TC_TY) % TC_TX, vz = tid / (TC_TY * TC_TX);
-  const int z = z0 + vz, xx = x0 + vx, y = y0 + vy;
-  if (z >= g.Nz || xx >= g.M || y >= g.M) return;
-  const int site = (z * g.M + xx) * g.M + y;
+  } else {
+    // planes of the layers z0 - 1, z0, z0 + 1 (plane p of the chunk, layer z0 + p, lives in
+    // slot (p + 1) & 3), all rows' loads in flight at once
+    constexpr int NR = (3 * TV_PROWS + TV_STAGE - 1) / TV_STAGE;
+    HaloRow hr[NR];
 #pragma unroll
-  for (int a = 0; a < 9; ++a) {
-    const float2 out = make_float2(__uint_as_float(r[2 * a]), __uint_as_float(r[2 * a + 1]));
-    const size_t e = (size_t)a * g.nsite + site;
-    if (h) h[e] = out;
-    if (init) acc[e] = c0 * (s * x[e]) + ch * out;
-    else acc[e] = acc[e] + ch * out;
+    for (int i = 0; i < NR; ++i) {
+      const int q = tid + i * TV_STAGE;
+      if (q < 3 * TV_PROWS) load_row(hr[i], q % TV_PROWS, tl.z0 + q / TV_PROWS - 1, tl, x, t4, g);
+    }
+#pragma unroll
+    for (int i = 0; i < NR; ++i) {
+      const int q = tid + i * TV_STAGE;
+      if (q < 3 * TV_PROWS) store_row01(hr[i], ring, q / TV_PROWS, q % TV_PROWS, s, t8 + (q / TV_PROWS) * TV_PROWS);
+    }
+    stage_bar();
+#pragma unroll
+    for (int i = 0; i < NR; ++i) {
+      const int q = tid + i * TV_STAGE;
+      if (q < 3 * TV_PROWS) store_row23(ring, q / TV_PROWS, q % TV_PROWS, t8 + (q / TV_PROWS) * TV_PROWS);
+    }
+    asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
   }
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+  const uint32_t tmem = *tmem_slot;
+  if (warp == 8) {
+    if (lane == 0) {
+      bool ok = mbar_wait_bounded(mb_w, 0u, status);  // the weights have landed
+      const uint64_t dB = umma_desc(b_a, TV_LBO_B, 128);
+      for (int j = 0; j < tl.zc && ok && !*abort_flag; ++j) {
+        // plane j + 1 staged and accumulator j & 1 drained: the staging warps' pass j - 1
+        if (j >= 1)
+          ok = mbar_wait_bounded(mb_staged + (uint32_t)(((j - 1) & 1) * 8), (uint32_t)(((j - 1) >> 1) & 1), status);
+        if (!ok) break;
+        asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+        uint64_t dA[3];
+#pragma unroll
+        for (int i = 0; i < 3; ++i)  // plane of layer z0 + j - (i - 1) in slot (j - i + 2) & 3
+          dA[i] = umma_desc(ring_a + (uint32_t)(((j - i + 2) & 3) * TV_PLANE), TV_LBO_A, TV_SBO_A);
+        issue_layer(tmem + (uint32_t)((j & 1) * TV_N), dA, dB);
+        asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(
+                         mb_done + (uint32_t)((j & 1) * 8))
+                     : "memory");
+      }
+      if (!ok) *abort_flag = 1;
+    }
+    __syncwarp();
+  } else {
+    // warps w and w + 4 read the lane quadrant w & 3: voxel row m, DOFs 0-4 (columns 0-9)
+    // or 5-8 (columns 10-17)
+    const int m = (warp & 3) * 32 + lane, half = warp >> 2;
+    const int xx = tl.x0 + (m >> 3), yy = tl.y0 + (m & 7);
+    const bool mine = xx < g.M && yy < g.M;
+    const int a0 = half ? 5 : 0, na = half ? 4 : 5;
+    for (int j = 0; j <= tl.zc; ++j) {
+      const bool stage = j + 2 <= tl.zc;
+      HaloRow hr;
+      if (stage && tid < TV_PROWS) load_row(hr, tid, tl.z0 + j + 2, tl, x, t4, g);
+      if (j >= 1) {
+        const int jp = j - 1;
+        const int site = ((tl.z0 + jp) * g.M + xx) * g.M + yy;
+        float2 pre[5];
+#pragma unroll
+        for (int i = 0; i < 5; ++i) {
+          pre[i] = make_float2(0.f, 0.f);
+          if (mine && i < na) {
+            const size_t e = (size_t)(a0 + i) * g.nsite + site;
+            pre[i] = init ? x[e] : acc[e];
+          }
+        }
+        bool ok = !*abort_flag;
+        if (ok) ok = mbar_wait_bounded(mb_done + (uint32_t)((jp & 1) * 8), (uint32_t)((jp >> 1) & 1), status);
+        if (!ok) *abort_flag = 1;
+        if (__all_sync(0xffffffffu, ok)) {
+          asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+          uint32_t r[10];
+          const uint32_t ta = tmem + ((uint32_t)((warp & 3) * 32) << 16) + (uint32_t)((jp & 1) * TV_N);
+          if (half == 0) {
+            asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];\n"
+                         : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+                           "=r"(r[7])
+                         : "r"(ta));
+            asm volatile("tcgen05.ld.sync.aligned.32x32b.x2.b32 {%0,%1}, [%2];\n" : "=r"(r[8]), "=r"(r[9]) : "r"(ta + 8u));
+          } else {
+            asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];\n"
+                         : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+                           "=r"(r[7])
+                         : "r"(ta + 10u));
+            r[8] = r[9] = 0u;
+          }
+          asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+          if (mine) {
+#pragma unroll
+            for (int i = 0; i < 5; ++i) {
+              if (i >= na) break;
+              const float2 out = make_float2(__uint_as_float(r[2 * i]), __uint_as_float(r[2 * i + 1]));
+              const size_t e = (size_t)(a0 + i) * g.nsite + site;
+              if (h) h[e] = out;
+              acc[e] = init ? c0 * (s * pre[i]) + ch * out : pre[i] + ch * out;
+            }
+          }
+        }
+      }
+      if (stage) {
+        // plane j + 2 (read by the MMAs of layer z0 + j + 1) into the slot the MMAs of
+        // layer z0 + j - 1 released (slot 3 is free at j = 0)
+        const int slot = (j + 3) & 3;
+        if (tid < TV_PROWS) store_row01(hr, ring, slot, tid, s, t8 + slot * TV_PROWS);
+        stage_bar();
+        if (tid < TV_PROWS) store_row23(ring, slot, tid, t8 + slot * TV_PROWS);
+      }
+      asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+      asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+      mbar_arrive(mb_staged + (uint32_t)((j & 1) * 8));
+    }
+  }
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+  if (warp == 8)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(2 * TV_N) : "memory");
+}
+
+inline uint16_t bf16_bits(__nv_bfloat16 v) {
+  uint16_t u;
+  std::memcpy(&u, &v, 2);
+  return u;
+}
+
+inline void put_b(uint16_t* out, int t, int n, int kl, uint16_t v) {
+  const int kc = kl / 8;
+  out[((size_t)t * TV_BTILE + (size_t)(kc * (TV_N / 8) + n / 8) * 128 + (size_t)(n % 8) * 16 + (size_t)(kl % 8) * 2) /
+      2] = v;
+}
+
+// real form of G[o][a][b] into rows 2 a, 2 a + 1 of tile t at K columns kre (re input)
+// and kre + 1 (im input)
+inline void put_block(uint16_t* out, int t, const __nv_bfloat162* G16, int o, int a, int b, int kre) {
+  const int dz = o / 9 - 1, dx = (o / 3) % 3 - 1, dy = o % 3 - 1;
+  const int zm = (dx == 0 ? 1 : 0) | (dy == 0 ? 2 : 0) | (dz == 0 ? 4 : 0);
+  if ((dof_parity(a) ^ dof_parity(b)) & zm) return;  // zero by symmetry
+  const __nv_bfloat162 gv = G16[o * 81 + a * 9 + b];
+  const uint16_t re = bf16_bits(gv.x), im = bf16_bits(gv.y);
+  put_b(out, t, 2 * a, kre, re);
+  put_b(out, t, 2 * a, kre + 1, (uint16_t)(im ^ 0x8000u));
+  put_b(out, t, 2 * a + 1, kre, im);
+  put_b(out, t, 2 * a + 1, kre + 1, re);
 }
 
 }  // namespace
 
+void nf_tc_pack_layer(const __nv_bfloat162* G16, uint16_t* out) {
+  std::memset(out, 0, NF_TC_LAYER_BYTES);
+  // tile o: DOFs 0-7 of offset o, K column 2 b + {re, im}
+  for (int o = 0; o < NF_OFFS; ++o)
+    for (int a = 0; a < 9; ++a)
+      for (int b = 0; b < 8; ++b) put_block(out, o, G16, o, a, b, 2 * b);
+  // tiles 27 + 2 (dz + 1) + part: DOF 8 of the taps (dx, dy = 1 - e), e = 0..2, read from
+  // K chunk c (0: chunk 2 of the row, 1: chunk 3) at K column 8 c + 2 e + {re, im};
+  // part 0: dx = +1 (c = 0) and dx = 0 (c = 1); part 1 (20 rows on): dx = -1 (c = 0)
+  for (int dz = -1; dz <= 1; ++dz)
+    for (int part = 0; part < 2; ++part)
+      for (int c = 0; c < 2; ++c) {
+        if (part == 1 && c == 1) continue;
+        const int dx = part == 0 ? (c == 0 ? 1 : 0) : -1;
+        for (int e = 0; e < 3; ++e) {
+          const int o = ((dz + 1) * 3 + dx + 1) * 3 + (1 - e) + 1;
+          for (int a = 0; a < 9; ++a) put_block(out, NF_OFFS + 2 * (dz + 1) + part, G16, o, a, 8, 8 * c + 2 * e);
+        }
+      }
+}
+
 int launch_nf_tc(msc_plan* pl, const float2* x, const double* scale, const float2* t4, float2* h, float2* acc,
-                 float2 ch, float2 c0, int init, const __nv_bfloat162* G16, const int* done) {
+                 float2 ch, float2 c0, int init, const void* Bpacked, const int* done) {
   const Geo& g = pl->g;
-  const int nb = ((g.M + TC_TY - 1) / TC_TY) * ((g.M + TC_TX - 1) / TC_TX) * ((g.Nz + TC_TZ - 1) / TC_TZ);
+  const int ncol = ((g.M + TV_TY - 1) / TV_TY) * ((g.M + TV_TX - 1) / TV_TX);
+  // layers per block: about two blocks per SM
+  static int sms = 0;
+  if (!sms) {
+    int dev = 0;
+    MSC_CUDA(cudaGetDevice(&dev));
+    MSC_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  }
+  const int nzc = std::min(g.Nz, std::max(1, (2 * sms + ncol - 1) / ncol));
+  const int zc = (g.Nz + nzc - 1) / nzc;
+  const int nb = ncol * ((g.Nz + zc - 1) / zc);
   MSC_CUDA(prep_kernel((const void*)k_nf_tc));
   int* status = (int*)pl->status.p;
-  k_nf_tc<<<nb, TC_M, TC_SMEM, pl->stream>>>(x, scale, t4, h, acc, ch, c0, init, G16, g, done, status);
+  k_nf_tc<<<nb, TV_THREADS, TV_SMEM, pl->stream>>>(x, scale, t4, h, acc, ch, c0, init, (const uint4*)Bpacked, g, zc,
+                                                   done, status);
   ::msc::note_launch();
   MSC_CUDA(cudaGetLastError());
   return MSC_OK;
