@@ -569,7 +569,7 @@ def run_precond_eval(args, wl, rank, world, local_rank) -> int:
         "config": {"workload": "cfg4", "lattice": f"{wl['M']}x{wl['M']}x{wl['N_z']}", "slabs": len(rows),
                    "ell": "U[2,6]", "std": "U[0.1,0.3]", "ka": "U[0.3,1]", "incidence_deg": "U[0,40]",
                    "wave": "P/SV", "tol": wl["tol"], "periodic": False, "restart": 30,
-                   "precond": (f"learned near-field network, degree {net.degree}, BF16 weights, trained on the GPU "
+                   "precond": (f"learned near-field network, degree {net.degree}, BF16 weights, layers on the tensor cores, trained on the GPU "
                                f"on {wl['precond_train']} slabs ({len(net.history[0]['losses'])} Adam steps, "
                                f"{t_train:.1f} s incl. residual generation and validation); selected: "
                                f"{net.history[-1].get('selected', 'trained')}"),

@@ -11,7 +11,8 @@ the truncated Neumann series (c = 1, w = 0). Training minimises the residual of 
 GMRES step on the preconditioned operator, min_alpha ||alpha A P r^ - r^||^2, over
 residuals r^ = r/||r|| of truncated GMRES runs on random contrast slabs, with the
 library's forward and backward kernels and Adam on the device (msc_nf_train); the
-layer weights are BF16 with FP32 accumulation in training and inference. The
+layer weights are BF16 with FP32 accumulation in training and inference, and inference
+runs each layer on the tensor cores (BF16 activations) by default. The
 reference solves without a preconditioner; this module has no counterpart there.
 
 Model selection: ``train_nearfield`` keeps the trained parameters only if flexible
@@ -43,14 +44,16 @@ __all__ = [
 class NearFieldPreconditioner:
     """Parameters of the learned near-field preconditioner: ``coef`` (degree + 1
     complex), ``w`` (degree x 27 x 9 x 9 complex, in units of max |G_nn|) and the Adam
-    state of its training. ``weights`` is the storage of the layer blocks in the
-    complex64 path ("bf16", the training form, or "fp32")."""
+    state of its training. ``weights`` is the form of the layer blocks in the complex64
+    path: "bf16_tc" (default; BF16 blocks and activations on the tensor cores, FP32
+    accumulation), "bf16" (BF16 blocks on the CUDA cores with FP32 activations, the
+    training form) or "fp32"."""
 
     degree: int = 2
     coef: np.ndarray = None
     w: np.ndarray = None
     adam: np.ndarray | None = None
-    weights: str = "bf16"
+    weights: str = "bf16_tc"
     history: list = field(default_factory=list)
 
     def __post_init__(self):

@@ -499,12 +499,14 @@ _NETWORK = None
 
 
 def _packaged_network():
-    """The packaged learned near-field preconditioner (data/nearfield_grf.npz), loaded once."""
+    """The packaged learned near-field preconditioner (data/nearfield_grf.npz), loaded once;
+    its layers run on the tensor cores."""
     global _NETWORK
     if _NETWORK is None:
         from .learned import NearFieldPreconditioner
 
         _NETWORK = NearFieldPreconditioner.load(Path(__file__).resolve().parent / "data" / "nearfield_grf.npz")
+        _NETWORK.weights = "bf16_tc"
     return _NETWORK
 
 
