@@ -644,6 +644,47 @@ def run_matvecs(wl: dict, n: int) -> int:
     return 0
 
 
+def run_precond_apply(wl: dict, n: int) -> int:
+    """Plan + T0 + G0 of the workload, then for the degree-4 near-field polynomial with
+    FP32 blocks (CUDA cores) and with BF16 blocks on the tensor cores: 3 untimed and n
+    timed complex64 applications through msc_precondition (each: 2 layout transposes
+    and 4 stencil launches). Prints the mean time per application of each."""
+    import ctypes as C
+
+    import torch
+
+    from multiplescatteringcalculations_b200 import SlabPlan, _native
+
+    dev = torch.device("cuda", 0)
+    ref, geom, mat, k_hat, omega = make_problem(wl, seed=1000)
+    plan = SlabPlan(geom, ref, periodic=wl["periodic"], device=dev)
+    plan.build_t0(mat, omega)
+    plan.build_g0(omega)
+    lib = _native.load()
+    x = torch.randn(geom.N_z, geom.M, geom.M, 9, dtype=torch.complex64, device=dev)
+    z = torch.empty_like(x)
+    out = {"applications": n, "degree": 4}
+    for weights in ("fp32", "bf16_tc"):
+        plan.set_nearfield(4, weights=weights)
+
+        def apply():
+            _native.check(lib.msc_precondition(plan.handle, C.c_void_p(x.data_ptr()), C.c_void_p(z.data_ptr()),
+                                               _native.MSC_COMPLEX64), "precondition")
+        for _ in range(3):
+            apply()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(n):
+            apply()
+        e1.record()
+        torch.cuda.synchronize()
+        out[f"us_per_application_{weights}"] = e0.elapsed_time(e1) * 1e3 / n
+    print(json.dumps(out))
+    plan.close()
+    return 0
+
+
 def run_sphere(args, wl, rank, local_rank) -> int:
     """Sphere workload: one step = compute_sphere_foldy_lax_fft_gpu (T0, G0, the 9
     incident patterns, 9 mixed-precision solves, T_comp) on the n_sub^3 lattice; the CPU
@@ -720,6 +761,9 @@ def main(argv=None) -> int:
     ap.add_argument("--solve-only", action="store_true", help="timed solves only (for profiler launch lists)")
     ap.add_argument("--train-only", type=int, default=0, metavar="N",
                     help="N Adam steps of the learned preconditioner on one 64x64x16 GRF slab (for kernel profiles)")
+    ap.add_argument("--precond-only", type=int, default=0, metavar="N",
+                    help="build the plan and run N degree-4 near-field preconditioner applications with FP32 "
+                         "blocks and with BF16 blocks on the tensor cores (for kernel profiles)")
     ap.add_argument("--matvec-only", type=int, default=0, metavar="N",
                     help="build the plan and run N complex64 matvecs through msc_matvec (for kernel profiles)")
     args = ap.parse_args(argv)
@@ -731,6 +775,8 @@ def main(argv=None) -> int:
         return run_reference(args, wl, rank, world)
     if args.matvec_only:
         return run_matvecs(wl, args.matvec_only)
+    if args.precond_only:
+        return run_precond_apply(wl, args.precond_only)
     if args.train_only:
         return run_train_steps(args.train_only)
     if "precond_eval" in wl:
