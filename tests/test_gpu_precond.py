@@ -145,3 +145,32 @@ def test_precondition_bf16_tensor_cores_match_oracle(M, Nz):
         assert _rel(got, want) < 2e-2
         # the complex128 path keeps FP64 weights
         assert _rel(plan.precondition(xt).cpu().numpy().ravel(), want) < 1e-12
+
+
+def test_precondition_tensor_cores_several_layers_per_block():
+    """A 100 x 100 x 7 lattice: 91 tile columns, so on a 148-SM B200 each block sweeps a
+    chunk of layers (3, 3 and 1), which exercises the ring of halo planes, the double-
+    buffered accumulator and the mbarrier hand-offs between the staging warps and the MMA
+    warp; the tiles are ragged in x and y (100 = 6 x 16 + 4 = 12 x 8 + 4). The blocks are
+    the plan's own (pinned against the oracle by test_nearfield_blocks_match_oracle); the
+    stencil and polynomial are the oracle's."""
+    M, Nz = 100, 7
+    om = 0.7 * REF.beta
+    g = SlabGeometry(M, Nz, 1.0)
+    mat = random_slab_material(g, REF, MaterialContrast(2e9, 1e9, 300.0), 0.5, seed=5)
+    plan = SlabPlan(g, REF)
+    plan.build_t0(mat, om)
+    plan.build_g0(om)
+    t4 = O.t0_scalars(om, 1.0, REF.alpha, REF.beta, REF.rho, mat.Dlambda, mat.Dmu, mat.Drho)
+    blocks = plan.nearfield_blocks()
+    rng = np.random.default_rng(2)
+    x = rng.standard_normal(Nz * M * M * 9) + 1j * rng.standard_normal(Nz * M * M * 9)
+    xt = torch.from_numpy(x.reshape(Nz, M, M, 9))
+    coef = np.array([1.0, 0.8 + 0.1j, 0.5 - 0.2j, 0.1j])
+    dbl = (rng.standard_normal((3, 27, 9, 9)) + 1j * rng.standard_normal((3, 27, 9, 9))) * 0.1 * np.abs(blocks).max()
+    plan.set_nearfield(3, coef, dbl, weights="bf16_tc")
+    want = O.nearfield_precondition(x, t4, blocks, M, Nz, coef, dbl)
+    got = plan.precondition(xt, "complex64").cpu().numpy().ravel()
+    assert _rel(got, want) < 2e-2
+    # two applications in a row give the same result (no state carried between launches)
+    assert np.array_equal(plan.precondition(xt, "complex64").cpu().numpy().ravel(), got)
