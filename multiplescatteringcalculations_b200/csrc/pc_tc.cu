@@ -255,39 +255,39 @@ __global__ void __launch_bounds__(TV_THREADS, 2)
   tl.z0 = chunk * zc;
   tl.zc = min(zc, g.Nz - tl.z0);
   const float s = scale ? (float)(*scale) : 1.f;
-  if (warp == 8) {
-    if (lane == 0) {
-      // the layer's packed weights: one bulk copy into shared memory, completed on mb_w
-      asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(mb_w), "r"(TV_B_BYTES)
-                   : "memory");
-      asm volatile(
-          "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(b_a),
-          "l"(Bg), "r"(TV_B_BYTES), "r"(mb_w)
-          : "memory");
-    }
-  } else {
-    // planes of the layers z0 - 1, z0, z0 + 1 (plane p of the chunk, layer z0 + p, lives in
-    // slot (p + 1) & 3), all rows' loads in flight at once
-    constexpr int NR = (3 * TV_PROWS + TV_STAGE - 1) / TV_STAGE;
+  if (warp == 8 && lane == 0) {
+    // the layer's packed weights: one bulk copy into shared memory, completed on mb_w
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(mb_w), "r"(TV_B_BYTES)
+                 : "memory");
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(b_a),
+        "l"(Bg), "r"(TV_B_BYTES), "r"(mb_w)
+        : "memory");
+  }
+  // planes of the layers z0 - 1, z0, z0 + 1 (plane p of the chunk, layer z0 + p, lives in
+  // slot (p + 1) & 3), staged by all 288 threads (the MMA warp has nothing to issue yet),
+  // each thread's rows' loads in flight at once
+  constexpr int NR = (3 * TV_PROWS + TV_THREADS - 1) / TV_THREADS;
+  {
     HaloRow hr[NR];
 #pragma unroll
     for (int i = 0; i < NR; ++i) {
-      const int q = tid + i * TV_STAGE;
+      const int q = tid + i * TV_THREADS;
       if (q < 3 * TV_PROWS) load_row(hr[i], q % TV_PROWS, tl.z0 + q / TV_PROWS - 1, tl, x, t4, g);
     }
 #pragma unroll
     for (int i = 0; i < NR; ++i) {
-      const int q = tid + i * TV_STAGE;
+      const int q = tid + i * TV_THREADS;
       if (q < 3 * TV_PROWS) store_row01(hr[i], ring, q / TV_PROWS, q % TV_PROWS, s, t8 + (q / TV_PROWS) * TV_PROWS);
     }
-    stage_bar();
-#pragma unroll
-    for (int i = 0; i < NR; ++i) {
-      const int q = tid + i * TV_STAGE;
-      if (q < 3 * TV_PROWS) store_row23(ring, q / TV_PROWS, q % TV_PROWS, t8 + (q / TV_PROWS) * TV_PROWS);
-    }
-    asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
   }
+  __syncthreads();
+#pragma unroll
+  for (int i = 0; i < NR; ++i) {
+    const int q = tid + i * TV_THREADS;
+    if (q < 3 * TV_PROWS) store_row23(ring, q / TV_PROWS, q % TV_PROWS, t8 + (q / TV_PROWS) * TV_PROWS);
+  }
+  asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
   const uint32_t tmem = *tmem_slot;
