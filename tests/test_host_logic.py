@@ -136,3 +136,37 @@ def test_result_arrays_are_recycled_only_when_unreferenced():
     del c
     d = S._host_array((3, 7))[0]
     assert d is not v.base  # a view keeps it alive
+
+
+def test_nearfield_network_parameters_roundtrip(tmp_path):
+    """The learned network's parameters survive save/load; its complex64 layers default to
+    the tensor cores ("bf16_tc"), and a saved weight form is kept as saved."""
+    from multiplescatteringcalculations_b200 import NearFieldPreconditioner
+
+    net = NearFieldPreconditioner(3)
+    assert net.weights == "bf16_tc"
+    assert_array_equal(net.coef, np.ones(4))
+    assert net.w.shape == (3, 27, 9, 9) and not net.w.any()
+    rng = np.random.default_rng(0)
+    net.coef = rng.standard_normal(4) + 1j * rng.standard_normal(4)
+    net.w = rng.standard_normal((3, 27, 9, 9)) + 1j * rng.standard_normal((3, 27, 9, 9))
+    net.weights = "bf16"
+    net.save(tmp_path / "net.npz")
+    back = NearFieldPreconditioner.load(tmp_path / "net.npz")
+    assert back.degree == 3 and back.weights == "bf16" and back.adam is None
+    assert_array_equal(back.coef, net.coef)
+    assert_array_equal(back.w, net.w)
+    with pytest.raises(ValueError):
+        NearFieldPreconditioner(7)
+    with pytest.raises(ValueError):
+        NearFieldPreconditioner(2, coef=np.ones(5))
+
+
+def test_packaged_network_runs_on_tensor_cores():
+    """The packaged network (data/nearfield_grf.npz, trained in the BF16 form) is installed
+    with its layers on the tensor cores."""
+    from multiplescatteringcalculations_b200.slab import _packaged_network
+
+    net = _packaged_network()
+    assert net.weights == "bf16_tc"
+    assert net.degree == 4 and net.w.shape == (4, 27, 9, 9)
