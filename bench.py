@@ -163,22 +163,31 @@ def rank_seed(base: int, rank: int) -> int:
     return base + rank
 
 
+# The reference arm's CPU solves take about 20 s each at cfg2; the arm times at most
+# this many (after one untimed solve) so that a run with the driver's step count still
+# ends within minutes.
+REFERENCE_MAX_STEPS = 4
+
+
 def run_reference(args, wl, rank, world):
     if rank != 0:
         return 0
     threads = os.cpu_count() or 1
+    steps = max(1, min(args.steps, REFERENCE_MAX_STEPS))
+    warm = min(args.warmup, 1)
     times = []
     last = None
-    for i in range(args.warmup + args.steps):
-        dt, r, tm = cpu_baseline(wl, threads, seed=0)
-        if i >= args.warmup:
+    for i in range(warm + steps):
+        # the slab our arm solves on rank 0 (same seed): the ratio compares the same solve
+        dt, r, tm = cpu_baseline(wl, threads, seed=rank_seed(1000, 0))
+        if i >= warm:
             times.append(dt)
             last = (r, tm)
     ms = float(np.mean(times)) * 1e3
     value = 1e3 / ms
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": args.gpus,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+        "steps": steps, "warmup": warm, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "c128", "data": "synthetic",
         "config": {"workload": args.workload, **_cfg_desc(wl)},
         "cpu_baseline": {"value": value, "unit": "solves/s", "cores": threads, "kind": "port",
@@ -187,6 +196,9 @@ def run_reference(args, wl, rank, world):
                                    f"{last[1]['kernel']:.2f}, solve {last[1]['solve']:.2f}; {last[0]['n_matvec']} "
                                    "matvecs"},
         "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "note": (f"CPU arm: {steps} timed solves after {warm} untimed (of --steps {args.steps} --warmup "
+                 f"{args.warmup}; at most {REFERENCE_MAX_STEPS} timed), each a full solve of the seed-1000 slab "
+                 "that the GPU arm solves"),
     }
     print(json.dumps(line), flush=True)
     return 0
@@ -195,7 +207,194 @@ def run_reference(args, wl, rank, world):
 def _cfg_desc(wl):
     return {"lattice": f"{wl['M']}x{wl['M']}x{wl['N_z']}", "ka": wl["ka"], "incidence_deg": wl["angle"],
             "wave": wl["wave"], "material": list(wl["mat"]), "tol": wl["tol"], "periodic": wl["periodic"],
-            "l2": "inputs larger than L2 (G0 spectrum build and matvec stream > 126 MB per step)"}
+            "seed": 1000,
+            "l2": ("each step rebuilds the G0 spectrum through an FP64 scratch larger than L2 (377 MB at 64x64x16), "
+                   "which flushes L2 between steps; within a step the matvec's working set (octant spectrum and "
+                   "workspace, 45 MB at 64x64x16) stays L2-resident across the GMRES iterations")}
+
+
+def matvec_alg_bytes(plan, geom, entries: int = 45, nrhs: int = 1) -> tuple[int, int]:
+    """Algorithmic bytes of one complex64 operator application on nrhs fields: the
+    stored octant of the G0 spectrum (kz <= Lz/2, ky <= Ly/2, kx <= Lx/2; 45 entries of
+    the symmetric K D form), read once; the 4 T0 scalars per voxel; each field read and
+    its result written once. Also returns the same count for the reference's layout
+    (81 entries on the full padded grid)."""
+    Lz, Lx, Ly = plan.fft_sizes()
+    ns = geom.N_z * geom.M * geom.M
+    b = entries * (Lz // 2 + 1) * (Ly // 2 + 1) * (Lx // 2 + 1) * 8 + 4 * ns * 8 + nrhs * 2 * 9 * ns * 8
+    b_ref = 81 * Lz * Lx * Ly * 8 + 4 * ns * 8 + nrhs * 2 * 9 * ns * 8
+    return b, b_ref
+
+
+def time_matvec_soa(plan, geom, dev, nrep: int = 50, warm: int = 5) -> float:
+    """Seconds per complex64 operator application through msc_matvec_soa (the matvec
+    kernels alone, on the solver's component-major layout), timed with CUDA events on
+    the stream the plan orders its launches after."""
+    import ctypes as C
+
+    import torch
+
+    from multiplescatteringcalculations_b200 import _native
+
+    lib = _native.load()
+    x = torch.randn(9, geom.N_z, geom.M, geom.M, dtype=torch.complex64, device=dev)
+    y = torch.empty_like(x)
+
+    def mv():
+        _native.check(lib.msc_matvec_soa(plan.handle, C.c_void_p(x.data_ptr()), C.c_void_p(y.data_ptr()),
+                                         _native.MSC_COMPLEX64), "msc_matvec_soa")
+    for _ in range(warm):
+        mv()
+    torch.cuda.synchronize()
+    m0, m1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    m0.record(plan.stream)
+    for _ in range(nrep):
+        mv()
+    m1.record(plan.stream)
+    torch.cuda.synchronize()
+    return m0.elapsed_time(m1) / nrep / 1e3
+
+
+def _traffic(name: str):
+    """dram bytes per launch of the committed ncu summary profiles/<name>, if any."""
+    tf = ROOT / "profiles" / name
+    if tf.exists():
+        for ln in tf.read_text().splitlines():
+            if ln.startswith("dram_bytes_per_matvec:"):
+                return float(ln.split(":")[1])
+    return None
+
+
+def matvec_roofline(plan, geom, workload: str, dev) -> dict:
+    """The roofline entry of the complex64 matvec of this plan (HBM bound)."""
+    t_mv = time_matvec_soa(plan, geom, dev)
+    b_alg, b_ref = matvec_alg_bytes(plan, geom)
+    peak, peak_kind = _peaks()
+    achieved = b_alg / t_mv / 1e9
+    return {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+            "traffic": _traffic(f"matvec_{workload}_traffic.txt"),
+            "kernel": "complex64 matvec (msc_matvec_soa: the operator's launches, no layout conversion)",
+            "us_per_matvec": t_mv * 1e6, "alg_bytes": b_alg, "peak_kind": peak_kind,
+            "effective_gbs_reference_layout": b_ref / t_mv / 1e9}
+
+
+def large_grid_roofline(dev) -> dict:
+    """The complex64 matvec on the largest lattice of the workloads: 256 x 256 x 32
+    periodic (ka = 1, GRF std 40 %, seed 1000), padded grid 64 x 256 x 256, octant
+    spectrum 198 MB, above the 126 MB L2, so HBM binds."""
+    wl = WORKLOADS["cfg5"]
+    from multiplescatteringcalculations_b200 import SlabPlan
+
+    ref, geom, mat, k_hat, omega = make_problem(wl, seed=1000)
+    plan = SlabPlan(geom, ref, periodic=True, device=dev)
+    plan.build_t0(mat, omega)
+    plan.build_g0(omega)
+    out = matvec_roofline(plan, geom, "cfg5", dev)
+    out["lattice"] = "256x256x32 periodic"
+    out["fft"] = list(plan.fft_sizes())
+    plan.close()
+    return out
+
+
+def cfg1_sample(dev, nrep: int = 20) -> dict:
+    """The CPU-runnable 16 x 16 x 4 case (ka 0.2, i.i.d. +-10 %, seed 0, periodic,
+    normal P, tol 1e-10): GPU ms per solve (T0, G0, incident, solve, R_PP) and psi and
+    R_PP against the oracle's FP64 solve (tol 1e-12)."""
+    import torch
+
+    from multiplescatteringcalculations_b200 import SlabPlan
+    from oracle import slab_oracle as O
+
+    wl = WORKLOADS["cfg1"]
+    ref, geom, mat, k_hat, omega = make_problem(wl, seed=0)
+    plan = SlabPlan(geom, ref, periodic=True, device=dev)
+
+    def step():
+        plan.build_t0(mat, omega)
+        plan.build_g0(omega)
+        psi0 = plan.incident(omega, k_hat, wl["wave"])
+        x, st = plan.solve(psi0, tol=wl["tol"], max_iter=500, restart=30, precision="mixed")
+        return x, st, plan.rpp_periodic(x, omega)
+
+    for _ in range(3):
+        step()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(plan.stream)
+    for _ in range(nrep):
+        x, st, rpp = step()
+    e1.record(plan.stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / nrep
+    ora = O.solve(geom.M, geom.N_z, geom.a, ref.alpha, ref.beta, ref.rho, mat.Dlambda, mat.Dmu, mat.Drho, omega,
+                  k_hat, wl["wave"], 1e-12, 500, periodic=True, restart=30)
+    rpp_o = O.rpp_periodic(ora["psi"], ora["t4"], geom.M, geom.N_z, geom.a, omega, ref.alpha, ref.rho)
+    psi = x.cpu().numpy()
+    plan.close()
+    return {"lattice": "16x16x4", "ms_per_solve": ms, "solves_per_s": 1e3 / ms, "n_matvec": st["n_matvec"],
+            "residual": st["residual"],
+            "psi_rel_err": float(np.linalg.norm(psi - ora["psi"]) / np.linalg.norm(ora["psi"])),
+            "rpp_rel_err": float(abs(rpp - rpp_o) / abs(rpp_o))}
+
+
+# held-out slabs of the learned-preconditioner distribution (cfg4_problem seeds) on which
+# every solver setting converges within the budget
+CFG4_SAMPLE_SEEDS = (5003, 5005, 5007)
+
+
+def cfg4_sample(dev, seeds=CFG4_SAMPLE_SEEDS, tol: float = 1e-8) -> dict:
+    """Time to 1e-8 (FP64 true residual) per held-out 64 x 64 x 16 GRF slab of the
+    learned-preconditioner distribution for plain FP64 GMRES(30), plain mixed precision,
+    mixed precision with the physics Neumann polynomial of the network's degree (layers
+    on the tensor cores), and mixed precision with the packaged learned network (no
+    training in the timed region); each solve includes T0, G0, incident and R_PP; one
+    untimed and one timed solve per slab and setting."""
+    import torch
+
+    from multiplescatteringcalculations_b200 import SlabPlan
+    from multiplescatteringcalculations_b200.learned import NearFieldPreconditioner
+    from multiplescatteringcalculations_b200.slab import _packaged_network
+
+    net = _packaged_network()
+    physics = NearFieldPreconditioner(net.degree)
+    variants = {"fp64": ("fp64", None), "mixed": ("mixed", None),
+                f"mixed_nearfield_d{net.degree}_tc": ("mixed", physics), "mixed_learned": ("mixed", net)}
+    wl = WORKLOADS["cfg4"]
+    rows = []
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    for seed in seeds:
+        ref, g, mat, kh, om, wave, par = cfg4_problem(wl, seed)
+        plan = SlabPlan(g, ref, periodic=False, device=dev)
+        md = type(mat)(torch.from_numpy(mat.Dlambda).to(dev), torch.from_numpy(mat.Dmu).to(dev),
+                       torch.from_numpy(mat.Drho).to(dev), ref)
+        row = {"seed": seed, "ell": par[0], "std": par[1], "ka": par[2], "wave": wave}
+        for name, (prec, pc) in variants.items():
+            def step():
+                plan.build_t0(md, om)
+                plan.build_g0(om)
+                psi0 = plan.incident(om, kh, wave)
+                if pc is not None:
+                    pc.install(plan)
+                x, st = plan.solve(psi0, tol=tol, max_iter=6000, restart=30, precision=prec,
+                                   preconditioner=None if pc is None else "nearfield")
+                plan.rpp_periodic(x, om)
+                return st
+            step()
+            torch.cuda.synchronize()
+            e0.record(plan.stream)
+            st = step()
+            e1.record(plan.stream)
+            torch.cuda.synchronize()
+            row[name] = {"ms": e0.elapsed_time(e1), "n_matvec": st["n_matvec"], "n_precond": st["n_precond"],
+                         "residual": st["residual"], "pc_fallback": st["pc_fallback"]}
+        rows.append(row)
+        plan.close()
+    tot = {n: float(sum(r[n]["ms"] for r in rows)) for n in variants}
+    return {"slabs": len(rows), "lattice": "64x64x16", "tol": tol,
+            "all_converged": all(r[n]["residual"] <= tol for r in rows for n in variants),
+            "ms_per_solve": {n: tot[n] / len(rows) for n in variants},
+            "speedup_vs_fp64_plain": {n: tot["fp64"] / tot[n] for n in variants},
+            "per_slab": rows}
 
 
 def run_ours(args, wl, rank, world, local_rank):
@@ -224,6 +423,7 @@ def run_ours(args, wl, rank, world, local_rank):
                            preconditioner=None if args.precond == "none" else args.precond)
         stats.update(st)
         stats["rpp"] = plan.rpp_periodic(x, omega)
+        stats["x"] = x
         return x
 
     for _ in range(args.warmup):
@@ -257,96 +457,68 @@ def run_ours(args, wl, rank, world, local_rank):
         plan.close()
         return 0
 
-    # ---- the plain FP64 GMRES solve of the same slab (the comparator) ----
-    def step64():
-        plan.build_t0(mat_dev, omega)
-        plan.build_g0(omega)
-        psi0 = plan.incident(omega, k_hat, wl["wave"])
-        return plan.solve(psi0, tol=wl["tol"], max_iter=1000, restart=args.restart, precision="fp64")[1]
+    # ---- the comparator and the other solver settings on the same slab ----
+    from multiplescatteringcalculations_b200.slab import _packaged_network
 
-    step64()
-    torch.cuda.synchronize()
+    net = _packaged_network()
+
+    def pc_nearfield_tc(p):
+        p.set_nearfield(2, weights="bf16_tc")
+
+    arms = {
+        # plain FP64 GPU GMRES(30): the comparator of the metric
+        "fp64": ("fp64", None),
+        # the near-field Neumann polynomial (degree 2), layers on the tensor cores
+        "mixed_nearfield_tc": ("mixed", pc_nearfield_tc),
+        # the packaged learned network (degree 4, BF16, layers on the tensor cores)
+        "mixed_learned": ("mixed", net.install),
+    }
+    if args.precond != "none":
+        arms["mixed_plain"] = ("mixed", None)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    nrep64 = max(1, min(args.steps, 3))
-    for _ in range(nrep64):
-        st64 = step64()
-    e1.record(stream)
-    torch.cuda.synchronize()
-    ms64 = e0.elapsed_time(e1) / nrep64
+    nrep = max(1, min(args.steps, 3))
+    arm_out = {}
+    for name, (prec, pc) in arms.items():
+        def step_arm():
+            plan.build_t0(mat_dev, omega)
+            plan.build_g0(omega)
+            psi0 = plan.incident(omega, k_hat, wl["wave"])
+            if pc is not None:
+                pc(plan)
+            return plan.solve(psi0, tol=wl["tol"], max_iter=1000, restart=args.restart, precision=prec,
+                              preconditioner=None if pc is None else "nearfield")[1]
 
-    # ---- the other mixed-precision variant (with / without the near-field preconditioner) ----
-    other = "nearfield" if args.precond == "none" else "none"
+        step_arm()
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for _ in range(nrep):
+            st_a = step_arm()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        arm_out[name] = {"ms_per_solve": e0.elapsed_time(e1) / nrep, "n_matvec": st_a["n_matvec"],
+                         "n_precond": st_a["n_precond"], "pc_fallback": st_a["pc_fallback"],
+                         "residual": st_a["residual"]}
+    ms64 = arm_out["fp64"]["ms_per_solve"]
+    for a in arm_out.values():
+        a["speedup_vs_fp64_plain"] = ms64 / a["ms_per_solve"]
+    ms_main = ms_max / args.steps
 
-    def step_other():
-        plan.build_t0(mat_dev, omega)
-        plan.build_g0(omega)
-        psi0 = plan.incident(omega, k_hat, wl["wave"])
-        if other != "none":
-            plan.set_nearfield()
-        return plan.solve(psi0, tol=wl["tol"], max_iter=1000, restart=args.restart, precision="mixed",
-                          preconditioner=None if other == "none" else other)[1]
-
-    step_other()
-    torch.cuda.synchronize()
-    e0.record(stream)
-    for _ in range(nrep64):
-        st_o = step_other()
-    e1.record(stream)
-    torch.cuda.synchronize()
-    ms_o = e0.elapsed_time(e1) / nrep64
-
-    # ---- roofline of the complex64 matvec, timed live ----
-    x32 = torch.randn(geom.N_z, geom.M, geom.M, 9, dtype=torch.complex64, device=dev)
+    # ---- roofline of the complex64 matvec, timed live on the plan's stream ----
+    roof = matvec_roofline(plan, geom, args.workload, dev)
     Lz, Lx, Ly = plan.fft_sizes()
-    import ctypes as C
-
     ns = geom.N_z * geom.M * geom.M
-    # octant kernel spectrum (kz <= Lz/2, ky <= Ly/2, kx <= Lx/2; 45 entries, complex64)
-    E = 45
-    b_alg = E * (Lz // 2 + 1) * (Ly // 2 + 1) * (Lx // 2 + 1) * 8 + 4 * ns * 8 + 2 * 9 * ns * 8
-    b_alg_ref = 81 * Lz * Lx * Ly * 8 + 4 * ns * 8 + 2 * 9 * ns * 8
-    # the SoA matvec (no layout conversion): measured through the internal launcher
-    y32 = torch.empty_like(x32)
-    nrep = 50
-    for _ in range(5):
-        lib.msc_matvec(plan.handle, C.c_void_p(x32.data_ptr()), C.c_void_p(y32.data_ptr()), 0)
-    torch.cuda.synchronize()
-    m0, m1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    m0.record(stream)
-    for _ in range(nrep):
-        lib.msc_matvec(plan.handle, C.c_void_p(x32.data_ptr()), C.c_void_p(y32.data_ptr()), 0)
-    m1.record(stream)
-    torch.cuda.synchronize()
-    t_mv = m0.elapsed_time(m1) / nrep / 1e3
-    # the layout conversions of msc_matvec (2 transposes of the field) are part of this time
-    peak, peak_kind = _peaks()
-    achieved = b_alg / t_mv / 1e9
-    traffic = None
-    tf = ROOT / "profiles" / f"matvec_{args.workload}_traffic.txt"  # warm-cache ncu capture, per matvec
-    if tf.exists():
-        for ln in tf.read_text().splitlines():
-            if ln.startswith("dram_bytes_per_matvec:"):
-                traffic = float(ln.split(":")[1])
-
     line = {
         "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
+        "warmup": args.warmup, "ms_per_step": ms_main, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "c64+c128", "data": "synthetic",
         "config": {"workload": args.workload, **_cfg_desc(wl), "restart": args.restart, "fft": [Lz, Lx, Ly]},
         "gpu_launches": int(launches),
         "solve": {"n_matvec": stats["n_matvec"], "n_matvec64": stats["n_matvec64"], "n_outer": stats["n_outer"],
                   "n_precond": stats["n_precond"], "pc_fallback": stats["pc_fallback"], "precond": args.precond,
                   "residual": stats["residual"], "rpp": [stats["rpp"].real, stats["rpp"].imag]},
-        "fp64": {"ms_per_solve": ms64, "n_matvec": st64["n_matvec"], "residual": st64["residual"],
-                 "speedup_mixed_vs_fp64": ms64 / (ms_max / args.steps)},
-        f"mixed_precond_{other}": {"ms_per_solve": ms_o, "n_matvec": st_o["n_matvec"], "n_precond": st_o["n_precond"],
-                                   "residual": st_o["residual"]},
-        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                     "traffic": traffic, "kernel": "complex64 matvec (3 launches + 2 layout transposes)",
-                     "us_per_matvec": t_mv * 1e6, "alg_bytes": b_alg,
-                     "peak_kind": peak_kind,
-                     "effective_gbs_reference_layout": b_alg_ref / t_mv / 1e9},
+        "fp64": {**arm_out["fp64"], "speedup_mixed_vs_fp64": ms64 / ms_main},
+        **{k: v for k, v in arm_out.items() if k != "fp64"},
+        "roofline": roof,
     }
     if rank == 0 and not args.no_e2e:
         # public API from pinned host arrays; the plan cache keeps allocations out of the loop
@@ -373,14 +545,27 @@ def run_ours(args, wl, rank, world, local_rank):
                        "d2h_bytes_per_step": 2 * 9 * ns * 16 + 4 * ns * 16,
                        "ms_per_solve": dt / args.steps * 1e3, "ms_per_call": [round(c, 2) for c in calls],
                        "residual": r.gmres_residual}
+    if rank == 0 and world == 1 and args.workload == "cfg2" and not args.no_extra:
+        line["roofline_large"] = large_grid_roofline(dev)
+        line["cfg1"] = cfg1_sample(dev)
+        line["cfg4_sample"] = cfg4_sample(dev)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        from oracle import slab_oracle as O
+
         threads = os.cpu_count() or 1
-        dt, rr, tm = cpu_baseline(wl, threads, seed=1000)
+        dt, rr, tm = cpu_baseline(wl, threads, seed=rank_seed(1000, rank))
         line["cpu_baseline"] = {"value": 1.0 / dt, "unit": "solves/s", "cores": threads, "kind": "port",
-                                "sample": f"one {args.workload} solve by the oracle port (numpy/scipy FP64, scipy "
-                                          f"GMRES(30) to {wl['tol']:g}; t0 {tm['t0']:.2f} s, kernel "
-                                          f"{tm['kernel']:.2f} s, solve {tm['solve']:.2f} s, "
+                                "sample": f"one {args.workload} solve (seed 1000, the slab the GPU solves) by the "
+                                          f"oracle port (numpy/scipy FP64, scipy GMRES(30) to {wl['tol']:g}; t0 "
+                                          f"{tm['t0']:.2f} s, kernel {tm['kernel']:.2f} s, solve {tm['solve']:.2f} s, "
                                           f"{rr['n_matvec']} matvecs)"}
+        # the GPU's solution of the timed step against the oracle's FP64 solve of the same slab
+        psi = stats["x"].cpu().numpy()
+        rpp_o = O.rpp_periodic(rr["psi"], rr["t4"], geom.M, geom.N_z, geom.a, omega, ref.alpha, ref.rho)
+        line["parity"] = {"psi_rel_err": float(np.linalg.norm(psi - rr["psi"]) / np.linalg.norm(rr["psi"])),
+                          "rpp_rel_err": float(abs(stats["rpp"] - rpp_o) / abs(rpp_o)),
+                          "oracle_residual": rr["residual"], "gpu_residual": stats["residual"],
+                          "note": "both solves to the workload's tolerance on the same seed-1000 slab"}
     line["clocks"] = clk.summary()
     if rank == 0:
         print(json.dumps(line), flush=True)
@@ -701,17 +886,17 @@ def run_sphere(args, wl, rank, local_rank) -> int:
     con = MaterialContrast(2.0e9, 1.0e9, 100.0)
     omega = wl["ka_p"] * ref.alpha / wl["radius"]
 
-    def step():
+    def step(solver="multi"):
         return compute_sphere_foldy_lax_fft_gpu(omega, wl["radius"], ref, con, wl["n_sub"], wave_type=wl["wave"],
-                                                gmres_tol=wl["tol"], gmres_maxiter=2000, device=dev)
+                                                gmres_tol=wl["tol"], gmres_maxiter=2000, device=dev, solver=solver)
 
     for _ in range(max(3, args.warmup)):
         step()
     torch.cuda.synchronize()
     n0 = lib.msc_launch_count()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    stream = torch.cuda.current_stream(dev)
     with ClockSampler(local_rank) as clk:
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        stream = torch.cuda.current_stream(dev)
         e0.record(stream)
         for _ in range(args.steps):
             r = step()
@@ -720,6 +905,17 @@ def run_sphere(args, wl, rank, local_rank) -> int:
     ms = e0.elapsed_time(e1) / args.steps
     launches = lib.msc_launch_count() - n0
     nmv = [st["n_matvec"] for st in r.stats]
+    # the reference's form: one GMRES solve per incident pattern
+    for _ in range(2):
+        step("columns")
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(args.steps):
+        rc = step("columns")
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms_cols = e0.elapsed_time(e1) / args.steps
+    t_err = float(np.linalg.norm(r.T_comp_9x9 - rc.T_comp_9x9) / np.linalg.norm(rc.T_comp_9x9))
     line = {
         "metric": "sphere composite T-matrices/s (9 right-hand sides each)", "value": 1e3 / ms,
         "unit": "T-matrices/s", "n_gpus": 1, "steps": args.steps, "warmup": max(3, args.warmup), "ms_per_step": ms,
@@ -727,8 +923,12 @@ def run_sphere(args, wl, rank, local_rank) -> int:
         "config": {"workload": "sphere", "n_sub": wl["n_sub"], "cells": r.n_cells, "radius": wl["radius"],
                    "ka_p": wl["ka_p"], "wave": wl["wave"], "tol": wl["tol"], "precision": "mixed",
                    "l2": "inputs larger than L2 (G0 spectrum build per step)"},
-        "gpu_launches": int(launches), "n_matvec_per_column": nmv,
-        "max_residual": max(st["residual"] for st in r.stats), "clocks": clk.summary(),
+        "gpu_launches": int(launches),
+        "solver": "the 9 patterns as one stacked system of multi-RHS matvecs (msc_solve_multi)",
+        "n_multi_matvec": nmv[0], "max_residual": max(st["residual"] for st in r.stats),
+        "columns": {"ms_per_step": ms_cols, "n_matvec_per_column": [st["n_matvec"] for st in rc.stats],
+                    "speedup_multi_vs_columns": ms_cols / ms, "T_comp_rel_diff": t_err},
+        "clocks": clk.summary(),
     }
     if rank == 0 and not args.no_cpu_baseline:
         from oracle import slab_oracle as O
@@ -758,6 +958,8 @@ def main(argv=None) -> int:
     ap.add_argument("--restart", type=int, default=30, help="GMRES restart length of the timed solves")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-extra", action="store_true",
+                    help="cfg2: skip the large-grid roofline, the cfg1 case and the cfg4 held-out sample")
     ap.add_argument("--solve-only", action="store_true", help="timed solves only (for profiler launch lists)")
     ap.add_argument("--train-only", type=int, default=0, metavar="N",
                     help="N Adam steps of the learned preconditioner on one 64x64x16 GRF slab (for kernel profiles)")

@@ -33,7 +33,8 @@ enum msc_status {
   MSC_ERR_CUDA = -3,         /* CUDA runtime error */
   MSC_ERR_NOMEM = -4,        /* device allocation failed */
   MSC_ERR_STATE = -5,        /* call out of order (e.g. matvec before build_t0/build_g0) */
-  MSC_ERR_NONFINITE = -6     /* NaN/Inf met in the solve */
+  MSC_ERR_NONFINITE = -6,    /* NaN/Inf met in the solve */
+  MSC_ERR_TIMEOUT = -7       /* a kernel's bounded wait ran out (msc_plan_set_wait_limit); the result is invalid */
 };
 
 enum msc_precision { MSC_COMPLEX64 = 0, MSC_COMPLEX128 = 1 };
@@ -86,6 +87,19 @@ int msc_plan_set_stream(msc_plan* plan, void* stream);
 int msc_plan_fft_sizes(const msc_plan* plan, int32_t* out3);
 /* Device bytes currently held by the plan. */
 int64_t msc_plan_device_bytes(const msc_plan* plan);
+/* Polls of an mbarrier before a bounded wait inside the tensor-core stencil gives up
+ * (0 = the default, 2^22 polls, far beyond any wait of a correct launch; a poll may
+ * itself suspend the thread for a short hardware-defined time). When a wait runs out
+ * the kernel stops issuing work, drains its copies and MMAs already in flight, frees
+ * its tensor memory, records the timeout in the plan's status word and returns;
+ * msc_solve then returns MSC_ERR_TIMEOUT. inject = 1 makes the stencil also wait on an
+ * mbarrier that nothing completes, so that this path runs (with a small limit, quickly)
+ * and can be tested without a fault; inject = 0 for normal work. No counterpart in the
+ * reference (failure handling of this library). */
+int msc_plan_set_wait_limit(msc_plan* plan, int64_t polls, int inject);
+/* The plan's status word (synchronises the plan's stream) and clear it: *word = 1 when
+ * a bounded wait ran out since the last read. No counterpart in the reference. */
+int msc_plan_status(msc_plan* plan, int32_t* word);
 
 /* Per-voxel T0 from the contrasts dlam, dmu, drho (device, float64, N_z*M*M each,
  * (N_z, M, M) C order) at angular frequency omega. Replaces compute_slab_tmatrices
@@ -116,17 +130,27 @@ int msc_incident(msc_plan* plan, double omega, const double* k_hat, int wave_typ
  * _slab_matvec (slab_scattering.py:359-418). x and y may not alias. */
 int msc_matvec(msc_plan* plan, const void* x, void* y, int precision);
 
+/* The same operator on the component-major layout the solver keeps its Krylov
+ * vectors in: x, y (9, N_z, M, M) complex, x[c][n][i][j]. No layout conversion and no
+ * allocation (the plan's workspace exists from msc_plan_create); this is the operator
+ * alone, as GMRES applies it. x and y may not alias. The reference has one layout
+ * only; this is the kernel part of _slab_matvec_gpu (slab_scattering_gpu.py:95-155). */
+int msc_matvec_soa(msc_plan* plan, const void* x, void* y, int precision);
+
 /* The same operator as msc_matvec, for callers that cannot allocate device memory
  * when they apply it: a host framework whose allocator owns the device memory and
  * forbids other allocations, or a real-time loop that must not risk an allocation's
  * latency or failure mid-run. msc_matvec allocates two field copies on first use;
  * this call allocates nothing. Its scratch is one static device array of this
  * library, at most 64 MiB, resident on every GPU that loads the library until the
- * process exits. A plan needing more (9*Lz*Ly*Lx + 18*N_z*M*M complex elements,
- * each aligned up to 256 bytes) is rejected with MSC_ERR_INVALID. The first call on a
- * device looks the array up with cudaGetSymbolAddress (make it with that device
- * current, before any stream capture). All calls share the array: calls whose GPU
- * work overlaps race on it. No counterpart in the reference. */
+ * process exits. A plan needing more (a workspace of 9*N_z*Ly*Lx complex elements
+ * plus two fields of 9*N_z*M*M, each part aligned up to 256 bytes; (Lz, Lx, Ly) from
+ * msc_plan_fft_sizes) is rejected with MSC_ERR_INVALID, and so is a call made while
+ * another device than the plan's is current. The first call on a device looks the
+ * array up with cudaGetSymbolAddress (make it before any stream capture); the address
+ * is kept until exit, so the library is not usable across a cudaDeviceReset. All
+ * calls share the array: calls whose GPU work overlaps race on it. No counterpart
+ * in the reference. */
 int msc_matvec_noalloc(msc_plan* plan, const void* x, void* y, int precision);
 
 /* Near-field polynomial preconditioner (an addition of this library; the reference
@@ -175,6 +199,31 @@ int msc_nf_loss_grad(msc_plan* plan, const void* r, int precision, int degree, c
  * start) carries the optimiser state between calls; losses (steps doubles) may be NULL. */
 int msc_nf_train(msc_plan* plan, const void* r, int n_res, int degree, int steps, double lr, double* coef, double* w,
                  double* adam, double* losses);
+
+/* Largest number of right-hand sides of msc_solve_multi and msc_matvec_multi. */
+#define MSC_MAX_RHS 64
+
+/* y_r = (I - G0 T0) x_r for nrhs fields at once: x, y (nrhs, 9, N_z, M, M) complex of
+ * the given precision in the component-major layout of msc_matvec_soa, one field after
+ * the other. Each block of the fused z pass stages its slice of the G0 spectrum once
+ * and applies it to the same columns of all nrhs fields, so the spectrum is read once
+ * per application instead of once per field. The plan keeps a workspace of nrhs
+ * fields (allocated on first use). The reference applies its operator one column at a
+ * time (sphere_scattering_fft_gpu.py:199-216); this is the batched form. */
+int msc_matvec_multi(msc_plan* plan, int nrhs, const void* x, void* y, int precision);
+
+/* Solve (I - G0 T0) x_r = b_r for nrhs right-hand sides at once; b, x complex128
+ * (nrhs, N_z, M, M, 9). Each b_r is scaled to unit norm and the stacked system is
+ * solved by one restarted GMRES (mixed precision or FP64 as opts->precision; the near-
+ * field preconditioner as opts->preconditioner) whose operator applications are
+ * msc_matvec_multi, to a stacked relative residual of tol / sqrt(nrhs), which bounds
+ * every right-hand side's relative residual by tol. stats (nrhs entries, may be NULL)
+ * gets the shared counters (n_matvec counts multi-RHS applications) with each right-
+ * hand side's FP64 residual and status; the return is the worst status. Replaces the
+ * loop of one GMRES solve per incident pattern of compute_sphere_foldy_lax_fft_gpu
+ * (sphere_scattering_fft_gpu.py:199-216). */
+int msc_solve_multi(msc_plan* plan, int nrhs, const void* b, void* x, const msc_solve_opts* opts,
+                    msc_solve_stats* stats);
 
 /* Solve (I - G0 T0) x = b; b, x complex128 (N_z, M, M, 9). Restarted GMRES with
  * CGS2 Arnoldi and FP64 Givens/least squares; precision MIXED runs complex64

@@ -21,6 +21,8 @@ MSC_ERR_CUDA = -3
 MSC_ERR_NOMEM = -4
 MSC_ERR_STATE = -5
 MSC_ERR_NONFINITE = -6
+MSC_ERR_TIMEOUT = -7
+MSC_MAX_RHS = 64
 
 MSC_COMPLEX64 = 0
 MSC_COMPLEX128 = 1
@@ -101,6 +103,8 @@ SIGNATURES = {
     "msc_plan_set_stream": (C.c_int, [C.c_void_p, C.c_void_p]),
     "msc_plan_fft_sizes": (C.c_int, [C.c_void_p, C.POINTER(C.c_int32)]),
     "msc_plan_device_bytes": (C.c_int64, [C.c_void_p]),
+    "msc_plan_set_wait_limit": (C.c_int, [C.c_void_p, C.c_int64, C.c_int]),
+    "msc_plan_status": (C.c_int, [C.c_void_p, C.POINTER(C.c_int32)]),
     "msc_build_t0": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_double]),
     "msc_t0_scalars": (C.c_int, [C.c_void_p, C.c_void_p]),
     "msc_set_t0_scalars": (C.c_int, [C.c_void_p, C.c_void_p, C.c_double]),
@@ -108,7 +112,11 @@ SIGNATURES = {
     "msc_incident": (C.c_int, [C.c_void_p, C.c_double, C.c_void_p, C.c_int, C.c_void_p]),
     "msc_matvec": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int]),
     "msc_matvec_noalloc": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int]),
+    "msc_matvec_soa": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int]),
     "msc_solve": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(SolveOpts), C.POINTER(SolveStats)]),
+    "msc_solve_multi": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.POINTER(SolveOpts),
+                                  C.POINTER(SolveStats)]),
+    "msc_matvec_multi": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_int]),
     "msc_set_nearfield": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]),
     "msc_batch_solve": (C.c_int, [C.POINTER(BatchItem), C.c_int, C.POINTER(SolveOpts), C.c_int,
                                   C.POINTER(C.c_int)]),

@@ -152,6 +152,15 @@ static int nice_length(int n) {
   }
 }
 
+int read_status(msc_plan* pl, int* word) {
+  *word = 0;
+  if (!pl->status.p) return MSC_OK;
+  MSC_CUDA(cudaMemcpyAsync(word, pl->status.p, sizeof(int), cudaMemcpyDeviceToHost, pl->stream));
+  MSC_CUDA(cudaStreamSynchronize(pl->stream));
+  if (*word) MSC_CUDA(cudaMemsetAsync(pl->status.p, 0, sizeof(int), pl->stream));
+  return MSC_OK;
+}
+
 }  // namespace msc
 
 using namespace msc;
@@ -169,6 +178,7 @@ const char* msc_status_string(int s) {
     case MSC_ERR_NOMEM: return "MSC_ERR_NOMEM";
     case MSC_ERR_STATE: return "MSC_ERR_STATE";
     case MSC_ERR_NONFINITE: return "MSC_ERR_NONFINITE";
+    case MSC_ERR_TIMEOUT: return "MSC_ERR_TIMEOUT";
     default: return "MSC_UNKNOWN";
   }
 }
@@ -279,7 +289,7 @@ int msc_plan_destroy(msc_plan* pl) {
     pl->nf = nullptr;
   }
   DBuf* bufs[] = {&pl->tw64_z, &pl->tw64_xy, &pl->tw32_z, &pl->tw32_xy, &pl->t4_64, &pl->t4_32, &pl->khat64,
-                  &pl->khat32, &pl->va_blocks, &pl->g0_scratch, &pl->W64, &pl->W32, &pl->f64a, &pl->f64b, &pl->f32a, &pl->f32b,
+                  &pl->khat32, &pl->va_blocks, &pl->g0_scratch, &pl->W64, &pl->W32, &pl->Wm64, &pl->Wm32, &pl->f64a, &pl->f64b, &pl->f32a, &pl->f32b,
                   &pl->red, &pl->status};
   for (DBuf* b : bufs) dfree(pl, *b);
   cudaStreamSynchronize(pl->stream);
@@ -306,6 +316,25 @@ int msc_plan_fft_sizes(const msc_plan* pl, int32_t* o) {
 }
 
 int64_t msc_plan_device_bytes(const msc_plan* pl) { return pl ? pl->bytes : 0; }
+
+int msc_plan_set_wait_limit(msc_plan* pl, int64_t polls, int inject) {
+  if (!pl) { set_error("null plan"); return MSC_ERR_INVALID; }
+  if (polls < 0) { set_error("the wait limit must be >= 0 (0 = default), got %lld", (long long)polls); return MSC_ERR_INVALID; }
+  if (inject != 0 && inject != 1) { set_error("inject must be 0 or 1, got %d", inject); return MSC_ERR_INVALID; }
+  pl->wait_limit = polls;
+  pl->inject_wait = inject;
+  ++pl->gen;  // captured solver graphs bind both as kernel parameters
+  return MSC_OK;
+}
+
+int msc_plan_status(msc_plan* pl, int32_t* word) {
+  StreamFence fence(pl);
+  if (!pl || !word) { set_error("null argument"); return MSC_ERR_INVALID; }
+  int w = 0;
+  MSC_TRY(read_status(pl, &w));
+  *word = w;
+  return MSC_OK;
+}
 
 int msc_build_t0(msc_plan* pl, const double* dlam, const double* dmu, const double* drho, double omega) {
   StreamFence fence(pl);
@@ -388,6 +417,16 @@ int msc_matvec(msc_plan* pl, const void* x, void* y, int precision) {
   return MSC_OK;
 }
 
+int msc_matvec_soa(msc_plan* pl, const void* x, void* y, int precision) {
+  StreamFence fence(pl);
+  if (!pl || !x || !y) { set_error("null argument"); return MSC_ERR_INVALID; }
+  if (x == y) { set_error("x and y may not alias"); return MSC_ERR_INVALID; }
+  if (precision == MSC_COMPLEX128) return launch_matvec<double>(pl, (const double2*)x, nullptr, (double2*)y, nullptr);
+  if (precision == MSC_COMPLEX64) return launch_matvec<float>(pl, (const float2*)x, nullptr, (float2*)y, nullptr);
+  set_error("precision must be 0 (complex64) or 1 (complex128)");
+  return MSC_ERR_INVALID;
+}
+
 int msc_set_nearfield(msc_plan* pl, int degree, const double* coef, const double* dblocks) {
   if (!pl) { set_error("null plan"); return MSC_ERR_INVALID; }
   if (degree < 1 || degree > NF_MAXL) { set_error("degree must be in [1, %d], got %d", NF_MAXL, degree); return MSC_ERR_INVALID; }
@@ -466,6 +505,41 @@ int msc_solve(msc_plan* pl, const void* b, void* x, const msc_solve_opts* o, msc
     return MSC_ERR_INVALID;
   }
   return solve(pl, (const double2*)b, (double2*)x, o, st);
+}
+
+int msc_solve_multi(msc_plan* pl, int nrhs, const void* b, void* x, const msc_solve_opts* o, msc_solve_stats* st) {
+  StreamFence fence(pl);
+  if (!pl || !b || !x || !o) { set_error("null argument"); return MSC_ERR_INVALID; }
+  if (nrhs < 1 || nrhs > MSC_MAX_RHS) { set_error("nrhs must be in [1, %d], got %d", MSC_MAX_RHS, nrhs); return MSC_ERR_INVALID; }
+  if (b == x) { set_error("b and x may not alias"); return MSC_ERR_INVALID; }
+  if (o->precision != MSC_SOLVE_MIXED && o->precision != MSC_SOLVE_FP64) {
+    set_error("precision must be mixed (0) or fp64 (1)");
+    return MSC_ERR_INVALID;
+  }
+  if (o->initial_guess != 0 && o->initial_guess != 1) {
+    set_error("initial_guess must be 0 (born) or 1 (zero)");
+    return MSC_ERR_INVALID;
+  }
+  return solve_multi(pl, nrhs, (const double2*)b, (double2*)x, o, st);
+}
+
+int msc_matvec_multi(msc_plan* pl, int nrhs, const void* x, void* y, int precision) {
+  StreamFence fence(pl);
+  if (!pl || !x || !y) { set_error("null argument"); return MSC_ERR_INVALID; }
+  if (nrhs < 1 || nrhs > MSC_MAX_RHS) { set_error("nrhs must be in [1, %d], got %d", MSC_MAX_RHS, nrhs); return MSC_ERR_INVALID; }
+  if (x == y) { set_error("x and y may not alias"); return MSC_ERR_INVALID; }
+  if (!pl->has_t0 || !pl->has_g0) { set_error("matvec needs build_t0 and build_g0 first"); return MSC_ERR_STATE; }
+  const Geo& g = pl->g;
+  if (precision == MSC_COMPLEX128) {
+    MSC_TRY(dalloc(pl, pl->Wm64, sizeof(double2) * ws_elems(g) * nrhs));
+    return launch_matvec_ws<double>(pl, (const double2*)x, nullptr, (double2*)y, (double2*)pl->Wm64.p, nullptr, nrhs);
+  }
+  if (precision == MSC_COMPLEX64) {
+    MSC_TRY(dalloc(pl, pl->Wm32, sizeof(float2) * ws_elems(g) * nrhs));
+    return launch_matvec_ws<float>(pl, (const float2*)x, nullptr, (float2*)y, (float2*)pl->Wm32.p, nullptr, nrhs);
+  }
+  set_error("precision must be 0 (complex64) or 1 (complex128)");
+  return MSC_ERR_INVALID;
 }
 
 int msc_rpp_periodic(msc_plan* pl, const void* psi, double omega, double p, int flags, double* out) {

@@ -56,6 +56,7 @@ struct GmresWork {
     cudaGraphExec_t exec = nullptr;
     int m = 0;
     bool cgs2 = false;
+    int nrhs = 1;  // right-hand sides of the matvec the graph holds
     uint64_t gen = 0;
     int warm = 0;  // cycles of this kind run uncaptured (kernel attributes set, buffers allocated)
   } graph[2][2];
@@ -594,10 +595,20 @@ static int resid_norm(msc_plan* pl, GmresWork* gw, const cx<T>* b, const cx<T>* 
   return MSC_OK;
 }
 
+// ||v||^2 of n elements into out (device, FP64, deterministic)
+static int norm2_n(msc_plan* pl, GmresWork* gw, const double2* v, size_t n, double* out) {
+  GState* st = (GState*)gw->state.p;
+  const int nb = std::min<long long>(NB, ceil_div((long long)n, NTH));
+  k_resid_norm<double><<<nb, NTH, 0, pl->stream>>>(v, nullptr, nullptr, n, (double2*)gw->part.p, &st->counter[2],
+                                                   (double2*)out); ::msc::note_launch();
+  MSC_CUDA(cudaGetLastError());
+  return MSC_OK;
+}
+
 static int ensure_work(msc_plan* pl, int m) {
   if (!pl->gw) pl->gw = new GmresWork();
   GmresWork* gw = pl->gw;
-  const size_t n = field_elems(pl->g);
+  const size_t n = field_elems(pl->g) * (size_t)pl->nrhs;
   if (gw->m >= m && gw->n == n) return MSC_OK;
   gw->m = std::max(m, gw->m);
   gw->n = n;
@@ -707,7 +718,7 @@ static int gmres_core(msc_plan* pl, int m, const cx<T>* rhs, cx<T>* x, bool x_ze
     // short-lived plan does not repay the capture and instantiation) when the budget
     // covers m steps, and replayed while the plan generation holds. Plans with graphs
     // off (the batch's) always run uncaptured.
-    const bool graph_ok = gr.exec && gr.m == m && gr.cgs2 == cgs2 && gr.gen == pl->gen;
+    const bool graph_ok = gr.exec && gr.m == m && gr.cgs2 == cgs2 && gr.nrhs == pl->nrhs && gr.gen == pl->gen;
     if (pl->graphs && (graph_ok || gr.warm >= 2) && used + m <= max_mv) {
       if (!graph_ok) {
         if (use_pc) MSC_TRY(nearfield_refresh(pl));
@@ -728,6 +739,7 @@ static int gmres_core(msc_plan* pl, int m, const cx<T>* rhs, cx<T>* x, bool x_ze
         MSC_CUDA(ie);
         gr.m = m;
         gr.cgs2 = cgs2;
+        gr.nrhs = pl->nrhs;
         gr.gen = pl->gen;
       }
       if (use_pc) MSC_TRY(nearfield_refresh(pl));  // new blocks (a new frequency) into the same buffers
@@ -805,53 +817,26 @@ static int gmres_core(msc_plan* pl, int m, const cx<T>* rhs, cx<T>* x, bool x_ze
   return MSC_OK;
 }
 
-int solve(msc_plan* pl, const double2* b_ref, double2* x_ref, const msc_solve_opts* o, msc_solve_stats* stats) {
-  if (!pl->has_t0 || !pl->has_g0) {
-    set_error("solve needs build_t0 and build_g0 first");
-    return MSC_ERR_STATE;
-  }
-  const int m = std::max(1, std::min(o->restart > 0 ? o->restart : 30, 32));
-  MSC_TRY(ensure_work(pl, m));
+// The FP64 or mixed-precision solve of A x = b on the plan's component-major vectors
+// (gw->n elements: pl->nrhs fields one after the other). x holds the initial guess on
+// entry and the solution on return; b has the FP64 norm bnorm; the target is the
+// relative residual tol. On return gw->r64 holds b - A x of the final x and s the
+// counters, the status and the relative residual.
+static int solve_core(msc_plan* pl, const double2* b, double2* x, double bnorm, double tol, const msc_solve_opts* o,
+                      msc_solve_stats& s) {
   GmresWork* gw = pl->gw;
   HessPtr h = hess_ptrs(gw);
   const size_t n = gw->n;
-  double2* x = (double2*)gw->x64.p;
+  const int m = std::max(1, std::min(o->restart > 0 ? o->restart : 30, 32));
   double2* r = (double2*)gw->r64.p;
   double2* ax = (double2*)gw->ax64.p;
-  double2* b = (double2*)pl->f64a.p;
-  MSC_TRY(dalloc(pl, pl->f64a, sizeof(double2) * n));
-  b = (double2*)pl->f64a.p;
-  MSC_TRY(launch_ref_to_soa<double, double>(pl, b_ref, b));
-  if (pl->bloch) {
-    // the solve runs in the demodulated frame; b arrives physical
-    MSC_TRY(bloch_modulate(pl, b, -1));
-  }
-  if (o->initial_guess == 0)
-    MSC_CUDA(cudaMemcpyAsync(x, b, sizeof(double2) * n, cudaMemcpyDeviceToDevice, pl->stream));
-  else
-    MSC_CUDA(cudaMemsetAsync(x, 0, sizeof(double2) * n, pl->stream));
-  // ||b||
   double* dn = &h.nrm[1].x;  // outer ||.||^2 (h.nrm[1].y is scratch of the reduction)
-  MSC_TRY(resid_norm<double>(pl, gw, b, nullptr, nullptr, dn));
-  double bn2 = 0;
-  MSC_CUDA(cudaMemcpyAsync(&bn2, dn, sizeof(double), cudaMemcpyDeviceToHost, pl->stream));
-  MSC_CUDA(cudaStreamSynchronize(pl->stream));
-  const double bnorm = std::sqrt(bn2);
-  msc_solve_stats s{};
   s.status = MSC_NOT_CONVERGED;
-  const double tol = o->tol > 0 ? o->tol : 1e-6;
   const int max_mv = o->max_iter > 0 ? o->max_iter : 500;
-  if (o->preconditioner < 0 || o->preconditioner > 1) {
-    set_error("unknown preconditioner %d", o->preconditioner);
-    return MSC_ERR_INVALID;
-  }
   const bool pc = o->preconditioner == MSC_PC_NEARFIELD;
-  if (pc && (!pl->nf || !pl->nf->ready)) {
-    set_error("the near-field preconditioner needs build_g0 first");
-    return MSC_ERR_STATE;
-  }
   if (bnorm == 0.0) {
     MSC_CUDA(cudaMemsetAsync(x, 0, sizeof(double2) * n, pl->stream));
+    MSC_CUDA(cudaMemsetAsync(r, 0, sizeof(double2) * n, pl->stream));
     s.status = MSC_OK;
     s.residual = 0.0;
   } else if (o->precision == MSC_SOLVE_FP64) {
@@ -911,7 +896,7 @@ int solve(msc_plan* pl, const double2* b_ref, double2* x_ref, const msc_solve_op
         s.status = MSC_ERR_NONFINITE;
         break;
       }
-      // x += ||r|| d
+      // x += ||r|| d (d = 0 when the inner solve made no step: x and r stay as they are)
       k_sqrt<<<1, 32, 0, pl->stream>>>(dn, dn); ::msc::note_launch();
       k_axpy_mixed<<<std::min<long long>(NB, ceil_div((long long)n, NTH)), NTH, 0, pl->stream>>>(x, d, n, dn); ::msc::note_launch();
       MSC_CUDA(cudaGetLastError());
@@ -921,20 +906,171 @@ int solve(msc_plan* pl, const double2* b_ref, double2* x_ref, const msc_solve_op
     s.n_outer = outer;
     s.residual = res;
   }
+  return MSC_OK;
+}
+
+static int check_solve_opts(msc_plan* pl, const msc_solve_opts* o) {
+  if (!pl->has_t0 || !pl->has_g0) {
+    set_error("solve needs build_t0 and build_g0 first");
+    return MSC_ERR_STATE;
+  }
+  if (o->preconditioner < 0 || o->preconditioner > 1) {
+    set_error("unknown preconditioner %d", o->preconditioner);
+    return MSC_ERR_INVALID;
+  }
+  if (o->preconditioner == MSC_PC_NEARFIELD && (!pl->nf || !pl->nf->ready)) {
+    set_error("the near-field preconditioner needs build_g0 first");
+    return MSC_ERR_STATE;
+  }
+  return MSC_OK;
+}
+
+// The plan's bounded-wait status after a solve: a timeout invalidates the result.
+static int solve_timeout_status(msc_plan* pl) {
+  int kerr = 0;
+  MSC_TRY(read_status(pl, &kerr));
+  if (kerr) {
+    set_error("a kernel's bounded wait on its asynchronous copies or tensor-core work ran out; the result is invalid");
+    return MSC_ERR_TIMEOUT;
+  }
+  return MSC_OK;
+}
+
+int solve(msc_plan* pl, const double2* b_ref, double2* x_ref, const msc_solve_opts* o, msc_solve_stats* stats) {
+  MSC_TRY(check_solve_opts(pl, o));
+  const int m = std::max(1, std::min(o->restart > 0 ? o->restart : 30, 32));
+  MSC_TRY(ensure_work(pl, m));
+  GmresWork* gw = pl->gw;
+  HessPtr h = hess_ptrs(gw);
+  const size_t n = gw->n;
+  double2* x = (double2*)gw->x64.p;
+  MSC_TRY(dalloc(pl, pl->f64a, sizeof(double2) * n));
+  double2* b = (double2*)pl->f64a.p;
+  MSC_TRY(launch_ref_to_soa<double, double>(pl, b_ref, b));
+  if (pl->bloch) {
+    // the solve runs in the demodulated frame; b arrives physical
+    MSC_TRY(bloch_modulate(pl, b, -1));
+  }
+  if (o->initial_guess == 0)
+    MSC_CUDA(cudaMemcpyAsync(x, b, sizeof(double2) * n, cudaMemcpyDeviceToDevice, pl->stream));
+  else
+    MSC_CUDA(cudaMemsetAsync(x, 0, sizeof(double2) * n, pl->stream));
+  // ||b||
+  double* dn = &h.nrm[1].x;
+  MSC_TRY(resid_norm<double>(pl, gw, b, nullptr, nullptr, dn));
+  double bn2 = 0;
+  MSC_CUDA(cudaMemcpyAsync(&bn2, dn, sizeof(double), cudaMemcpyDeviceToHost, pl->stream));
+  MSC_CUDA(cudaStreamSynchronize(pl->stream));
+  msc_solve_stats s{};
+  MSC_TRY(solve_core(pl, b, x, std::sqrt(bn2), o->tol > 0 ? o->tol : 1e-6, o, s));
   // x back to the caller's layout (and physical frame)
   if (pl->bloch) {
     MSC_TRY(bloch_modulate(pl, x, +1));
   }
   MSC_TRY(launch_soa_to_ref<double, double>(pl, x, x_ref));
-  int kerr = 0;
-  MSC_CUDA(cudaMemcpyAsync(&kerr, pl->status.p, sizeof(int), cudaMemcpyDeviceToHost, pl->stream));
-  MSC_CUDA(cudaStreamSynchronize(pl->stream));
-  if (kerr) {
-    set_error("a kernel's bounded wait for its asynchronous copies timed out");
-    return MSC_ERR_CUDA;
-  }
+  const int ts = solve_timeout_status(pl);
   if (stats) *stats = s;
+  if (ts != MSC_OK) return ts;
+  if (s.status == MSC_ERR_NONFINITE)
+    set_error("the solve met a non-finite (NaN or Inf) residual: check the contrasts, T0 and the frequency");
   return s.status;
+}
+
+// Scales the field v (n elements) by f on the device.
+__global__ void k_scale_field(double2* __restrict__ v, size_t n, double f) {
+  for (size_t k = (size_t)blockIdx.x * NTH + threadIdx.x; k < n; k += (size_t)gridDim.x * NTH) {
+    v[k].x *= f;
+    v[k].y *= f;
+  }
+}
+
+// Sets the plan's right-hand-side count for the duration of a multi-RHS solve (a
+// captured solver graph records the count it was captured with and serves only that).
+struct NrhsScope {
+  msc_plan* pl;
+  NrhsScope(msc_plan* p, int r) : pl(p) { pl->nrhs = r; }
+  ~NrhsScope() { pl->nrhs = 1; }
+};
+
+int solve_multi(msc_plan* pl, int R, const double2* b_ref, double2* x_ref, const msc_solve_opts* o,
+                msc_solve_stats* stats) {
+  MSC_TRY(check_solve_opts(pl, o));
+  const Geo& g = pl->g;
+  const size_t nf = field_elems(g);
+  // workspaces of R right-hand sides, kept by the plan for its next multi-RHS solve
+  MSC_TRY(dalloc(pl, pl->Wm64, sizeof(double2) * ws_elems(g) * R));
+  MSC_TRY(dalloc(pl, pl->Wm32, sizeof(float2) * ws_elems(g) * R));
+  NrhsScope scope(pl, R);
+  const int m = std::max(1, std::min(o->restart > 0 ? o->restart : 30, 32));
+  MSC_TRY(ensure_work(pl, m));
+  GmresWork* gw = pl->gw;
+  HessPtr h = hess_ptrs(gw);
+  const size_t n = gw->n;  // R nf
+  double2* x = (double2*)gw->x64.p;
+  MSC_TRY(dalloc(pl, pl->f64a, sizeof(double2) * n));
+  double2* b = (double2*)pl->f64a.p;
+  const int nbk = (int)std::min<long long>(NB, ceil_div((long long)nf, NTH));
+  double* dn = &h.nrm[1].x;
+  // each right-hand side in the solver's layout (and frame), scaled to unit norm
+  std::vector<double> bn(R, 0.0);
+  for (int r = 0; r < R; ++r) {
+    double2* br = b + (size_t)r * nf;
+    MSC_TRY(launch_ref_to_soa<double, double>(pl, b_ref + (size_t)r * nf, br));
+    if (pl->bloch) MSC_TRY(bloch_modulate(pl, br, -1));
+    MSC_TRY(norm2_n(pl, gw, br, nf, dn));
+    double v = 0;
+    MSC_CUDA(cudaMemcpyAsync(&v, dn, sizeof(double), cudaMemcpyDeviceToHost, pl->stream));
+    MSC_CUDA(cudaStreamSynchronize(pl->stream));
+    bn[r] = std::sqrt(v);
+    if (bn[r] > 0) {
+      k_scale_field<<<nbk, NTH, 0, pl->stream>>>(br, nf, 1.0 / bn[r]);
+      ::msc::note_launch();
+    }
+  }
+  int nz = 0;
+  for (int r = 0; r < R; ++r) nz += bn[r] > 0 ? 1 : 0;
+  if (o->initial_guess == 0)
+    MSC_CUDA(cudaMemcpyAsync(x, b, sizeof(double2) * n, cudaMemcpyDeviceToDevice, pl->stream));
+  else
+    MSC_CUDA(cudaMemsetAsync(x, 0, sizeof(double2) * n, pl->stream));
+  // One Krylov space of the stacked system: every right-hand side has unit norm, so a
+  // stacked relative residual of tol / sqrt(R) bounds each one's by tol.
+  const double tol = o->tol > 0 ? o->tol : 1e-6;
+  msc_solve_stats s{};
+  MSC_TRY(solve_core(pl, b, x, std::sqrt((double)nz), tol / std::sqrt((double)std::max(1, nz)), o, s));
+  // per right-hand side: the FP64 residual of the final x (gw->r64 = b - A x), the
+  // field unscaled, back to the caller's frame and layout
+  const double2* res = (const double2*)gw->r64.p;
+  std::vector<double> rr(R, 0.0);
+  for (int r = 0; r < R; ++r) {
+    MSC_TRY(norm2_n(pl, gw, res + (size_t)r * nf, nf, dn));
+    double v = 0;
+    MSC_CUDA(cudaMemcpyAsync(&v, dn, sizeof(double), cudaMemcpyDeviceToHost, pl->stream));
+    MSC_CUDA(cudaStreamSynchronize(pl->stream));
+    rr[r] = bn[r] > 0 ? std::sqrt(v) : 0.0;
+    double2* xr = x + (size_t)r * nf;
+    k_scale_field<<<nbk, NTH, 0, pl->stream>>>(xr, nf, bn[r]);
+    ::msc::note_launch();
+    if (pl->bloch) MSC_TRY(bloch_modulate(pl, xr, +1));
+    MSC_TRY(launch_soa_to_ref<double, double>(pl, xr, x_ref + (size_t)r * nf));
+  }
+  MSC_CUDA(cudaGetLastError());
+  const int ts = solve_timeout_status(pl);
+  int worst = MSC_OK;
+  for (int r = 0; r < R; ++r) {
+    msc_solve_stats sr = s;
+    sr.residual = rr[r];
+    if (s.status == MSC_ERR_NONFINITE || !(rr[r] == rr[r]))
+      sr.status = MSC_ERR_NONFINITE;
+    else
+      sr.status = rr[r] <= tol ? MSC_OK : MSC_NOT_CONVERGED;
+    if (stats) stats[r] = sr;
+    if (sr.status < 0 || (worst >= 0 && sr.status > worst)) worst = sr.status;
+  }
+  if (ts != MSC_OK) return ts;
+  if (worst == MSC_ERR_NONFINITE)
+    set_error("the solve met a non-finite (NaN or Inf) residual: check the contrasts, T0 and the frequency");
+  return worst;
 }
 
 }  // namespace msc

@@ -133,15 +133,16 @@ int launch_fft_contig(msc_plan* pl, const cx<T>* in, cx<T>* out, long long nline
                       long long stride, int n_in, int n_out, const FftPlan1D& f, const cx<T>* tw, int dir,
                       const int* done);
 template <typename T>
-int launch_t0_fft_y(msc_plan* pl, const cx<T>* x, const double* scale, cx<T>* W, const cx<T>* tw, const int* done);
+int launch_t0_fft_y(msc_plan* pl, const cx<T>* x, const double* scale, cx<T>* W, const cx<T>* tw, const int* done,
+                    int nrhs);
 template <typename T>
 int launch_fft_strided(msc_plan* pl, const cx<T>* in, long long es, long long S1, long long S2, cx<T>* out,
                        long long eo, long long O1, long long O2, float2* out32, int ncol, int n1, int n2, int n_in,
                        int n_out, const FftPlan1D& f, const cx<T>* tw, int dir, const int* done);
 template <typename T>
-int launch_zbz(msc_plan* pl, cx<T>* W, const int* done);
+int launch_zbz(msc_plan* pl, cx<T>* W, const int* done, int nrhs);
 template <typename T>
 int launch_fft_y_out(msc_plan* pl, const cx<T>* W, const cx<T>* x, const double* scale, cx<T>* y, const cx<T>* tw,
-                     const int* done);
+                     const int* done, int nrhs);
 
 }  // namespace msc

@@ -80,6 +80,9 @@ __global__ void __launch_bounds__(PlaneCfg<L>::NT) k_plane_fwd(const float2* __r
   float2* tb = reinterpret_cast<float2*>(smem_raw);  // [LINES][LS] transpose slots
   float2* T = tb + LINES * LS;                        // [L][TP]: [ky][x], x < L/2
   const int n = blockIdx.x, c = blockIdx.y;
+  // blockIdx.z: the right-hand side (fields and workspaces follow each other)
+  x += (size_t)blockIdx.z * 9 * g.nsite;
+  W += (size_t)blockIdx.z * 9 * g.Nz * L * L;
   const int q = threadIdx.x / 8, t = threadIdx.x % 8;
   const float s = scale ? (float)(*scale) : 1.f;
   float2* ls = tb + q * LS;
@@ -137,6 +140,10 @@ __global__ void __launch_bounds__(PlaneCfg<L>::NT) k_plane_inv(const float2* __r
   float2* tb = reinterpret_cast<float2*>(smem_raw);
   float2* T = tb + LINES * LS;  // [ky][x], x < L/2
   const int n = blockIdx.x, c = blockIdx.y;
+  // blockIdx.z: the right-hand side
+  W += (size_t)blockIdx.z * 9 * g.Nz * L * L;
+  x += (size_t)blockIdx.z * 9 * g.nsite;
+  y += (size_t)blockIdx.z * 9 * g.nsite;
   const int q = threadIdx.x / 8, t = threadIdx.x % 8;
   float2* ls = tb + q * LS;
   const float2* Wp = W + (size_t)(c * g.Nz + n) * L * L;
@@ -183,7 +190,7 @@ bool plane_fused_ok(const msc_plan* pl) {
   return !pl->desc.periodic && g.Lx == g.Ly && (g.Lx == 64 || g.Lx == 128) && 2 * g.M <= g.Lx;
 }
 
-int launch_plane_fwd(msc_plan* pl, const float2* x, const double* scale, float2* W, const int* done) {
+int launch_plane_fwd(msc_plan* pl, const float2* x, const double* scale, float2* W, const int* done, int nrhs) {
   const Geo& g = pl->g;
   const float2* t4 = (const float2*)pl->t4_32.p;
   const float2* tw = (const float2*)pl->tw32_xy.p;
@@ -193,13 +200,13 @@ int launch_plane_fwd(msc_plan* pl, const float2* x, const double* scale, float2*
   MSC_CUDA(prep_kernel(kern));
   Geo gg = g;
   void* args[] = {(void*)&x, (void*)&scale, (void*)&t4, (void*)&W, (void*)&gg, (void*)&tw, (void*)&done};
-  MSC_CUDA(launch_pdl(kern, dim3((unsigned)g.Nz, 9), dim3(nt), args, sm, pl->stream));
+  MSC_CUDA(launch_pdl(kern, dim3((unsigned)g.Nz, 9, (unsigned)nrhs), dim3(nt), args, sm, pl->stream));
   ::msc::note_launch();
   return MSC_OK;
 }
 
 int launch_plane_inv(msc_plan* pl, const float2* W, const float2* x, const double* scale, float2* y,
-                     const int* done) {
+                     const int* done, int nrhs) {
   const Geo& g = pl->g;
   const float2* tw = (const float2*)pl->tw32_xy.p;
   const void* kern = g.Lx == 64 ? (const void*)k_plane_inv<64> : (const void*)k_plane_inv<128>;
@@ -208,7 +215,7 @@ int launch_plane_inv(msc_plan* pl, const float2* W, const float2* x, const doubl
   MSC_CUDA(prep_kernel(kern));
   Geo gg = g;
   void* args[] = {(void*)&W, (void*)&x, (void*)&scale, (void*)&y, (void*)&gg, (void*)&tw, (void*)&done};
-  MSC_CUDA(launch_pdl(kern, dim3((unsigned)g.Nz, 9), dim3(nt), args, sm, pl->stream));
+  MSC_CUDA(launch_pdl(kern, dim3((unsigned)g.Nz, 9, (unsigned)nrhs), dim3(nt), args, sm, pl->stream));
   ::msc::note_launch();
   return MSC_OK;
 }

@@ -35,7 +35,14 @@ __global__ void __launch_bounds__(256, 4) k_t0_fft_y(const cx<T>* __restrict__ x
   C* ta = tw + Ly;
   C* tb = ta + (size_t)Ly * P;
   const int tid = threadIdx.x;
-  const int c = blockIdx.z, n = blockIdx.y, i0 = blockIdx.x * TR;
+  // blockIdx.z = 9 rh + c: component c of right-hand side rh (fields and workspaces
+  // of the right-hand sides follow each other)
+  const int c = blockIdx.z % 9, n = blockIdx.y, i0 = blockIdx.x * TR;
+  {
+    const size_t rh = blockIdx.z / 9;
+    x += rh * 9 * (size_t)g.nsite;
+    W += rh * 9 * (size_t)g.Nz * g.Ly * g.Lx;
+  }
   const int nr = min(TR, g.M - i0);
   const T s = load_scale<T>(scale);
   for (int t = tid; t < Ly; t += NT) tw[t] = twg[t];
@@ -76,13 +83,14 @@ __global__ void __launch_bounds__(256, 4) k_t0_fft_y(const cx<T>* __restrict__ x
 }
 
 template <typename T>
-int launch_t0_fft_y(msc_plan* pl, const cx<T>* x, const double* scale, cx<T>* W, const cx<T>* tw, const int* done) {
+int launch_t0_fft_y(msc_plan* pl, const cx<T>* x, const double* scale, cx<T>* W, const cx<T>* tw, const int* done,
+                    int nrhs) {
   const Geo& g = pl->g;
   constexpr int TR = Tile<T>::W;
   const cx<T>* t4 = (const cx<T>*)(sizeof(T) == 8 ? pl->t4_64.p : pl->t4_32.p);
   const int nthr = 256;
   const size_t sm = sizeof(cx<T>) * ((size_t)g.Ly + 2 * (size_t)g.Ly * (TR + 1));
-  dim3 grid((unsigned)((g.M + TR - 1) / TR), (unsigned)g.Nz, 9);
+  dim3 grid((unsigned)((g.M + TR - 1) / TR), (unsigned)g.Nz, 9u * (unsigned)nrhs);
   const void* kern;
   const bool pr = 2 * g.M <= g.Ly;
 #define LEN(LL) kern = pr ? (const void*)k_t0_fft_y<T, true, LL, true> : (const void*)k_t0_fft_y<T, true, LL, false>;
@@ -104,7 +112,8 @@ int launch_t0_fft_y(msc_plan* pl, const cx<T>* x, const double* scale, cx<T>* W,
   ::msc::note_launch();
   return MSC_OK;
 }
-template int launch_t0_fft_y<float>(msc_plan*, const float2*, const double*, float2*, const float2*, const int*);
-template int launch_t0_fft_y<double>(msc_plan*, const double2*, const double*, double2*, const double2*, const int*);
+template int launch_t0_fft_y<float>(msc_plan*, const float2*, const double*, float2*, const float2*, const int*, int);
+template int launch_t0_fft_y<double>(msc_plan*, const double2*, const double*, double2*, const double2*, const int*,
+                                     int);
 
 }  // namespace msc

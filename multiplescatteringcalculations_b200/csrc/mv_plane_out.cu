@@ -24,7 +24,14 @@ __global__ void __launch_bounds__(256, 4) k_fft_y_out(const cx<T>* __restrict__ 
   C* ta = tw + Ly;
   C* tb = ta + (size_t)Ly * P;
   const int tid = threadIdx.x;
-  const int c = blockIdx.z, m = blockIdx.y, x0 = blockIdx.x * TR;
+  // blockIdx.z = 9 rh + c: component c of right-hand side rh
+  const int c = blockIdx.z % 9, m = blockIdx.y, x0 = blockIdx.x * TR;
+  {
+    const size_t rh = blockIdx.z / 9;
+    W += rh * 9 * (size_t)g.Nz * g.Ly * g.Lx;
+    x += rh * 9 * (size_t)g.nsite;
+    y += rh * 9 * (size_t)g.nsite;
+  }
   const int nr = min(TR, g.M - x0);
   for (int t = tid; t < Ly; t += NT) tw[t] = twg[t];
   const C* Wl = W + ((size_t)(c * g.Nz + m) * g.Ly) * g.Lx + x0;
@@ -59,12 +66,12 @@ __global__ void __launch_bounds__(256, 4) k_fft_y_out(const cx<T>* __restrict__ 
 
 template <typename T>
 int launch_fft_y_out(msc_plan* pl, const cx<T>* W, const cx<T>* x, const double* scale, cx<T>* y, const cx<T>* tw,
-                     const int* done) {
+                     const int* done, int nrhs) {
   const Geo& g = pl->g;
   constexpr int TR = Tile<T>::W;
   const int nthr = 256;
   const size_t sm = sizeof(cx<T>) * ((size_t)g.Ly + 2 * (size_t)g.Ly * (TR + 1));
-  dim3 grid((unsigned)((g.M + TR - 1) / TR), (unsigned)g.Nz, 9);
+  dim3 grid((unsigned)((g.M + TR - 1) / TR), (unsigned)g.Nz, 9u * (unsigned)nrhs);
   const void* kern;
   const bool pr = 2 * g.M <= g.Ly;
 #define LEN(LL) kern = pr ? (const void*)k_fft_y_out<T, true, LL, true> : (const void*)k_fft_y_out<T, true, LL, false>;
@@ -87,8 +94,8 @@ int launch_fft_y_out(msc_plan* pl, const cx<T>* W, const cx<T>* x, const double*
   return MSC_OK;
 }
 template int launch_fft_y_out<float>(msc_plan*, const float2*, const float2*, const double*, float2*, const float2*,
-                                     const int*);
+                                     const int*, int);
 template int launch_fft_y_out<double>(msc_plan*, const double2*, const double2*, const double*, double2*,
-                                      const double2*, const int*);
+                                      const double2*, const int*, int);
 
 }  // namespace msc

@@ -2,5 +2,5 @@
 #include "mv_zbz.cuh"
 
 namespace msc {
-template int launch_zbz<float>(msc_plan*, float2*, const int*);
+template int launch_zbz<float>(msc_plan*, float2*, const int*, int);
 }  // namespace msc

@@ -110,10 +110,13 @@ template <bool SYM, typename LD> __device__ __forceinline__ void block_mul(LD ld
 // KX = KXC; LC = 0: both from the plan and the layout at run time. The block size is a multiple of NL and of
 // 8 KX, so a thread keeps one line in the load and store loops and one slot in
 // the multiply.
+//
+// nrhs > 1: the block applies its slice of the spectrum (staged once) to the same
+// columns of nrhs vectors in turn, vector r's workspace at W + r * 9 N_z Ly Lx.
 template <typename T, int LC, int KXC, bool SYM, bool OCT, bool POW2>
 __global__ void __launch_bounds__(ZBZ_THREADS, 2) k_zbz(cx<T>* __restrict__ W, const kent<T>* __restrict__ khat, Geo g,
                                                         ZbzLayout lay, FftPlan1D pl, const cx<T>* __restrict__ twg,
-                                                        const int* done) {
+                                                        const int* done, int nrhs) {
   pdl_wait();
   pdl_trigger();
   if (done && *done) return;
@@ -168,7 +171,9 @@ __global__ void __launch_bounds__(ZBZ_THREADS, 2) k_zbz(cx<T>* __restrict__ W, c
   __syncthreads();
   // this thread's line and rows kz = r0, r0 + RS, ...
   const int line = tid % NL, r0 = tid / NL, RS = NT / NL;
-  const long long o = loff[line];
+  const long long o0 = loff[line];
+  for (int rh = 0; rh < nrhs; ++rh) {
+  const long long o = o0 >= 0 ? o0 + (long long)rh * 9 * cstride : -1;
   {
     // compile time: only rows kz < Lz/2 are read by the pruned first FFT stage (N_z <= Lz/2)
     const int nrow = (CT && (LC / 2) % (NT / (36 * (CT ? KXC : 1))) == 0) ? (LC / 2) / (NT / (36 * (CT ? KXC : 1)))
@@ -246,6 +251,9 @@ __global__ void __launch_bounds__(ZBZ_THREADS, 2) k_zbz(cx<T>* __restrict__ W, c
       W[o + kz * plane] = out[kz * P + line];
     }
   }
+  // the next vector's gather writes the tiles this vector's store reads
+  if (rh + 1 < nrhs) __syncthreads();
+  }
 }
 
 // Register-resident variant for short power-of-two Lz (octant spectrum): one thread
@@ -257,10 +265,13 @@ __global__ void __launch_bounds__(ZBZ_THREADS, 2) k_zbz(cx<T>* __restrict__ W, c
 // multiple of 8 KX, as the multiply's item walk needs).
 template <int KX> constexpr int zbz_reg_threads() { return ((36 * KX + 31) / 32) * 32; }
 
+//
+// nrhs > 1: as in k_zbz, the staged slice serves the same columns of nrhs vectors in
+// turn.
 template <typename T, int LC, int KXC, bool SYM>
 __global__ void __launch_bounds__(zbz_reg_threads<KXC>(), 3)
     k_zbz_reg(cx<T>* __restrict__ W, const kent<T>* __restrict__ khat, Geo g, ZbzLayout lay,
-              const cx<T>* __restrict__ twg, const int* done) {
+              const cx<T>* __restrict__ twg, const int* done, int nrhs) {
   pdl_wait();
   pdl_trigger();
   if (done && *done) return;
@@ -303,7 +314,9 @@ __global__ void __launch_bounds__(zbz_reg_threads<KXC>(), 3)
   for (int t = tid; t < Lz; t += NT) tw[t] = twg[t];
   __syncthreads();
   const int line = tid;
-  const long long o = line < NL ? loff[line] : -1;
+  const long long o0 = line < NL ? loff[line] : -1;
+  for (int rh = 0; rh < nrhs; ++rh) {
+  const long long o = o0 >= 0 ? o0 + (long long)rh * 9 * cstride : -1;
   C v[Lz];
   if (line < NL) {
     // N_z <= Lz/2: only the first half of the line holds data
@@ -354,13 +367,16 @@ __global__ void __launch_bounds__(zbz_reg_threads<KXC>(), 3)
     for (int n = 0; n < Lz / 2; ++n)
       if (n < g.Nz) W[o + n * plane] = v[n];
   }
+  // a thread writes and reads back only its own line of the tile outside the multiply,
+  // which the barriers around it separate: the next vector needs no barrier here
+  }
 }
 
 // Compile-time KX of a power-of-two Lz (the layout's choice for an octant spectrum).
 template <typename T> constexpr int zbz_kx_ct(int L, int E) { return zbz_layout<T>(L, L / 2 + 1, 1, E, true).KX; }
 
 template <typename T>
-int launch_zbz(msc_plan* pl, cx<T>* W, const int* done) {
+int launch_zbz(msc_plan* pl, cx<T>* W, const int* done, int nrhs) {
   const Geo& g = pl->g;
   const kent<T>* kh = (const kent<T>*)(sizeof(T) == 8 ? pl->khat64.p : pl->khat32.p);
   const cx<T>* tw = (const cx<T>*)(sizeof(T) == 8 ? pl->tw64_z.p : pl->tw32_z.p);
@@ -411,7 +427,7 @@ int launch_zbz(msc_plan* pl, cx<T>* W, const int* done) {
         MSC_CUDA(prep_kernel(rk));
         Geo gg = g;
         ZbzLayout ll = lay;
-        void* args[] = {(void*)&W, (void*)&kh, (void*)&gg, (void*)&ll, (void*)&tw, (void*)&done};
+        void* args[] = {(void*)&W, (void*)&kh, (void*)&gg, (void*)&ll, (void*)&tw, (void*)&done, (void*)&nrhs};
         MSC_CUDA(launch_pdl(rk, grid, dim3(nt), args, sm, pl->stream));
         ::msc::note_launch();
         return MSC_OK;
@@ -429,7 +445,8 @@ int launch_zbz(msc_plan* pl, cx<T>* W, const int* done) {
   Geo gg = g;
   ZbzLayout ll = lay;
   FftPlan1D ff = pl->fz;
-  void* args[] = {(void*)&W, (void*)&kh, (void*)&gg, (void*)&ll, (void*)&ff, (void*)&tw, (void*)&done};
+  void* args[] = {(void*)&W, (void*)&kh, (void*)&gg, (void*)&ll, (void*)&ff, (void*)&tw, (void*)&done,
+                  (void*)&nrhs};
   MSC_CUDA(launch_pdl(kern, grid, dim3(ZBZ_THREADS), args, lay.smem, pl->stream));
   ::msc::note_launch();
   return MSC_OK;

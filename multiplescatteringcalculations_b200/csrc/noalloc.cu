@@ -28,7 +28,9 @@ constexpr size_t NOALLOC_SCRATCH_BYTES = size_t(64) << 20;  // 64 MiB
 static __device__ __align__(256) unsigned char g_noalloc_scratch[NOALLOC_SCRATCH_BYTES];
 
 // Device address of the array per device, looked up on the first call on that
-// device (with that device current).
+// device (with that device current) and kept for the life of the process. A
+// cudaDeviceReset destroys the array's allocation together with every plan of that
+// device, so the library does not support being used across a device reset.
 static int scratch_address(int dev, void** out) {
   static std::mutex mu;
   static void* addr[128] = {nullptr};
@@ -100,6 +102,13 @@ extern "C" int msc_matvec_noalloc(msc_plan* pl, const void* x, void* y, int prec
   }
   int dev = 0;
   MSC_CUDA(cudaGetDevice(&dev));
+  if (dev != pl->device) {
+    // the array's address is per device: another device's copy would be read by
+    // kernels launched on this plan's stream
+    set_error("msc_matvec_noalloc: the current device is %d but the plan lives on device %d; make the plan's "
+              "device current first", dev, pl->device);
+    return MSC_ERR_INVALID;
+  }
   void* base = nullptr;
   MSC_TRY(scratch_address(dev, &base));
   unsigned char* s = static_cast<unsigned char*>(base);

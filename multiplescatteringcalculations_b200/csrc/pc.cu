@@ -247,7 +247,7 @@ int nearfield_refresh(msc_plan* pl) {
 }
 
 template <typename T>
-int nearfield_apply(msc_plan* pl, const cx<T>* v, const double* scale, cx<T>* z, const int* done) {
+static int nearfield_apply_one(msc_plan* pl, const cx<T>* v, const double* scale, cx<T>* z, const int* done) {
   NearField* nf = pl->nf;
   if (!nf || !nf->ready) {
     set_error("the near-field preconditioner needs build_g0 first");
@@ -303,6 +303,15 @@ int nearfield_apply(msc_plan* pl, const cx<T>* v, const double* scale, cx<T>* z,
     in = h;
     sc = nullptr;
   }
+  return MSC_OK;
+}
+
+// z = P v for each of the plan's pl->nrhs fields (one after the other)
+template <typename T>
+int nearfield_apply(msc_plan* pl, const cx<T>* v, const double* scale, cx<T>* z, const int* done) {
+  const size_t nf = field_elems(pl->g);
+  for (int r = 0; r < pl->nrhs; ++r)
+    MSC_TRY(nearfield_apply_one<T>(pl, v + (size_t)r * nf, scale, z + (size_t)r * nf, done));
   return MSC_OK;
 }
 

@@ -31,9 +31,11 @@
 // 9 DOFs) and write h = y and acc = c0 s x + ch y or acc += ch y; then they stage plane
 // j + 2 into the slot the MMAs of layer j - 1 released.
 //
-// Every wait on an mbarrier is bounded: when one runs out the kernel records a timeout in
-// the plan's status word and sets the block's abort flag, after which no warp issues or
-// waits for further work, and the tensor memory is freed.
+// Every wait on an mbarrier is bounded (the plan's wait limit, msc_plan_set_wait_limit):
+// when one runs out the kernel records a timeout in the plan's status word and sets the
+// block's abort flag, after which no warp issues or waits for further work; the MMA warp
+// then drains the weights' bulk copy and its last commits (with the fixed limit) before
+// the tensor memory is freed and the block exits.
 #include <cuda_bf16.h>
 
 #include <algorithm>
@@ -64,6 +66,8 @@ static_assert(TV_B_BYTES == NF_TC_LAYER_BYTES, "packed layer size");
 static_assert(TV_M == 128, "one accumulator lane per voxel row");
 constexpr int TV_ALIGN = 1024;                // operand base alignment in the shared window
 constexpr int TV_T8_BYTES = TV_RING * TV_PROWS * 8;
+// + 64: mbarriers done[2], weights, staged[2] (40 bytes), the tensor-memory address and
+// the abort flag (8 bytes), the never-completed mbarrier (8 bytes)
 constexpr size_t TV_SMEM = TV_ALIGN + (size_t)TV_B_BYTES + (size_t)TV_RING * TV_PLANE + TV_T8_BYTES + 64;
 constexpr long long TV_WAIT_LIMIT = 1ll << 22;  // mbarrier polls before a timeout is recorded
 
@@ -100,15 +104,25 @@ __device__ __forceinline__ bool mbar_try_wait(uint32_t addr, uint32_t phase) {
   return ok != 0;
 }
 
-// bounded wait; on a timeout the status word is set and the wait is tried once more
-__device__ __forceinline__ bool mbar_wait_bounded(uint32_t addr, uint32_t phase, int* status) {
+// bounded wait of the pipeline (`limit` polls, the plan's setting); on a timeout the
+// status word is set and the wait is tried once more
+__device__ __forceinline__ bool mbar_wait_bounded(uint32_t addr, uint32_t phase, int* status, long long limit) {
   bool ok = false;
-  for (long long it = 0; it < TV_WAIT_LIMIT && !ok; ++it) ok = mbar_try_wait(addr, phase);
+  for (long long it = 0; it < limit && !ok; ++it) ok = mbar_try_wait(addr, phase);
   if (!ok) {
     if (status) atomicExch(status, 1);
-    for (long long it = 0; it < TV_WAIT_LIMIT && !ok; ++it) ok = mbar_try_wait(addr, phase);
+    for (long long it = 0; it < limit && !ok; ++it) ok = mbar_try_wait(addr, phase);
   }
   return ok;
+}
+
+// the drain before the block releases its tensor memory and exits: wait, with the fixed
+// limit TV_WAIT_LIMIT whatever the pipeline's limit, for an asynchronous operation of this
+// block (the weights' bulk copy, the MMAs of a commit) to complete
+__device__ __forceinline__ void mbar_drain(uint32_t addr, uint32_t phase, int* status) {
+  bool ok = false;
+  for (long long it = 0; it < TV_WAIT_LIMIT && !ok; ++it) ok = mbar_try_wait(addr, phase);
+  if (!ok && status) atomicExch(status, 1);
 }
 
 struct TvTile {
@@ -210,7 +224,7 @@ __device__ __forceinline__ void mbar_arrive(uint32_t addr) {
 __global__ void __launch_bounds__(TV_THREADS, 2)
     k_nf_tc(const float2* __restrict__ x, const double* scale, const float2* __restrict__ t4, float2* __restrict__ h,
             float2* __restrict__ acc, float2 ch, float2 c0, int init, const uint4* __restrict__ Bg, Geo g, int zc,
-            const int* done, int* status) {
+            const int* done, int* status, long long wait_limit, int inject_wait) {
   pdl_wait();
   pdl_trigger();
   if (done && *done) return;
@@ -226,6 +240,9 @@ __global__ void __launch_bounds__(TV_THREADS, 2)
   uint64_t* mbar = reinterpret_cast<uint64_t*>(ring + TV_RING * TV_PLANE + TV_T8_BYTES);
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(mbar + 5);
   volatile int* abort_flag = reinterpret_cast<volatile int*>(mbar + 5) + 1;
+  // an mbarrier that nothing arrives at: the wait on it that inject_wait asks for runs
+  // out (the plan's failure-path test)
+  const uint32_t mb_never = (uint32_t)__cvta_generic_to_shared(mbar + 6);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const uint32_t mb = (uint32_t)__cvta_generic_to_shared(mbar);
   const uint32_t mb_done = mb, mb_w = mb + 16u, mb_staged = mb + 24u;
@@ -235,6 +252,7 @@ __global__ void __launch_bounds__(TV_THREADS, 2)
     asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(mb_w) : "memory");
     asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(mb_staged), "n"(TV_STAGE) : "memory");
     asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(mb_staged + 8u), "n"(TV_STAGE) : "memory");
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(mb_never) : "memory");
     *abort_flag = 0;
     asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
   }
@@ -293,12 +311,15 @@ __global__ void __launch_bounds__(TV_THREADS, 2)
   const uint32_t tmem = *tmem_slot;
   if (warp == 8) {
     if (lane == 0) {
-      bool ok = mbar_wait_bounded(mb_w, 0u, status);  // the weights have landed
+      bool ok = mbar_wait_bounded(mb_w, 0u, status, wait_limit);  // the weights have landed
+      if (ok && inject_wait) ok = mbar_wait_bounded(mb_never, 0u, status, wait_limit);
       const uint64_t dB = umma_desc(b_a, TV_LBO_B, 128);
+      int issued = 0;
       for (int j = 0; j < tl.zc && ok && !*abort_flag; ++j) {
         // plane j + 1 staged and accumulator j & 1 drained: the staging warps' pass j - 1
         if (j >= 1)
-          ok = mbar_wait_bounded(mb_staged + (uint32_t)(((j - 1) & 1) * 8), (uint32_t)(((j - 1) >> 1) & 1), status);
+          ok = mbar_wait_bounded(mb_staged + (uint32_t)(((j - 1) & 1) * 8), (uint32_t)(((j - 1) >> 1) & 1), status,
+                                 wait_limit);
         if (!ok) break;
         asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
         uint64_t dA[3];
@@ -309,8 +330,16 @@ __global__ void __launch_bounds__(TV_THREADS, 2)
         asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(
                          mb_done + (uint32_t)((j & 1) * 8))
                      : "memory");
+        issued = j + 1;
       }
       if (!ok) *abort_flag = 1;
+      // Drain (a no-op unless a wait ran out): the weights' bulk copy has landed and the
+      // MMAs of the last commit on each accumulator have completed before the tensor
+      // memory is released and the block's shared memory is given back. Layer j's commit
+      // is phase j >> 1 of done[j & 1], the newest on that barrier for the last two layers.
+      mbar_drain(mb_w, 0u, status);
+      for (int j = std::max(0, issued - 2); j < issued; ++j)
+        mbar_drain(mb_done + (uint32_t)((j & 1) * 8), (uint32_t)((j >> 1) & 1), status);
     }
     __syncwarp();
   } else {
@@ -337,7 +366,8 @@ __global__ void __launch_bounds__(TV_THREADS, 2)
           }
         }
         bool ok = !*abort_flag;
-        if (ok) ok = mbar_wait_bounded(mb_done + (uint32_t)((jp & 1) * 8), (uint32_t)((jp >> 1) & 1), status);
+        if (ok)
+          ok = mbar_wait_bounded(mb_done + (uint32_t)((jp & 1) * 8), (uint32_t)((jp >> 1) & 1), status, wait_limit);
         if (!ok) *abort_flag = 1;
         if (__all_sync(0xffffffffu, ok)) {
           asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
@@ -455,8 +485,9 @@ int launch_nf_tc(msc_plan* pl, const float2* x, const double* scale, const float
   const int nb = ncol * ((g.Nz + zc - 1) / zc);
   MSC_CUDA(prep_kernel((const void*)k_nf_tc));
   int* status = (int*)pl->status.p;
+  const long long limit = pl->wait_limit > 0 ? pl->wait_limit : TV_WAIT_LIMIT;
   k_nf_tc<<<nb, TV_THREADS, TV_SMEM, pl->stream>>>(x, scale, t4, h, acc, ch, c0, init, (const uint4*)Bpacked, g, zc,
-                                                   done, status);
+                                                   done, status, limit, pl->inject_wait);
   ::msc::note_launch();
   MSC_CUDA(cudaGetLastError());
   return MSC_OK;

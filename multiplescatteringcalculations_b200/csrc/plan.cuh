@@ -88,6 +88,15 @@ struct msc_plan {
   msc::DBuf red;
   // device status words: [0] = a bounded wait of a kernel timed out
   msc::DBuf status;
+  // polls of an mbarrier before a kernel's bounded wait gives up (0 = the kernel's default)
+  long long wait_limit = 0;
+  // 1: the tensor-core stencil also waits on an mbarrier that never completes, so its
+  // bounded wait runs out (msc_plan_set_wait_limit's failure-path test)
+  int inject_wait = 0;
+  // right-hand sides of the solve in progress (msc_solve_multi: > 1); the matvec then
+  // runs on [nrhs][9][nsite] fields with the workspace Wm
+  int nrhs = 1;
+  msc::DBuf Wm64, Wm32;
   // GMRES workspace (lazily grown)
   msc::GmresWork* gw = nullptr;
   // near-field preconditioner (blocks from the last G0 build, coefficients)
@@ -136,21 +145,31 @@ template <typename Tin, typename Tout>
 int launch_ref_to_soa(msc_plan* pl, const cx<Tin>* in, cx<Tout>* out);
 template <typename Tin, typename Tout>
 int launch_soa_to_ref(msc_plan* pl, const cx<Tin>* in, cx<Tout>* out);
-// y = x - G0 T0 (scale * x), SoA; scale may be null (1). done may be null.
+// y = x - G0 T0 (scale * x), SoA; scale may be null (1). done may be null. With
+// pl->nrhs = R > 1, x and y hold R fields one after the other ([R][9][nsite]) and the
+// operator is applied to each (the plan's multi-RHS workspace).
 template <typename T>
 int launch_matvec(msc_plan* pl, const cx<T>* x, const double* scale, cx<T>* y, const int* done);
 // complex64 plane passes with the y and x transforms fused (mv_plane_fused.cu)
 bool plane_fused_ok(const msc_plan* pl);
-int launch_plane_fwd(msc_plan* pl, const float2* x, const double* scale, float2* W, const int* done);
+int launch_plane_fwd(msc_plan* pl, const float2* x, const double* scale, float2* W, const int* done, int nrhs);
 int launch_plane_inv(msc_plan* pl, const float2* W, const float2* x, const double* scale, float2* y,
-                     const int* done);
-// the same on a caller-provided workspace of ws_elems(g) elements
+                     const int* done, int nrhs);
+// the same on a caller-provided workspace of nrhs * ws_elems(g) elements, for nrhs
+// fields [nrhs][9][nsite]
 template <typename T>
-int launch_matvec_ws(msc_plan* pl, const cx<T>* x, const double* scale, cx<T>* y, cx<T>* W, const int* done);
+int launch_matvec_ws(msc_plan* pl, const cx<T>* x, const double* scale, cx<T>* y, cx<T>* W, const int* done,
+                     int nrhs = 1);
 
 int rpp_periodic(msc_plan* pl, const double2* psi_ref, double omega, double p, int flags, double* out);
 int reflected_field(msc_plan* pl, const double2* psi_ref, double omega, const double* k_hat, double* out);
 int solve(msc_plan* pl, const double2* b_ref, double2* x_ref, const msc_solve_opts* o, msc_solve_stats* st);
+// R right-hand sides b_ref[R][N_z][M][M][9] as one stacked system (msc_solve_multi)
+int solve_multi(msc_plan* pl, int R, const double2* b_ref, double2* x_ref, const msc_solve_opts* o,
+                msc_solve_stats* stats);
+// read the plan's device status word (synchronising the plan's stream) and clear it;
+// *word = 1 when a kernel's bounded wait ran out since the last read
+int read_status(msc_plan* pl, int* word);
 void gmres_free(msc_plan* pl);
 // v *= exp(sign i k_par . x) at the cube centres (SoA complex128 field)
 int bloch_modulate(msc_plan* pl, double2* v, int sign);

@@ -302,6 +302,49 @@ class SlabPlan:
                  "residual": st.residual, "n_precond": st.n_precond, "pc_fallback": bool(st.pc_fallback)}
         return xx, stats
 
+    def solve_multi(self, b: torch.Tensor, *, tol: float, max_iter: int, restart: int = 30, precision: str = "mixed",
+                    initial_guess: str = "born", inner_tol: float = 0.0, ortho: str = "auto",
+                    preconditioner: str | None = None):
+        """Solve (I - G0 T0) x_r = b_r for the R right-hand sides b (R, N_z, M, M, 9) as
+        one stacked system (msc_solve_multi): each operator application is the multi-RHS
+        matvec, which reads the G0 spectrum once for all R. Returns (x (R, N_z, M, M, 9),
+        list of R stats dicts; ``n_matvec`` counts multi-RHS applications and
+        ``residual`` is each right-hand side's FP64 relative residual)."""
+        if precision not in ("mixed", "fp64"):
+            raise ValueError(f"precision must be 'mixed' or 'fp64', got {precision!r}")
+        pcs = {None: N.MSC_PC_NONE, "none": N.MSC_PC_NONE, "nearfield": N.MSC_PC_NEARFIELD}
+        if preconditioner not in pcs:
+            raise ValueError(f"preconditioner must be None or 'nearfield', got {preconditioner!r}")
+        if ortho not in ("auto", "cgs1", "cgs2"):
+            raise ValueError(f"ortho must be 'auto', 'cgs1' or 'cgs2', got {ortho!r}")
+        g = self.geometry
+        bb = b.to(device=self.device, dtype=torch.complex128).contiguous()
+        if bb.dim() != 5 or tuple(bb.shape[1:]) != (g.N_z, g.M, g.M, 9):
+            raise ValueError(f"b must have shape (R, {g.N_z}, {g.M}, {g.M}, 9), got {tuple(bb.shape)}")
+        R = int(bb.shape[0])
+        xx = torch.empty_like(bb)
+        opts = N.SolveOpts(float(tol), int(max_iter), int(restart),
+                           N.MSC_SOLVE_MIXED if precision == "mixed" else N.MSC_SOLVE_FP64,
+                           0 if initial_guess == "born" else 1, float(inner_tol),
+                           {"auto": 0, "cgs1": 1, "cgs2": 2}[ortho], pcs[preconditioner])
+        st = (N.SolveStats * max(1, R))()
+        N.check(self.lib.msc_solve_multi(self.handle, R, _ptr(bb), _ptr(xx), C.byref(opts), st), "msc_solve_multi")
+        stats = [{"n_matvec": s.n_matvec, "n_matvec64": s.n_matvec64, "n_outer": s.n_outer, "status": s.status,
+                  "residual": s.residual, "n_precond": s.n_precond, "pc_fallback": bool(s.pc_fallback)}
+                 for s in st[:R]]
+        return xx, stats
+
+    def matvec_multi(self, x: torch.Tensor, precision: str = "complex64") -> torch.Tensor:
+        """(I - G0 T0) x_r for R fields x (R, 9, N_z, M, M) in the component-major layout
+        (msc_matvec_multi)."""
+        dt = torch.complex128 if precision == "complex128" else torch.complex64
+        xx = x.to(device=self.device, dtype=dt).contiguous()
+        y = torch.empty_like(xx)
+        N.check(self.lib.msc_matvec_multi(self.handle, int(xx.shape[0]), _ptr(xx), _ptr(y),
+                                          N.MSC_COMPLEX128 if dt == torch.complex128 else N.MSC_COMPLEX64),
+                "msc_matvec_multi")
+        return y
+
     def set_nearfield(self, degree: int = 2, coef=None, dblocks=None, weights: str = "fp32") -> None:
         """Near-field polynomial preconditioner P = sum_l c_l S_l ... S_1 with
         S_l x = (G_nn + dG_l)(T0 x): ``coef`` (degree + 1 complex, default all ones:

@@ -100,12 +100,16 @@ def _t0_apply(t4: torch.Tensor, x: torch.Tensor) -> torch.Tensor:
 def compute_sphere_foldy_lax_fft_gpu(omega: float, radius: float, ref: ReferenceMedium, contrast, n_sub: int,
                                      k_hat=None, wave_type: str = "S", gmres_tol: float = 1e-8,
                                      gmres_maxiter: int = 200, initial_guess: str = "born", device=None, dtype=None,
-                                     *, precision: str = "mixed", restart: int = 30) -> SphereDecompositionResult:
+                                     *, precision: str = "mixed", restart: int = 30,
+                                     solver: str = "multi") -> SphereDecompositionResult:
     """Composite T-matrix of a sphere by FFT Foldy-Lax on the GPU (the reference's
     signature, sphere_scattering_fft_gpu.py:131-145). ``contrast`` has Dlambda, Dmu,
     Drho (MaterialContrast); ``k_hat`` defaults to (0, 0, 1) as in the reference.
     Keyword-only additions: ``precision`` ("mixed": complex64 GMRES inside FP64
-    refinement; "fp64") and ``restart``. ``dtype`` is accepted for compatibility; the
+    refinement; "fp64"), ``restart`` and ``solver`` ("multi", the default: the 9
+    incident patterns as one stacked system whose operator applications are the multi-
+    RHS matvec, msc_solve_multi; "columns": one GMRES solve per pattern, as the
+    reference). ``dtype`` is accepted for compatibility; the
     returned arrays are complex128 with FP64 true residuals. Non-convergence of a column
     warns, as the reference does."""
     if wave_type not in ("S", "P"):
@@ -116,6 +120,8 @@ def compute_sphere_foldy_lax_fft_gpu(omega: float, radius: float, ref: Reference
         raise ValueError(f"n_sub must be >= 1, got {n_sub}")
     if initial_guess not in ("born", "zero"):
         raise ValueError(f"initial_guess must be 'born' or 'zero', got {initial_guess!r}")
+    if solver not in ("multi", "columns"):
+        raise ValueError(f"solver must be 'multi' or 'columns', got {solver!r}")
     n = int(n_sub)
     mask, grid_idx, centres, a_sub = sphere_grid(radius, n)
     nC = len(centres)
@@ -138,12 +144,22 @@ def compute_sphere_foldy_lax_fft_gpu(omega: float, radius: float, ref: Reference
     idx = torch.from_numpy(grid_idx).to(dev)
     psi = torch.empty((nC, 9, 9), dtype=torch.complex128, device=dev)
     tcomp = torch.empty((9, 9), dtype=torch.complex128, device=dev)
-    stats = []
-    for col in range(9):
-        b = _incident_column(col, pos, mask_t, phase, x_mean)
-        x, st = plan.solve(b, tol=gmres_tol, max_iter=gmres_maxiter, restart=restart, precision=precision,
-                           initial_guess=initial_guess)
-        stats.append(st)
+    if solver == "multi":
+        # the 9 incident patterns as one stacked system: every operator application is the
+        # multi-RHS matvec, which reads the G0 spectrum once for the 9 fields
+        B = torch.stack([_incident_column(col, pos, mask_t, phase, x_mean) for col in range(9)])
+        X, stats = plan.solve_multi(B, tol=gmres_tol, max_iter=gmres_maxiter, restart=restart,
+                                    precision=precision, initial_guess=initial_guess)
+        cols = [(col, X[col], stats[col]) for col in range(9)]
+    else:
+        cols, stats = [], []
+        for col in range(9):
+            b = _incident_column(col, pos, mask_t, phase, x_mean)
+            x, st = plan.solve(b, tol=gmres_tol, max_iter=gmres_maxiter, restart=restart, precision=precision,
+                               initial_guess=initial_guess)
+            stats.append(st)
+            cols.append((col, x, st))
+    for col, x, st in cols:
         if st["residual"] > gmres_tol:
             warnings.warn(f"GPU GMRES did not converge for column {col}: rel_res={st['residual']:.2e} after "
                           f"{st['n_matvec']} matvecs", UserWarning, stacklevel=2)

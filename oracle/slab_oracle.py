@@ -832,6 +832,56 @@ def nearfield_precondition(x, t4, blocks, M, N_z, coef=(1, 1, 1), dblocks=None):
     return out
 
 
+def round_bf16(x):
+    """Round real values to bfloat16 as the device does (to float32 first, then to
+    nearest even on the upper 16 bits); returned as float64."""
+    f = np.ascontiguousarray(np.asarray(x, dtype=np.float32)).view(np.uint32).astype(np.uint64)
+    r = ((f + 0x7FFF + ((f >> 16) & 1)) & 0xFFFF0000).astype(np.uint32)
+    return r.view(np.float32).astype(np.float64)
+
+
+def _cbf16(z):
+    z = np.asarray(z)
+    return round_bf16(z.real) + 1j * round_bf16(z.imag)
+
+
+def nearfield_precondition_rounded(x, t4, blocks, M, N_z, coef=(1, 1, 1), dblocks=None, activations="bf16"):
+    """The complex64 preconditioner with the device's roundings restated (an addition
+    of this build): layer blocks G_nn + dG_l rounded to float32 and then to BF16; the
+    stencil input tau = T0 h formed in float32 and, with activations="bf16" (the
+    tensor-core form), rounded to BF16, kept in float32 with activations="fp32" (the
+    CUDA-core BF16-weight form); the products summed in FP64 (the device sums in FP32);
+    each layer output h_l stored in float32. What remains between this and the device is
+    the FP32 summation order, so a wrong tap or operand shows up far above it."""
+    if activations not in ("bf16", "fp32"):
+        raise ValueError(activations)
+    mask = nearfield_symmetry_mask()
+    t4c = np.asarray(t4).reshape(4, N_z, M, M).astype(np.complex64)
+    h = np.asarray(x).reshape(N_z, M, M, 9).astype(np.complex64)
+    out = coef[0] * h.astype(complex)
+    for l in range(1, len(coef)):
+        b = blocks if dblocks is None else blocks + dblocks[l - 1]
+        b = _cbf16(b.astype(np.complex64)) * mask
+        tr = h[..., 3] + h[..., 4] + h[..., 5]
+        tau = np.empty_like(h)
+        for c in range(3):
+            tau[..., c] = t4c[0] * h[..., c]
+        for c in range(3, 6):
+            tau[..., c] = t4c[1] * tr + t4c[2] * h[..., c]
+        for c in range(6, 9):
+            tau[..., c] = t4c[3] * h[..., c]
+        tau = _cbf16(tau) if activations == "bf16" else tau.astype(complex)
+        tp = np.zeros((N_z + 2, M + 2, M + 2, 9), dtype=complex)
+        tp[1:-1, 1:-1, 1:-1] = tau
+        y = np.zeros((N_z, M, M, 9), dtype=complex)
+        for o in range(27):
+            dz, dx, dy = o // 9 - 1, (o // 3) % 3 - 1, o % 3 - 1
+            y += tp[1 - dz:1 - dz + N_z, 1 - dx:1 - dx + M, 1 - dy:1 - dy + M] @ b[o].T
+        h = y.astype(np.complex64)
+        out = out + coef[l] * h.astype(complex)
+    return out.ravel()
+
+
 def nearfield_stencil_adjoint(y, t4, blocks, M, N_z):
     """S^H y = T0^H (sum_o G_o^H y(. + o)): the adjoint of nearfield_stencil in the
     Euclidean inner product (T0 is complex symmetric, so T0^H = conj(T0))."""

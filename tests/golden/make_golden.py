@@ -4,7 +4,8 @@ Run from the repository root where the reference checkout is available:
 
     python tests/golden/make_golden.py [path-to-reference-checkout]
 
-The default path is /root/reference. The script imports the reference package
+The path of the reference checkout comes from the argument or, without one, from
+the environment variable ``MSC_REFERENCE_ROOT``. The script imports the reference package
 ``cubic_scattering`` read-only and writes small ``.npz`` files next to this
 script. Those files pin the oracle (``oracle/slab_oracle.py``) and, through it,
 the CUDA path. Nothing at test time reads the reference checkout; only these
@@ -25,7 +26,12 @@ import numpy as np
 HERE = Path(__file__).resolve().parent
 
 
-def main(ref_root: str = "/root/reference") -> None:
+def main(ref_root: str | None = None) -> None:
+    import os
+
+    ref_root = ref_root or os.environ.get("MSC_REFERENCE_ROOT")
+    if not ref_root:
+        raise SystemExit("give the reference checkout's path as the argument or in MSC_REFERENCE_ROOT")
     sys.path.insert(0, ref_root)
     from cubic_scattering import slab_scattering as ss
     from cubic_scattering.effective_contrasts import MaterialContrast, ReferenceMedium, compute_cube_tmatrix

@@ -4,7 +4,8 @@ Run from the repository root where the reference checkout is available:
 
     python tests/golden/make_sphere_golden.py [path-to-reference-checkout]
 
-The default path is /root/reference. The script imports the reference package
+The path of the reference checkout comes from the argument or, without one, from
+the environment variable ``MSC_REFERENCE_ROOT``. The script imports the reference package
 ``cubic_scattering`` read-only, runs its CPU solver ``compute_sphere_foldy_lax_fft``
 (sphere_scattering_fft.py:228-330, scipy GMRES at rtol 1e-12) on small spheres and
 writes ``sphere.npz`` next to this script. Nothing at test time reads the reference
@@ -28,7 +29,12 @@ CASES = [
 ]
 
 
-def main(ref_root: str = "/root/reference") -> None:
+def main(ref_root: str | None = None) -> None:
+    import os
+
+    ref_root = ref_root or os.environ.get("MSC_REFERENCE_ROOT")
+    if not ref_root:
+        raise SystemExit("give the reference checkout's path as the argument or in MSC_REFERENCE_ROOT")
     sys.path.insert(0, ref_root)
     from cubic_scattering.effective_contrasts import MaterialContrast, ReferenceMedium, compute_cube_tmatrix
     from cubic_scattering.resonance_tmatrix import _sub_cell_tmatrix_9x9

@@ -395,3 +395,29 @@ def test_run_from_config_matches_oracle():
     ora = O.solve(6, 3, 1.0, 5000.0, 3000.0, 2500.0, mat.Dlambda, mat.Dmu, mat.Drho, 150.0, KZ, "P", 1e-13)
     assert res.gmres_residual < 1e-10
     assert _rel(res.psi, ora["psi"]) < 1e-9
+
+
+@pytest.mark.parametrize("M,Nz,periodic", [(12, 3, False), (64, 16, False), (16, 5, True)])
+def test_matvec_soa_equals_matvec(M, Nz, periodic):
+    """msc_matvec_soa applies the same operator on the component-major layout
+    (9, N_z, M, M) that GMRES keeps its vectors in."""
+    import ctypes as C
+
+    from multiplescatteringcalculations_b200 import SlabPlan, _native, random_slab_material
+
+    lib = _native.load()
+    g = SlabGeometry(M, Nz, 1.0)
+    mat = random_slab_material(g, REF, CONTRAST, 0.5, seed=M + Nz)
+    plan = SlabPlan(g, REF, periodic=periodic)
+    plan.build_t0(mat, OMEGA)
+    plan.build_g0(OMEGA)
+    for prec, dt, tol in ((_native.MSC_COMPLEX64, torch.complex64, 1e-6), (_native.MSC_COMPLEX128, torch.complex128,
+                                                                            1e-13)):
+        x = torch.randn(Nz, M, M, 9, dtype=dt, device=plan.device)
+        y_ref = plan.matvec(x, "complex64" if prec == _native.MSC_COMPLEX64 else "complex128")
+        xs = x.permute(3, 0, 1, 2).contiguous()
+        ys = torch.empty_like(xs)
+        assert lib.msc_matvec_soa(plan.handle, C.c_void_p(xs.data_ptr()), C.c_void_p(ys.data_ptr()), prec) == 0
+        got = ys.permute(1, 2, 3, 0).cpu().numpy()
+        assert _rel(got, y_ref.cpu().numpy()) < tol
+    plan.close()

@@ -35,9 +35,12 @@ def _run(k, **kw):
                                             str(GOLD[f"c{k}_wave"]), **kw)
 
 
+@pytest.mark.parametrize("solver", ["multi", "columns"])
 @pytest.mark.parametrize("k", range(int(GOLD["n_cases"])))
-def test_sphere_fp64_matches_reference(k):
-    r = _run(k, gmres_tol=1e-12, gmres_maxiter=2000, precision="fp64")
+def test_sphere_fp64_matches_reference(k, solver):
+    """Both solver forms: the 9 patterns as one stacked system of multi-RHS matvecs
+    (the default) and one GMRES per pattern (the reference's loop)."""
+    r = _run(k, gmres_tol=1e-12, gmres_maxiter=2000, precision="fp64", solver=solver)
     assert r.n_cells == len(GOLD[f"c{k}_centres"])
     assert np.array_equal(r.centres, GOLD[f"c{k}_centres"])
     assert _rel(r.T_comp_9x9, GOLD[f"c{k}_T_comp"]) < 1e-10
@@ -46,10 +49,12 @@ def test_sphere_fp64_matches_reference(k):
     assert all(st["residual"] <= 1e-12 for st in r.stats)
 
 
+@pytest.mark.parametrize("solver", ["multi", "columns"])
 @pytest.mark.parametrize("k", range(int(GOLD["n_cases"])))
-def test_sphere_mixed_precision(k):
+def test_sphere_mixed_precision(k, solver):
     """complex64 GMRES inside FP64 refinement reaches the FP64 answer to the tolerance."""
-    r = _run(k, gmres_tol=1e-10, gmres_maxiter=2000, precision="mixed")
+    r = _run(k, gmres_tol=1e-10, gmres_maxiter=2000, precision="mixed", solver=solver)
+    assert all(st["residual"] <= 1e-10 for st in r.stats)
     assert _rel(r.T_comp_9x9, GOLD[f"c{k}_T_comp"]) < 1e-8
     assert _rel(r.psi_exc, GOLD[f"c{k}_psi_exc"]) < 1e-8
 
@@ -62,6 +67,8 @@ def test_sphere_zero_contrast_and_errors():
         compute_sphere_foldy_lax_fft_gpu(500.0, 0.5, REF, CON, 4, wave_type="X")
     with pytest.raises(ValueError):
         compute_sphere_foldy_lax_fft_gpu(500.0, -1.0, REF, CON, 4)
+    with pytest.raises(ValueError):
+        compute_sphere_foldy_lax_fft_gpu(500.0, 0.5, REF, CON, 4, solver="blocks")
 
 
 def test_sphere_through_the_config_entry(tmp_path):

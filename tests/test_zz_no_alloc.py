@@ -82,3 +82,35 @@ def test_noalloc_rejects_bad_arguments():
     y = torch.empty_like(x)
     assert lib.msc_matvec_noalloc(plan.handle, C.c_void_p(x.data_ptr()), C.c_void_p(y.data_ptr()), 7) == \
         _native.MSC_ERR_INVALID
+
+
+def test_noalloc_on_fresh_plan_allocates_nothing():
+    """On a plan that has never run msc_matvec, the no-allocation call comes first:
+    the plan's device bytes and the device's free memory are the same before and
+    after it (the library's kernels and the static array are loaded beforehand by
+    calls of both precisions on another plan), and its result then matches
+    msc_matvec."""
+    lib = _native.load()
+    g0, warm = _plan(8, 2, False)
+    for prec, dt in ((_native.MSC_COMPLEX64, torch.complex64), (_native.MSC_COMPLEX128, torch.complex128)):
+        xw = torch.randn(2, 8, 8, 9, dtype=dt, device=warm.device)
+        assert _call(lib, "msc_matvec_noalloc", warm, xw, prec)[0] == 0
+    g, plan = _plan(32, 8, False)
+    torch.manual_seed(5)
+    for precision, dt, rtol in ((_native.MSC_COMPLEX64, torch.complex64, 1e-5),
+                                (_native.MSC_COMPLEX128, torch.complex128, 1e-10)):
+        x = torch.randn(8, 32, 32, 9, dtype=dt, device=plan.device)
+        y = torch.empty_like(x)
+        torch.cuda.synchronize()
+        plan_bytes = lib.msc_plan_device_bytes(plan.handle)
+        free0 = torch.cuda.mem_get_info()[0]
+        st = lib.msc_matvec_noalloc(plan.handle, C.c_void_p(x.data_ptr()), C.c_void_p(y.data_ptr()), precision)
+        torch.cuda.synchronize()
+        assert st == 0, lib.msc_last_error()
+        assert lib.msc_plan_device_bytes(plan.handle) == plan_bytes
+        assert torch.cuda.mem_get_info()[0] == free0
+        st_ref, y_ref = _call(lib, "msc_matvec", plan, x, precision)
+        assert st_ref == 0
+        assert lib.msc_plan_device_bytes(plan.handle) > plan_bytes  # msc_matvec allocated its field copies
+        a, b = y.cpu().numpy(), y_ref.cpu().numpy()
+        assert np.linalg.norm(a - b) <= rtol * np.linalg.norm(b)
