@@ -338,8 +338,9 @@ def cfg1_sample(dev, nrep: int = 20) -> dict:
 
 
 # held-out slabs of the learned-preconditioner distribution (cfg4_problem seeds) on which
-# every solver setting converges within the budget
-CFG4_SAMPLE_SEEDS = (5003, 5005, 5007)
+# every solver setting converges within the budget; on 5000 the near-field polynomial
+# slows the solve down, on 5005 it speeds it up several times
+CFG4_SAMPLE_SEEDS = (5000, 5003, 5005, 5007)
 
 
 def cfg4_sample(dev, seeds=CFG4_SAMPLE_SEEDS, tol: float = 1e-8) -> dict:
@@ -347,8 +348,9 @@ def cfg4_sample(dev, seeds=CFG4_SAMPLE_SEEDS, tol: float = 1e-8) -> dict:
     learned-preconditioner distribution for plain FP64 GMRES(30), plain mixed precision,
     mixed precision with the physics Neumann polynomial of the network's degree (layers
     on the tensor cores), and mixed precision with the packaged learned network (no
-    training in the timed region); each solve includes T0, G0, incident and R_PP; one
-    untimed and one timed solve per slab and setting."""
+    training in the timed region), each preconditioner under the adaptive cycle policy
+    and preconditioning every cycle ("_always"); each solve includes T0, G0, incident
+    and R_PP; one untimed and one timed solve per slab and setting."""
     import torch
 
     from multiplescatteringcalculations_b200 import SlabPlan
@@ -357,8 +359,12 @@ def cfg4_sample(dev, seeds=CFG4_SAMPLE_SEEDS, tol: float = 1e-8) -> dict:
 
     net = _packaged_network()
     physics = NearFieldPreconditioner(net.degree)
-    variants = {"fp64": ("fp64", None), "mixed": ("mixed", None),
-                f"mixed_nearfield_d{net.degree}_tc": ("mixed", physics), "mixed_learned": ("mixed", net)}
+    d = net.degree
+    variants = {"fp64": ("fp64", None, None), "mixed": ("mixed", None, None),
+                f"mixed_nearfield_d{d}_tc": ("mixed", physics, "nearfield"),
+                f"mixed_nearfield_d{d}_tc_always": ("mixed", physics, "nearfield_always"),
+                "mixed_learned": ("mixed", net, "nearfield"),
+                "mixed_learned_always": ("mixed", net, "nearfield_always")}
     wl = WORKLOADS["cfg4"]
     rows = []
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -368,15 +374,14 @@ def cfg4_sample(dev, seeds=CFG4_SAMPLE_SEEDS, tol: float = 1e-8) -> dict:
         md = type(mat)(torch.from_numpy(mat.Dlambda).to(dev), torch.from_numpy(mat.Dmu).to(dev),
                        torch.from_numpy(mat.Drho).to(dev), ref)
         row = {"seed": seed, "ell": par[0], "std": par[1], "ka": par[2], "wave": wave}
-        for name, (prec, pc) in variants.items():
+        for name, (prec, pc, mode) in variants.items():
             def step():
                 plan.build_t0(md, om)
                 plan.build_g0(om)
                 psi0 = plan.incident(om, kh, wave)
                 if pc is not None:
                     pc.install(plan)
-                x, st = plan.solve(psi0, tol=tol, max_iter=6000, restart=30, precision=prec,
-                                   preconditioner=None if pc is None else "nearfield")
+                x, st = plan.solve(psi0, tol=tol, max_iter=6000, restart=30, precision=prec, preconditioner=mode)
                 plan.rpp_periodic(x, om)
                 return st
             step()
@@ -386,6 +391,7 @@ def cfg4_sample(dev, seeds=CFG4_SAMPLE_SEEDS, tol: float = 1e-8) -> dict:
             e1.record(plan.stream)
             torch.cuda.synchronize()
             row[name] = {"ms": e0.elapsed_time(e1), "n_matvec": st["n_matvec"], "n_precond": st["n_precond"],
+                         "pc_cycles": st["pc_cycles"], "plain_cycles": st["plain_cycles"],
                          "residual": st["residual"], "pc_fallback": st["pc_fallback"]}
         rows.append(row)
         plan.close()
@@ -395,6 +401,79 @@ def cfg4_sample(dev, seeds=CFG4_SAMPLE_SEEDS, tol: float = 1e-8) -> dict:
             "ms_per_solve": {n: tot[n] / len(rows) for n in variants},
             "speedup_vs_fp64_plain": {n: tot["fp64"] / tot[n] for n in variants},
             "per_slab": rows}
+
+
+CFG5_BUDGETS = (100, 300, 1000)
+
+
+def run_cfg5(args, wl, local_rank) -> int:
+    """The large strong-contrast slab (256 x 256 x 32 periodic, ka = 1, GRF std 40 %, SV at
+    30 deg, 18.9 M unknowns). Restarted GMRES does not converge on it (the residual stalls,
+    plain or preconditioned); what is measured: the T0 and G0 setup, the complex64
+    matvec against the HBM roofline, and per solver setting the FP64 true residual
+    reached within growing matvec budgets with the time per operator application."""
+    import torch
+
+    from multiplescatteringcalculations_b200 import SlabPlan, _native
+    from multiplescatteringcalculations_b200.slab import _packaged_network
+
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    lib = _native.load()
+    ref, geom, mat, k_hat, omega = make_problem(wl, seed=1000)
+    plan = SlabPlan(geom, ref, periodic=True, device=dev)
+    md = type(mat)(torch.from_numpy(mat.Dlambda).to(dev), torch.from_numpy(mat.Dmu).to(dev),
+                   torch.from_numpy(mat.Drho).to(dev), ref)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    for _ in range(2):
+        e0.record(plan.stream)
+        plan.build_t0(md, omega)
+        plan.build_g0(omega)
+        psi0 = plan.incident(omega, k_hat, wl["wave"])
+        e1.record(plan.stream)
+        torch.cuda.synchronize()
+    ms_setup = e0.elapsed_time(e1)
+    roof = matvec_roofline(plan, geom, "cfg5", dev)
+    net = _packaged_network()
+
+    def pc_nf(p):
+        p.set_nearfield(2, weights="bf16_tc")
+
+    variants = {"fp64": ("fp64", None), "mixed": ("mixed", None), "mixed_nearfield_tc": ("mixed", pc_nf),
+                "mixed_learned": ("mixed", net.install)}
+    hist = {}
+    n0 = lib.msc_launch_count()
+    with ClockSampler(local_rank) as clk:
+        for name, (prec, pc) in variants.items():
+            rows = []
+            for budget in CFG5_BUDGETS:
+                if pc is not None:
+                    pc(plan)
+                torch.cuda.synchronize()
+                e0.record(plan.stream)
+                x, st = plan.solve(psi0, tol=wl["tol"], max_iter=budget, restart=30, precision=prec,
+                                   preconditioner=None if pc is None else "nearfield")
+                e1.record(plan.stream)
+                torch.cuda.synchronize()
+                ms = e0.elapsed_time(e1)
+                rows.append({"budget": budget, "n_matvec": st["n_matvec"], "residual": st["residual"], "ms": ms,
+                             "ms_per_matvec": ms / max(1, st["n_matvec"]), "pc_cycles": st["pc_cycles"],
+                             "plain_cycles": st["plain_cycles"]})
+            hist[name] = rows
+    launches = lib.msc_launch_count() - n0
+    converged = any(r["residual"] <= wl["tol"] for rows in hist.values() for r in rows)
+    line = {
+        "metric": "complex64 matvec GB/s on the 256x256x32 slab (the solve does not converge)",
+        "value": roof["achieved"], "unit": "GB/s", "n_gpus": 1, "steps": len(CFG5_BUDGETS), "warmup": 1,
+        "ms_per_step": roof["us_per_matvec"] / 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "c64+c128", "data": "synthetic",
+        "config": {"workload": "cfg5", **_cfg_desc(wl), "fft": list(plan.fft_sizes()), "unknowns": 9 * geom.N_z * geom.M ** 2},
+        "gpu_launches": int(launches), "setup_ms": ms_setup, "roofline": roof, "converged": converged,
+        "residual_history": hist, "clocks": clk.summary(),
+    }
+    print(json.dumps(line), flush=True)
+    plan.close()
+    return 0
 
 
 def run_ours(args, wl, rank, world, local_rank):
@@ -496,7 +575,8 @@ def run_ours(args, wl, rank, world, local_rank):
         e1.record(stream)
         torch.cuda.synchronize()
         arm_out[name] = {"ms_per_solve": e0.elapsed_time(e1) / nrep, "n_matvec": st_a["n_matvec"],
-                         "n_precond": st_a["n_precond"], "pc_fallback": st_a["pc_fallback"],
+                         "n_precond": st_a["n_precond"], "pc_cycles": st_a["pc_cycles"],
+                         "plain_cycles": st_a["plain_cycles"], "pc_fallback": st_a["pc_fallback"],
                          "residual": st_a["residual"]}
     ms64 = arm_out["fp64"]["ms_per_solve"]
     for a in arm_out.values():
@@ -983,6 +1063,8 @@ def main(argv=None) -> int:
         return run_train_steps(args.train_only)
     if "precond_eval" in wl:
         return run_precond_eval(args, wl, rank, world, local_rank)
+    if args.workload == "cfg5":
+        return run_cfg5(args, wl, local_rank)
     if "sphere" in wl:
         return run_sphere(args, wl, rank, local_rank)
     if "batch" in wl:

@@ -40,7 +40,13 @@ enum msc_status {
 enum msc_precision { MSC_COMPLEX64 = 0, MSC_COMPLEX128 = 1 };
 enum msc_solver_precision { MSC_SOLVE_MIXED = 0, MSC_SOLVE_FP64 = 1 };
 enum msc_wave { MSC_WAVE_P = 0, MSC_WAVE_S = 1 };
-enum msc_preconditioner { MSC_PC_NONE = 0, MSC_PC_NEARFIELD = 1 };
+/* MSC_PC_NEARFIELD: flexible GMRES with the near-field preconditioner on the right, in
+ * the cycles where it earns its cost: after a few preconditioned cycles one plain cycle
+ * is measured, each cycle's residual reduction per unit of device time is compared, and
+ * the faster form runs (the slower one is measured again now and then).
+ * MSC_PC_NEARFIELD_ALWAYS: every cycle preconditioned. Under both, a preconditioned
+ * cycle without any progress turns the preconditioner off for the solve. */
+enum msc_preconditioner { MSC_PC_NONE = 0, MSC_PC_NEARFIELD = 1, MSC_PC_NEARFIELD_ALWAYS = 2 };
 
 typedef struct msc_slab_desc {
   int32_t M;         /* lateral cubes per side (SlabGeometry.M) */
@@ -73,6 +79,9 @@ typedef struct msc_solve_stats {
   double residual;       /* true relative residual in FP64 (reference: gmres_residual) */
   int32_t n_precond;     /* preconditioner applications */
   int32_t pc_fallback;   /* 1: a preconditioned cycle failed to reduce the residual; plain GMRES finished */
+  int32_t pc_cycles;     /* GMRES cycles run with the preconditioner (flexible GMRES) */
+  int32_t plain_cycles;  /* cycles run without it: the policy's measurement cycles, the ones where the plain
+                            form reduced the residual faster per unit time, and the fallback */
 } msc_solve_stats;
 
 typedef struct msc_plan msc_plan;
@@ -243,6 +252,10 @@ typedef struct msc_batch_item {
   double k_hat[3];         /* incidence direction (z, x, y) */
   int32_t wave_type;       /* msc_wave */
   int32_t bloch;           /* periodic only: Bloch-phased fold at the incidence's k_par */
+  int32_t volume_averaged; /* 1: volume-averaged nearest-neighbour blocks (reference volume_averaged) */
+  int32_t n_orders;        /* orders of the volume-averaged blocks, 0 = 2 (the reference's default) */
+  double rpp_p;            /* horizontal slowness at which R_PP is evaluated (the reference's p); < 0: the
+                              incidence's slowness for Bloch items, 0 (normal incidence) for the others */
   void* psi;               /* out (may be NULL): (N_z, M, M, 9) complex128, host */
   double rpp[2];           /* out: specular R_PP (re, im) by the Weyl sum of the solution */
   msc_solve_stats stats;   /* out */

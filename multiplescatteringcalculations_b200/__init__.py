@@ -15,8 +15,10 @@ from .slab import (  # noqa: F401
     SlabMaterial,
     SlabPlan,
     SlabResult,
+    SlabSweepResult,
     clear_plan_cache,
     compute_slab_scattering_batch,
+    compute_slab_rpp_sweep,
     compute_slab_scattering_gpu,
     compute_slab_tmatrices,
     gaussian_random_field_material,

@@ -30,6 +30,7 @@ MSC_RPP_BLOCH = 1
 MSC_RPP_PLANE_WAVE_MOMENT = 2
 MSC_PC_NONE = 0
 MSC_PC_NEARFIELD = 1
+MSC_PC_NEARFIELD_ALWAYS = 2
 MSC_NF_WEIGHTS_FP32 = 0
 MSC_NF_WEIGHTS_BF16 = 1
 MSC_NF_WEIGHTS_BF16_TC = 2
@@ -75,6 +76,8 @@ class SolveStats(C.Structure):
         ("residual", C.c_double),
         ("n_precond", C.c_int32),
         ("pc_fallback", C.c_int32),
+        ("pc_cycles", C.c_int32),
+        ("plain_cycles", C.c_int32),
     ]
 
 
@@ -88,6 +91,9 @@ class BatchItem(C.Structure):
         ("k_hat", C.c_double * 3),
         ("wave_type", C.c_int32),
         ("bloch", C.c_int32),
+        ("volume_averaged", C.c_int32),
+        ("n_orders", C.c_int32),
+        ("rpp_p", C.c_double),
         ("psi", C.c_void_p),
         ("rpp", C.c_double * 2),
         ("stats", SolveStats),

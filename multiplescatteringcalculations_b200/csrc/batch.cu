@@ -9,14 +9,20 @@
 // solves of different workers overlap on the device; their GMRES cycles run
 // uncaptured (a graph capture per new plan costs more than a short solve saves).
 // Plan memory comes from the library's memory pool, so the plan churn of a batch over
-// many shapes reuses device memory instead of mapping it again. With workers = 0 an online autotuner times the first items at 1, 2 and 4
-// workers and finishes the batch with the fastest. Items are independent: a failed
-// item records its status and the others continue.
+// many shapes reuses device memory instead of mapping it again. A solved field leaves
+// the device by DMA into one of the worker's two page-locked buffers; a copier thread
+// moves it into the caller's array while the workers carry on. With workers = 0 an
+// online autotuner times the first items at 1, 2 and 4 workers and finishes the batch
+// with the fastest. Items are independent: a failed item records its status and the
+// others continue.
 #include <algorithm>
 #include <atomic>
 #include <chrono>
 #include <cmath>
+#include <condition_variable>
 #include <cstring>
+#include <deque>
+#include <mutex>
 #include <thread>
 #include <vector>
 
@@ -34,22 +40,120 @@ struct CachedPlan {
   long long last_use = 0;
 };
 
+// Page-locked host staging of one batch worker: the contrasts of an item on their way
+// in, and two buffers for fields on their way out. Kept per (device, worker index)
+// for the life of the process, grown to the largest item seen, so later batch calls
+// pay no cudaHostAlloc.
+struct PinnedStaging {
+  void* in = nullptr;
+  size_t in_bytes = 0;
+  void* out[2] = {nullptr, nullptr};
+  size_t out_bytes[2] = {0, 0};
+};
+
+PinnedStaging& pinned_staging(int device, int worker) {
+  static std::mutex mu;
+  static std::vector<std::vector<PinnedStaging*>> all;
+  std::lock_guard<std::mutex> lk(mu);
+  if ((int)all.size() <= device) all.resize(device + 1);
+  auto& v = all[device];
+  while ((int)v.size() <= worker) v.push_back(new PinnedStaging());
+  return *v[worker];
+}
+
+int grow_pinned(void*& p, size_t& have, size_t need) {
+  if (have >= need) return MSC_OK;
+  if (p) cudaFreeHost(p);
+  p = nullptr;
+  have = 0;
+  if (cudaMallocHost(&p, need) != cudaSuccess) {
+    cudaGetLastError();
+    set_error("batch: pinned staging of %zu bytes failed", need);
+    return MSC_ERR_NOMEM;
+  }
+  have = need;
+  return MSC_OK;
+}
+
+// Moves fields from the workers' pinned buffers into the callers' arrays on its own
+// host thread, so the host copy of one item overlaps the device work of the next ones.
+struct Copier {
+  struct Job {
+    cudaEvent_t ev;
+    const void* src;
+    void* dst;
+    size_t bytes;
+    std::atomic<int>* busy;
+  };
+  std::mutex mu;
+  std::condition_variable cv;
+  std::deque<Job> q;
+  bool stop = false;
+  std::atomic<bool> failed{false};
+  std::thread th;
+
+  explicit Copier(int device) {
+    th = std::thread([this, device]() {
+      cudaSetDevice(device);
+      while (true) {
+        Job j;
+        {
+          std::unique_lock<std::mutex> lk(mu);
+          cv.wait(lk, [&] { return stop || !q.empty(); });
+          if (q.empty()) return;
+          j = q.front();
+          q.pop_front();
+        }
+        if (cudaEventSynchronize(j.ev) != cudaSuccess) failed.store(true);
+        else std::memcpy(j.dst, j.src, j.bytes);
+        j.busy->store(0);
+      }
+    });
+  }
+  void push(const Job& j) {
+    {
+      std::lock_guard<std::mutex> lk(mu);
+      q.push_back(j);
+    }
+    cv.notify_one();
+  }
+  // drains the queue and ends the thread
+  void finish() {
+    {
+      std::lock_guard<std::mutex> lk(mu);
+      stop = true;
+    }
+    cv.notify_one();
+    if (th.joinable()) th.join();
+  }
+  ~Copier() { finish(); }
+};
+
 struct Worker {
   cudaStream_t stream = nullptr;
   int device = 0;
+  int index = 0;
   std::vector<CachedPlan> plans;
   long long tick = 0;
   // device staging: contrasts (3 N float64), psi0 and x (9 N complex128 each)
   void* dev = nullptr;
   size_t dev_bytes = 0;
-  // pinned host staging for the contrasts
-  void* host = nullptr;
-  size_t host_bytes = 0;
+  PinnedStaging* pin = nullptr;
+  // fields in flight to the caller: copied into pin->out[s] on the stream (event ev[s]),
+  // then into the caller's array by the copier; busy[s] until the copier is done
+  Copier* copier = nullptr;
+  cudaEvent_t ev[2] = {nullptr, nullptr};
+  std::atomic<int> busy[2];
+  int slot = 0;
 
-  Worker() = default;
+  Worker() {
+    busy[0] = 0;
+    busy[1] = 0;
+  }
   Worker(const Worker&) = delete;
   Worker& operator=(const Worker&) = delete;
   ~Worker() {
+    drain();
     for (auto& c : plans)
       if (c.plan) msc_plan_destroy(c.plan);
     if (dev) cudaFreeAsync(dev, stream);
@@ -57,7 +161,40 @@ struct Worker {
       cudaStreamSynchronize(stream);
       cudaStreamDestroy(stream);
     }
-    if (host) cudaFreeHost(host);
+    for (auto& e : ev)
+      if (e) cudaEventDestroy(e);
+  }
+
+  int init(int dev_index, int worker_index, Copier* c) {
+    device = dev_index;
+    index = worker_index;
+    copier = c;
+    pin = &pinned_staging(dev_index, worker_index);
+    MSC_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+    for (auto& e : ev) MSC_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    return MSC_OK;
+  }
+
+  void wait_slot(int s) {
+    while (busy[s].load()) std::this_thread::yield();
+  }
+  // every field of this worker has reached its caller's array
+  void drain() {
+    wait_slot(0);
+    wait_slot(1);
+  }
+
+  // queue the device field x (bytes) for the caller's host array h
+  int send(void* h, const void* x, size_t bytes) {
+    const int s = slot;
+    slot ^= 1;
+    wait_slot(s);
+    MSC_TRY(grow_pinned(pin->out[s], pin->out_bytes[s], bytes));
+    MSC_CUDA(cudaMemcpyAsync(pin->out[s], x, bytes, cudaMemcpyDeviceToHost, stream));
+    MSC_CUDA(cudaEventRecord(ev[s], stream));
+    busy[s].store(1);
+    copier->push(Copier::Job{ev[s], pin->out[s], h, bytes, &busy[s]});
+    return MSC_OK;
   }
 
   int plan_for(const msc_slab_desc& d, msc_plan** out) {
@@ -101,17 +238,9 @@ struct Worker {
       }
       dev_bytes = dbytes;
     }
-    if (host_bytes < hbytes) {
+    if (pin->in_bytes < hbytes) {
       cudaStreamSynchronize(stream);
-      if (host) cudaFreeHost(host);
-      host = nullptr;
-      host_bytes = 0;
-      if (cudaMallocHost(&host, hbytes) != cudaSuccess) {
-        cudaGetLastError();
-        set_error("batch: pinned staging of %zu bytes failed", hbytes);
-        return MSC_ERR_NOMEM;
-      }
-      host_bytes = hbytes;
+      MSC_TRY(grow_pinned(pin->in, pin->in_bytes, hbytes));
     }
     return MSC_OK;
   }
@@ -126,7 +255,7 @@ struct Worker {
     double* dc = (double*)dev;
     double2* psi0 = (double2*)(dc + 3 * ns);
     double2* x = psi0 + 9 * ns;
-    double* hc = (double*)host;
+    double* hc = (double*)pin->in;
     MSC_CUDA(cudaStreamSynchronize(stream));  // the pinned buffer is free again
     std::memcpy(hc, it.dlam, sizeof(double) * ns);
     std::memcpy(hc + ns, it.dmu, sizeof(double) * ns);
@@ -140,22 +269,22 @@ struct Worker {
       kpar[0] = it.omega / speed * it.k_hat[1] / nk;
       kpar[1] = it.omega / speed * it.k_hat[2] / nk;
     }
-    MSC_TRY(msc_build_g0(pl, it.omega, it.bloch ? kpar : nullptr, 0, 2));
+    MSC_TRY(msc_build_g0(pl, it.omega, it.bloch ? kpar : nullptr, it.volume_averaged ? 1 : 0,
+                         it.n_orders > 0 ? it.n_orders : 2));
     MSC_TRY(msc_incident(pl, it.omega, it.k_hat, it.wave_type, psi0));
     msc_solve_stats st{};
     const int s = msc_solve(pl, psi0, x, &o, &st);
     it.stats = st;
     if (s < 0) return s;
-    // specular R_PP: at the horizontal slowness of the incidence for Bloch items,
-    // else at normal incidence (the reference's default)
-    const double p = it.bloch ? std::sqrt(it.k_hat[1] * it.k_hat[1] + it.k_hat[2] * it.k_hat[2]) / nk / speed : 0.0;
+    // specular R_PP: at the item's slowness, by default the horizontal slowness of the
+    // incidence for Bloch items, else normal incidence (the reference's default)
+    const double p = it.rpp_p >= 0 ? it.rpp_p
+                     : it.bloch ? std::sqrt(it.k_hat[1] * it.k_hat[1] + it.k_hat[2] * it.k_hat[2]) / nk / speed
+                                : 0.0;
     MSC_TRY(msc_rpp_periodic(pl, x, it.omega, p, it.bloch ? MSC_RPP_BLOCH : 0, it.rpp));
-    if (it.psi) {
-      // straight into the caller's array: a second copy through the pinned staging
-      // buffer costs a host memcpy at single-thread bandwidth
-      MSC_CUDA(cudaMemcpyAsync(it.psi, x, fb, cudaMemcpyDeviceToHost, stream));
-      MSC_CUDA(cudaStreamSynchronize(stream));
-    }
+    // the field: a DMA into a pinned buffer on the stream; the host moves it into the
+    // caller's (pageable) array while the worker's next item runs on the device
+    if (it.psi) MSC_TRY(send(it.psi, x, fb));
     return s;
   }
 };
@@ -184,6 +313,8 @@ double run_workers(std::vector<Worker>& pool, int w, msc_batch_item* items, std:
           it.error[sizeof(it.error) - 1] = 0;
         }
       }
+      // the fields still in flight reach the caller before the chunk counts as done
+      wk.drain();
     });
   }
   for (auto& t : th) t.join();
@@ -219,11 +350,9 @@ extern "C" int msc_batch_solve(msc_batch_item* items, int n, const msc_solve_opt
   int device = 0;
   MSC_CUDA(cudaGetDevice(&device));
   const int maxw = workers > 0 ? workers : 4;
+  Copier copier(device);
   std::vector<Worker> pool(maxw);
-  for (auto& w : pool) {
-    w.device = device;
-    MSC_CUDA(cudaStreamCreateWithFlags(&w.stream, cudaStreamNonBlocking));
-  }
+  for (int i = 0; i < maxw; ++i) MSC_TRY(pool[i].init(device, i, &copier));
   std::atomic<int> next{0};
   int chosen = workers;
   if (workers == 0) {
@@ -245,6 +374,11 @@ extern "C" int msc_batch_solve(msc_batch_item* items, int n, const msc_solve_opt
     }
   }
   if (next.load() < n) run_workers(pool, chosen, items, next, n, *opts, device);
+  copier.finish();
+  if (copier.failed.load()) {
+    set_error("batch: a field's copy to the host failed");
+    return MSC_ERR_CUDA;
+  }
   if (workers_used) *workers_used = chosen;
   for (int i = 0; i < n; ++i)
     if (items[i].status != MSC_OK) return MSC_NOT_CONVERGED;

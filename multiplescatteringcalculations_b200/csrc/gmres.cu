@@ -51,6 +51,7 @@ struct GmresWork {
   DBuf part;              // partial sums [NB][33]
   GState* hstate = nullptr;  // pinned host mirror
   cudaEvent_t ev[2] = {nullptr, nullptr};
+  cudaEvent_t tev[2] = {nullptr, nullptr};  // timing of a cycle (preconditioner policy)
   // captured Arnoldi cycles, [precision][preconditioned]
   struct Graph {
     cudaGraphExec_t exec = nullptr;
@@ -628,6 +629,8 @@ static int ensure_work(msc_plan* pl, int m) {
     MSC_CUDA(cudaMallocHost((void**)&gw->hstate, sizeof(GState) * 2));
     MSC_CUDA(cudaEventCreateWithFlags(&gw->ev[0], cudaEventDisableTiming));
     MSC_CUDA(cudaEventCreateWithFlags(&gw->ev[1], cudaEventDisableTiming));
+    MSC_CUDA(cudaEventCreate(&gw->tev[0]));
+    MSC_CUDA(cudaEventCreate(&gw->tev[1]));
   }
   return MSC_OK;
 }
@@ -643,29 +646,76 @@ void gmres_free(msc_plan* pl) {
       if (gr.exec) cudaGraphExecDestroy(gr.exec);
   for (auto& e : gw->ev)
     if (e) cudaEventDestroy(e);
+  for (auto& e : gw->tev)
+    if (e) cudaEventDestroy(e);
   delete gw;
   pl->gw = nullptr;
 }
+
+// Which cycles of flexible GMRES run with the preconditioner (MSC_PC_NEARFIELD): it has
+// to earn its cost. Every cycle's residual reduction per millisecond of device time,
+// -ln(res / beta) / t, is kept for the preconditioned and for the plain form (the mean
+// with the previous value of that form). The solve starts preconditioned; after
+// PROBE_AFTER preconditioned cycles one plain cycle measures the other form (restarted
+// GMRES converges fastest in its first cycles, plain or not, so an early comparison
+// favours the plain form), and from then on the faster form runs. A preconditioned
+// form at least twice as fast keeps running; a closer race is measured again after
+// 8, 32, 128, ... cycles of the faster form. MSC_PC_NEARFIELD_ALWAYS runs every cycle
+// preconditioned. Under both, a preconditioned cycle that makes no progress at all (a
+// breakdown of A P included) turns the preconditioner off for the rest of the solve.
+// Cycles during which a graph was captured are not measured (the capture is host
+// time). The policy lives for one solve, across its refinement sweeps.
+struct PcPolicy {
+  static constexpr int PROBE_AFTER = 4;
+  bool allowed = false;       // a preconditioner is asked for and has not failed
+  bool adaptive = true;       // false: every cycle preconditioned (MSC_PC_NEARFIELD_ALWAYS)
+  bool on = true;             // form of the next cycle
+  double eff[2] = {-1, -1};   // [plain, preconditioned] log-reduction per ms; -1 unknown
+  int run = 0;                // cycles of the faster form since the last probe
+  int interval = 8;           // cycles between probes of the slower form
+  int cycles[2] = {0, 0};     // cycles run per form
+  bool failed = false;        // the no-progress fallback happened
+
+  void measure(bool pc, double beta, double res, float ms) {
+    if (!(beta > 0) || !(res > 0) || !(ms > 0)) return;
+    const double e = -std::log(res / beta) / (double)ms;
+    double& v = eff[pc ? 1 : 0];
+    v = v < 0 ? e : 0.5 * (v + e);
+  }
+  bool next() {
+    if (!allowed) return on = false;
+    if (!adaptive) return on = true;
+    if (eff[0] < 0) return on = cycles[1] < PROBE_AFTER;  // the first plain measurement
+    if (eff[1] < 0) return on = true;
+    const bool pc_faster = eff[1] >= eff[0];
+    if (eff[1] >= 2.0 * eff[0]) return on = true;
+    if (++run >= interval) {
+      run = 0;
+      interval *= 4;
+      return on = !pc_faster;
+    }
+    return on = pc_faster;
+  }
+};
 
 // One restarted GMRES(m) solve of A x = rhs in precision T (x in/out, same precision).
 // Stops when the residual estimate <= tol_abs or after max_mv operator applications.
 // Returns the number of matvecs used in *n_mv and the final estimate in *res.
 //
-// With `pc` the solve is flexible GMRES with the near-field preconditioner on the
-// right: z_j = P(v_j), w = A z_j, x += Z y. A cycle that does not reduce the
-// residual estimate turns the preconditioner off for the rest of the solve
-// (*pc_off = 1): plain GMRES is the fallback.
+// With a policy `pol` that allows it the solve is flexible GMRES with the near-field
+// preconditioner on the right, z_j = P(v_j), w = A z_j, x += Z y, in the cycles the
+// policy chooses; plain GMRES runs the others.
 template <typename T>
 static int gmres_core(msc_plan* pl, int m, const cx<T>* rhs, cx<T>* x, bool x_zero, double tol_abs, int max_mv,
-                      int* n_mv, double* res, int* status, bool cgs2, bool pc, int* n_pc, int* pc_off) {
+                      int* n_mv, double* res, int* status, bool cgs2, PcPolicy* pol, int* n_pc) {
   GmresWork* gw = pl->gw;
   GState* st = (GState*)gw->state.p;
   HessPtr h = hess_ptrs(gw);
   const size_t n = gw->n;
   cx<T>* V = (cx<T>*)(sizeof(T) == 8 ? gw->V64.p : gw->V32.p);
-  bool use_pc = pc;
+  bool use_pc = pol && pol->allowed && pol->on;
   cx<T>* Z = nullptr;
-  if (use_pc) {
+  if (pol && pol->allowed) {
     DBuf& zb = sizeof(T) == 8 ? gw->Z64 : gw->Z32;
     MSC_TRY(dalloc(pl, zb, sizeof(cx<T>) * (size_t)gw->m * n));
     Z = (cx<T>*)zb.p;
@@ -675,6 +725,9 @@ static int gmres_core(msc_plan* pl, int m, const cx<T>* rhs, cx<T>* x, bool x_ze
   *status = MSC_NOT_CONVERGED;
   bool first = true;
   while (true) {
+    const bool timed = pol && pol->allowed;
+    if (timed) MSC_CUDA(cudaEventRecord(gw->tev[0], pl->stream));
+    bool captured_now = false;
     // V0 = rhs - A x  (or rhs when x == 0 on the first cycle)
     if (first && x_zero) {
       MSC_CUDA(cudaMemcpyAsync(V, rhs, sizeof(cx<T>) * n, cudaMemcpyDeviceToDevice, pl->stream));
@@ -741,10 +794,12 @@ static int gmres_core(msc_plan* pl, int m, const cx<T>* rhs, cx<T>* x, bool x_ze
         gr.cgs2 = cgs2;
         gr.nrhs = pl->nrhs;
         gr.gen = pl->gen;
+        captured_now = true;
       }
       if (use_pc) MSC_TRY(nearfield_refresh(pl));  // new blocks (a new frequency) into the same buffers
       MSC_CUDA(cudaGraphLaunch(gr.exec, pl->stream));
       ::msc::note_launch();
+      if (timed) MSC_CUDA(cudaEventRecord(gw->tev[1], pl->stream));
       MSC_CUDA(cudaMemcpyAsync(&gw->hstate[0], st, sizeof(GState), cudaMemcpyDeviceToHost, pl->stream));
       MSC_CUDA(cudaStreamSynchronize(pl->stream));
       cur = gw->hstate[0];
@@ -776,11 +831,13 @@ static int gmres_core(msc_plan* pl, int m, const cx<T>* rhs, cx<T>* x, bool x_ze
         pending = slot;
       }
       // cycles that ended at step j (and not before) are visible in the newest state
+      if (timed) MSC_CUDA(cudaEventRecord(gw->tev[1], pl->stream));
       MSC_CUDA(cudaMemcpyAsync(&gw->hstate[0], st, sizeof(GState), cudaMemcpyDeviceToHost, pl->stream));
       MSC_CUDA(cudaStreamSynchronize(pl->stream));
       cur = gw->hstate[0];
       gr.warm += 1;
     }
+    if (pol && enq > 0) ++pol->cycles[use_pc ? 1 : 0];
     // x += V y (k columns), or Z y with the preconditioner
     if (cur.k > 0) {
       const int nb = std::min<long long>(NB, ceil_div((long long)n, NTH));
@@ -798,13 +855,20 @@ static int gmres_core(msc_plan* pl, int m, const cx<T>* rhs, cx<T>* x, bool x_ze
       *status = MSC_OK;
       break;
     }
-    // A preconditioned cycle that fails to reduce the residual estimate at all (a
-    // breakdown of A P included) turns the preconditioner off; slow progress, which
-    // plain GMRES shows as well on hard slabs, does not.
-    if (use_pc && cur.res >= (1.0 - 1e-6) * cur.beta) {
-      use_pc = false;
-      *pc_off = 1;
-      continue;
+    // The policy measures this cycle and picks the next cycle's form. A preconditioned
+    // cycle that fails to reduce the residual estimate at all (a breakdown of A P
+    // included) turns the preconditioner off for the rest of the solve.
+    if (pol && pol->allowed) {
+      float ms = 0.f;
+      if (!captured_now && cur.steps > 0) MSC_CUDA(cudaEventElapsedTime(&ms, gw->tev[0], gw->tev[1]));
+      pol->measure(use_pc, cur.beta, cur.res, captured_now ? 0.f : ms);
+      const bool stalled = use_pc && cur.res >= (1.0 - 1e-6) * cur.beta;
+      if (stalled) {
+        pol->allowed = false;
+        pol->failed = true;
+      }
+      use_pc = pol->next();
+      if (stalled) continue;
     }
     if (cur.status == MSC_BREAKDOWN) {
       *status = MSC_OK;
@@ -833,7 +897,10 @@ static int solve_core(msc_plan* pl, const double2* b, double2* x, double bnorm, 
   double* dn = &h.nrm[1].x;  // outer ||.||^2 (h.nrm[1].y is scratch of the reduction)
   s.status = MSC_NOT_CONVERGED;
   const int max_mv = o->max_iter > 0 ? o->max_iter : 500;
-  const bool pc = o->preconditioner == MSC_PC_NEARFIELD;
+  PcPolicy pol;
+  pol.allowed = o->preconditioner == MSC_PC_NEARFIELD || o->preconditioner == MSC_PC_NEARFIELD_ALWAYS;
+  pol.adaptive = o->preconditioner == MSC_PC_NEARFIELD;
+  PcPolicy* pp = pol.allowed ? &pol : nullptr;
   if (bnorm == 0.0) {
     MSC_CUDA(cudaMemsetAsync(x, 0, sizeof(double2) * n, pl->stream));
     MSC_CUDA(cudaMemsetAsync(r, 0, sizeof(double2) * n, pl->stream));
@@ -843,7 +910,7 @@ static int solve_core(msc_plan* pl, const double2* b, double2* x, double bnorm, 
     int used = 0, st = 0;
     double est = 0;
     MSC_TRY(gmres_core<double>(pl, m, b, x, o->initial_guess != 0, tol * bnorm, max_mv, &used, &est, &st,
-                               o->ortho != 1, pc, &s.n_precond, &s.pc_fallback));
+                               o->ortho != 1, pp, &s.n_precond));
     s.n_matvec = used;
     s.n_matvec64 = used;
     s.status = st;
@@ -888,8 +955,8 @@ static int solve_core(msc_plan* pl, const double2* b, double2* x, double bnorm, 
       const double target = std::max(inner, 0.5 * tol / res);
       int iu = 0, ist = 0;
       double est = 0;
-      MSC_TRY(gmres_core<float>(pl, m, r32, d, true, target, max_mv - used, &iu, &est, &ist, o->ortho == 2,
-                                pc && !s.pc_fallback, &s.n_precond, &s.pc_fallback));
+      MSC_TRY(gmres_core<float>(pl, m, r32, d, true, target, max_mv - used, &iu, &est, &ist, o->ortho == 2, pp,
+                                &s.n_precond));
       used += iu;
       ++outer;
       if (ist == MSC_ERR_NONFINITE) {
@@ -906,6 +973,9 @@ static int solve_core(msc_plan* pl, const double2* b, double2* x, double bnorm, 
     s.n_outer = outer;
     s.residual = res;
   }
+  s.pc_fallback = pol.failed ? 1 : 0;
+  s.pc_cycles = pol.cycles[1];
+  s.plain_cycles = pol.cycles[0];
   return MSC_OK;
 }
 
@@ -914,11 +984,11 @@ static int check_solve_opts(msc_plan* pl, const msc_solve_opts* o) {
     set_error("solve needs build_t0 and build_g0 first");
     return MSC_ERR_STATE;
   }
-  if (o->preconditioner < 0 || o->preconditioner > 1) {
+  if (o->preconditioner < 0 || o->preconditioner > 2) {
     set_error("unknown preconditioner %d", o->preconditioner);
     return MSC_ERR_INVALID;
   }
-  if (o->preconditioner == MSC_PC_NEARFIELD && (!pl->nf || !pl->nf->ready)) {
+  if (o->preconditioner != MSC_PC_NONE && (!pl->nf || !pl->nf->ready)) {
     set_error("the near-field preconditioner needs build_g0 first");
     return MSC_ERR_STATE;
   }

@@ -43,11 +43,16 @@ int launch_matvec_ws(msc_plan* pl, const cx<T>* x, const double* scale, cx<T>* y
   const cx<T>* twxy = (const cx<T>*)(sizeof(T) == 8 ? pl->tw64_xy.p : pl->tw32_xy.p);
   // x lines: the contiguous rows of the nrhs workspaces
   const long long G = (long long)nrhs * 9 * g.Nz * g.Ly;
+  bool yreg = false;
+  if constexpr (sizeof(T) == 4) yreg = y_reg_ok(pl);
   MSC_TRY(launch_t0_fft_y<T>(pl, x, scale, W, twxy, done, nrhs));                                 // A
   MSC_TRY(launch_fft_contig<T>(pl, W, W, G, G, 0, g.Lx, g.M, g.Lx, pl->fxy, twxy, -1, done));      // X
   MSC_TRY(launch_zbz<T>(pl, W, done, nrhs));                                                      // ZBZ'
   MSC_TRY(launch_fft_contig<T>(pl, W, W, G, G, 0, g.Lx, g.Lx, g.M, pl->fxy, twxy, +1, done));      // X'
-  MSC_TRY(launch_fft_y_out<T>(pl, W, x, scale, y, twxy, done, nrhs));                             // C
+  if constexpr (sizeof(T) == 4) {
+    if (yreg) MSC_TRY(launch_fft_y_out_reg(pl, W, x, scale, y, done, nrhs));                     // C
+  }
+  if (!yreg) MSC_TRY(launch_fft_y_out<T>(pl, W, x, scale, y, twxy, done, nrhs));                  // C
   return MSC_OK;
 }
 

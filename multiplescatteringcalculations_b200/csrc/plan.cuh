@@ -155,6 +155,11 @@ bool plane_fused_ok(const msc_plan* pl);
 int launch_plane_fwd(msc_plan* pl, const float2* x, const double* scale, float2* W, const int* done, int nrhs);
 int launch_plane_inv(msc_plan* pl, const float2* W, const float2* x, const double* scale, float2* y,
                      const int* done, int nrhs);
+// complex64 inverse y pass on the register four-step engine, Ly in {64, 128, 256}
+// (mv_plane_reg.cu)
+bool y_reg_ok(const msc_plan* pl);
+int launch_fft_y_out_reg(msc_plan* pl, const float2* W, const float2* x, const double* scale, float2* y,
+                         const int* done, int nrhs);
 // the same on a caller-provided workspace of nrhs * ws_elems(g) elements, for nrhs
 // fields [nrhs][9][nsite]
 template <typename T>

@@ -285,9 +285,10 @@ class SlabPlan:
         settings from ``set_nearfield``; plain GMRES takes over if it stalls)."""
         if precision not in ("mixed", "fp64"):
             raise ValueError(f"precision must be 'mixed' or 'fp64', got {precision!r}")
-        pcs = {None: N.MSC_PC_NONE, "none": N.MSC_PC_NONE, "nearfield": N.MSC_PC_NEARFIELD}
+        pcs = {None: N.MSC_PC_NONE, "none": N.MSC_PC_NONE, "nearfield": N.MSC_PC_NEARFIELD,
+               "nearfield_always": N.MSC_PC_NEARFIELD_ALWAYS}
         if preconditioner not in pcs:
-            raise ValueError(f"preconditioner must be None or 'nearfield', got {preconditioner!r}")
+            raise ValueError(f"preconditioner must be None, 'nearfield' or 'nearfield_always', got {preconditioner!r}")
         bb = b.to(device=self.device, dtype=torch.complex128).contiguous()
         xx = torch.empty_like(bb) if x is None else x
         if ortho not in ("auto", "cgs1", "cgs2"):
@@ -299,7 +300,8 @@ class SlabPlan:
         st = N.SolveStats()
         status = N.check(self.lib.msc_solve(self.handle, _ptr(bb), _ptr(xx), C.byref(opts), C.byref(st)), "msc_solve")
         stats = {"n_matvec": st.n_matvec, "n_matvec64": st.n_matvec64, "n_outer": st.n_outer, "status": status,
-                 "residual": st.residual, "n_precond": st.n_precond, "pc_fallback": bool(st.pc_fallback)}
+                 "residual": st.residual, "n_precond": st.n_precond, "pc_fallback": bool(st.pc_fallback),
+                 "pc_cycles": st.pc_cycles, "plain_cycles": st.plain_cycles}
         return xx, stats
 
     def solve_multi(self, b: torch.Tensor, *, tol: float, max_iter: int, restart: int = 30, precision: str = "mixed",
@@ -312,9 +314,10 @@ class SlabPlan:
         ``residual`` is each right-hand side's FP64 relative residual)."""
         if precision not in ("mixed", "fp64"):
             raise ValueError(f"precision must be 'mixed' or 'fp64', got {precision!r}")
-        pcs = {None: N.MSC_PC_NONE, "none": N.MSC_PC_NONE, "nearfield": N.MSC_PC_NEARFIELD}
+        pcs = {None: N.MSC_PC_NONE, "none": N.MSC_PC_NONE, "nearfield": N.MSC_PC_NEARFIELD,
+               "nearfield_always": N.MSC_PC_NEARFIELD_ALWAYS}
         if preconditioner not in pcs:
-            raise ValueError(f"preconditioner must be None or 'nearfield', got {preconditioner!r}")
+            raise ValueError(f"preconditioner must be None, 'nearfield' or 'nearfield_always', got {preconditioner!r}")
         if ortho not in ("auto", "cgs1", "cgs2"):
             raise ValueError(f"ortho must be 'auto', 'cgs1' or 'cgs2', got {ortho!r}")
         g = self.geometry
@@ -330,7 +333,8 @@ class SlabPlan:
         st = (N.SolveStats * max(1, R))()
         N.check(self.lib.msc_solve_multi(self.handle, R, _ptr(bb), _ptr(xx), C.byref(opts), st), "msc_solve_multi")
         stats = [{"n_matvec": s.n_matvec, "n_matvec64": s.n_matvec64, "n_outer": s.n_outer, "status": s.status,
-                  "residual": s.residual, "n_precond": s.n_precond, "pc_fallback": bool(s.pc_fallback)}
+                  "residual": s.residual, "n_precond": s.n_precond, "pc_fallback": bool(s.pc_fallback),
+                  "pc_cycles": s.pc_cycles, "plain_cycles": s.plain_cycles}
                  for s in st[:R]]
         return xx, stats
 
@@ -604,6 +608,7 @@ def compute_slab_scattering_gpu(
     inner_tol: float = 0.0,
     ortho: str = "auto",
     plan: SlabPlan | None = None,
+    pc_policy: str = "adaptive",
 ) -> SlabResult:
     """Solve (I - G0 T0) psi = psi0 on the GPU.
 
@@ -621,9 +626,14 @@ def compute_slab_scattering_gpu(
     near-field Neumann polynomial of the plan's settings), "learned" (the packaged
     network, trained on the GPU on Gaussian-random-field slabs:
     ``data/make_nearfield_weights.py``), or a ``NearFieldPreconditioner`` (its degree,
-    coefficients and learned block corrections); plain GMRES finishes the solve if a
-    preconditioned cycle stalls.
+    coefficients and learned block corrections). ``pc_policy``: "adaptive" (default:
+    after a few preconditioned GMRES cycles one plain cycle is measured, and the form
+    that reduces the residual faster per unit of device time runs, measured again now
+    and then) or "always" (every cycle preconditioned); under both, plain GMRES
+    finishes the solve if a preconditioned cycle makes no progress.
     """
+    if pc_policy not in ("adaptive", "always"):
+        raise ValueError(f"pc_policy must be 'adaptive' or 'always', got {pc_policy!r}")
     if wave_type not in ("P", "S"):
         raise ValueError(f"wave_type must be 'P' or 'S', got '{wave_type}'")
     if dtype is not None and dtype not in (torch.complex64, torch.complex128):
@@ -656,6 +666,8 @@ def compute_slab_scattering_gpu(
             preconditioner.install(plan)
         else:
             plan.set_nearfield()
+    if pc_mode is not None and pc_policy == "always":
+        pc_mode = "nearfield_always"
     x, st = plan.solve(psi0, tol=gmres_tol, max_iter=max_iter, restart=restart, precision=precision,
                        initial_guess=initial_guess, inner_tol=inner_tol, ortho=ortho, preconditioner=pc_mode)
     if st["residual"] > gmres_tol:
@@ -702,7 +714,10 @@ def compute_slab_scattering_gpu(
 
 @dataclass
 class BatchProblem:
-    """One slab of a batch: geometry, material, frequency and incidence."""
+    """One slab of a batch: geometry, material, frequency and incidence;
+    ``volume_averaged``/``n_orders`` as the reference's solver options; ``rpp_p`` the
+    horizontal slowness at which R_PP is evaluated (None: the incidence's slowness for
+    ``bloch`` items, normal incidence otherwise)."""
 
     geometry: SlabGeometry
     material: SlabMaterial
@@ -711,6 +726,9 @@ class BatchProblem:
     wave_type: str = "P"
     periodic: bool = False
     bloch: bool = False
+    volume_averaged: bool = False
+    n_orders: int = 2
+    rpp_p: float | None = None
 
 
 @dataclass
@@ -740,9 +758,10 @@ def compute_slab_scattering_batch(problems, *, gmres_tol: float = 1e-6, max_iter
     them."""
     if precision not in ("mixed", "fp64"):
         raise ValueError(f"precision must be 'mixed' or 'fp64', got {precision!r}")
-    pcs = {None: N.MSC_PC_NONE, "none": N.MSC_PC_NONE, "nearfield": N.MSC_PC_NEARFIELD}
+    pcs = {None: N.MSC_PC_NONE, "none": N.MSC_PC_NONE, "nearfield": N.MSC_PC_NEARFIELD,
+           "nearfield_always": N.MSC_PC_NEARFIELD_ALWAYS}
     if preconditioner not in pcs:
-        raise ValueError(f"preconditioner must be None or 'nearfield', got {preconditioner!r}")
+        raise ValueError(f"preconditioner must be None, 'nearfield' or 'nearfield_always', got {preconditioner!r}")
     if ortho not in ("auto", "cgs1", "cgs2"):
         raise ValueError(f"ortho must be 'auto', 'cgs1' or 'cgs2', got {ortho!r}")
     problems = list(problems)
@@ -768,6 +787,11 @@ def compute_slab_scattering_batch(problems, *, gmres_tol: float = 1e-6, max_iter
             it.k_hat[j] = float(kh[j])
         it.wave_type = N.MSC_WAVE_P if pr.wave_type == "P" else N.MSC_WAVE_S
         it.bloch = int(bool(pr.bloch))
+        it.volume_averaged = int(bool(pr.volume_averaged))
+        it.n_orders = int(pr.n_orders)
+        if pr.rpp_p is not None and not pr.rpp_p >= 0:
+            raise ValueError(f"item {i}: rpp_p must be >= 0, got {pr.rpp_p}")
+        it.rpp_p = -1.0 if pr.rpp_p is None else float(pr.rpp_p)
         out = np.empty((g.N_z, g.M, g.M, 9), dtype=np.complex128) if return_fields else None
         outs.append(out)
         it.psi = out.ctypes.data if out is not None else None
@@ -783,7 +807,8 @@ def compute_slab_scattering_batch(problems, *, gmres_tol: float = 1e-6, max_iter
         it = items[i]
         st = {"n_matvec": it.stats.n_matvec, "n_matvec64": it.stats.n_matvec64, "n_outer": it.stats.n_outer,
               "residual": it.stats.residual, "n_precond": it.stats.n_precond,
-              "pc_fallback": bool(it.stats.pc_fallback)}
+              "pc_fallback": bool(it.stats.pc_fallback), "pc_cycles": it.stats.pc_cycles,
+              "plain_cycles": it.stats.plain_cycles}
         if it.status != 0:
             bad.append((i, it.status, it.error.decode(errors="replace")))
         sols.append(BatchSolution(psi=outs[i], rpp=complex(it.rpp[0], it.rpp[1]), n_gmres_iter=int(it.stats.n_matvec),
@@ -791,6 +816,53 @@ def compute_slab_scattering_batch(problems, *, gmres_tol: float = 1e-6, max_iter
     if bad:
         warnings.warn(f"{len(bad)} batch item(s) did not converge or failed: {bad[:4]}", stacklevel=2)
     return sols, {"workers": int(used.value)}
+
+
+@dataclass
+class SlabSweepResult:
+    """Per-frequency results of ``compute_slab_rpp_sweep``: ``rpp`` (n,) complex, the
+    specular R_PP of each frequency's solution at slowness ``p``; ``n_gmres_iter`` and
+    ``gmres_residual`` per frequency; ``psi`` the fields (None unless asked for)."""
+
+    omegas: NDArray
+    rpp: NDArray
+    n_gmres_iter: list
+    gmres_residual: NDArray
+    status: list
+    psi: list | None
+
+
+def compute_slab_rpp_sweep(geometry: SlabGeometry, material: SlabMaterial, omegas, k_hat, p: float = 0.0, *,
+                           wave_type: str = "P", gmres_tol: float = 1e-6, max_iter: int = 500,
+                           volume_averaged: bool = False, n_orders: int = 2, bloch: bool = False,
+                           precision: str = "mixed", restart: int = 30, workers: int = 0,
+                           return_fields: bool = False) -> SlabSweepResult:
+    """The frequency loop of the reference's ocean-bottom model
+    (ocean_bottom.py:290-307): for every angular frequency w of ``omegas`` one periodic
+    slab solve at incidence ``k_hat`` and the specular R_PP of its solution at horizontal
+    slowness ``p`` by the reference's Weyl sum (``slab_rpp_periodic(result, T_local,
+    p=p)``), T0 built once per frequency. All frequencies go to the GPU in one batch call
+    (msc_batch_solve). ``bloch=False`` keeps the reference's fold without a Bloch phase;
+    ``bloch=True`` solves with the Bloch-phased fold at the incidence's k_par (R_PP then
+    demodulates the sources, as ``slab_rpp_periodic`` with ``bloch``)."""
+    om = np.atleast_1d(np.asarray(omegas, dtype=float)).ravel()
+    if om.size == 0:
+        raise ValueError("omegas is empty")
+    if not np.all(om > 0):
+        raise ValueError("every omega must be > 0")
+    if not p >= 0:
+        raise ValueError(f"p must be >= 0, got {p}")
+    kh = np.asarray(k_hat, dtype=float).ravel()
+    probs = [BatchProblem(geometry, material, float(w), kh, wave_type, periodic=True, bloch=bool(bloch),
+                          volume_averaged=bool(volume_averaged), n_orders=int(n_orders), rpp_p=float(p))
+             for w in om]
+    sols, _ = compute_slab_scattering_batch(probs, gmres_tol=gmres_tol, max_iter=max_iter, restart=restart,
+                                            precision=precision, workers=workers, return_fields=return_fields)
+    return SlabSweepResult(omegas=om, rpp=np.array([s.rpp for s in sols]),
+                           n_gmres_iter=[s.n_gmres_iter for s in sols],
+                           gmres_residual=np.array([s.gmres_residual for s in sols]),
+                           status=[s.status for s in sols],
+                           psi=[s.psi for s in sols] if return_fields else None)
 
 
 # ---------------------------------------------------------------------------

@@ -23,7 +23,7 @@ from dataclasses import dataclass, field
 import numpy as np
 import torch
 
-from .slab import ReferenceMedium, SlabGeometry, SlabMaterial, _cached_plan
+from .slab import ReferenceMedium, SlabGeometry, SlabMaterial, _cached_plan, _host_array
 
 __all__ = ["SphereDecompositionResult", "compute_sphere_foldy_lax_fft_gpu", "sphere_grid"]
 
@@ -166,7 +166,15 @@ def compute_sphere_foldy_lax_fft_gpu(omega: float, radius: float, ref: Reference
         psi[:, :, col] = x[idx[:, 0], idx[:, 1], idx[:, 2]]
         tcomp[:, col] = _t0_apply(t4, x).reshape(-1, 9).sum(0)
     T = tcomp.cpu().numpy()
+    # the exciting field (9 nC x 9 complex128, 22 MB at n_sub = 32) into a recycled host
+    # array: a page-locked one takes an asynchronous DMA instead of a pageable copy
+    psi_h, psi_pin = _host_array((9 * nC, 9))
+    if psi_pin is not None:
+        psi_pin.copy_(psi.reshape(9 * nC, 9), non_blocking=True)
+        torch.cuda.current_stream(dev).synchronize()
+    else:
+        torch.from_numpy(psi_h).copy_(psi.reshape(9 * nC, 9))
     return SphereDecompositionResult(
         T3x3=T[:3, :3].copy(), T_comp_9x9=T, centres=centres, n_sub=n, n_cells=nC, a_sub=a_sub,
-        condition_number=float("nan"), psi_exc=psi.reshape(9 * nC, 9).cpu().numpy(), omega=float(omega),
+        condition_number=float("nan"), psi_exc=psi_h, omega=float(omega),
         radius=float(radius), ref=ref, contrast=contrast, stats=stats)

@@ -81,3 +81,35 @@ def test_batch_without_fields_and_with_the_nearfield_preconditioner():
     sols, _ = compute_slab_scattering_batch(probs, gmres_tol=1e-10, return_fields=False, preconditioner="nearfield")
     for s in sols:
         assert s.psi is None and s.status == 0 and s.gmres_residual < 1e-10
+
+
+@pytest.mark.parametrize("volume_averaged", [False, True])
+def test_frequency_sweep_matches_oracle_per_frequency(volume_averaged):
+    """compute_slab_rpp_sweep serves the frequency loop of the reference's ocean-bottom
+    model (ocean_bottom.py:290-307): one periodic oblique slab per frequency, R_PP at the
+    incidence slowness p by the reference's Weyl sum; each frequency against the
+    oracle's FP64 solve and R_PP."""
+    from multiplescatteringcalculations_b200 import compute_slab_rpp_sweep
+
+    from oracle import slab_oracle as O
+
+    ref = ReferenceMedium(3000.0, 1732.0, 2500.0)
+    g = SlabGeometry(8, 3, 1.0)
+    mat = uniform_random_material(g, ref, 0.15, seed=11)
+    th = np.deg2rad(25.0)
+    k_hat = np.array([np.cos(th), np.sin(th), 0.0])
+    p = np.sin(th) / ref.alpha
+    omegas = np.array([0.1, 0.25, 0.4, 0.6]) * ref.beta
+    sw = compute_slab_rpp_sweep(g, mat, omegas, k_hat, p, gmres_tol=1e-11, max_iter=2000,
+                                volume_averaged=volume_averaged, return_fields=True)
+    assert list(sw.status) == [0] * len(omegas)
+    for i, w in enumerate(omegas):
+        ora = O.solve(8, 3, 1.0, ref.alpha, ref.beta, ref.rho, mat.Dlambda, mat.Dmu, mat.Drho, w, k_hat, "P",
+                      1e-13, 2000, periodic=True, restart=30, volume_averaged=volume_averaged)
+        rpp_o = O.rpp_periodic(ora["psi"], ora["t4"], 8, 3, 1.0, w, ref.alpha, ref.rho, p=p)
+        assert np.linalg.norm(sw.psi[i] - ora["psi"]) <= 1e-9 * np.linalg.norm(ora["psi"])
+        assert abs(sw.rpp[i] - rpp_o) <= 1e-8 * abs(rpp_o)
+    with pytest.raises(ValueError):
+        compute_slab_rpp_sweep(g, mat, [], k_hat, p)
+    with pytest.raises(ValueError):
+        compute_slab_rpp_sweep(g, mat, omegas, k_hat, -1.0)

@@ -164,6 +164,9 @@ def test_learned_preconditioner_ablation(capsys):
     else:
         assert np.array_equal(net.coef, np.ones(net.degree + 1)) and not net.w.any()
     assert sum(learned) < sum(plain)
+    # training earns its place on held-out slabs: no more operator applications than the
+    # untrained polynomial of the same degree
+    assert sum(learned) <= sum(start)
 
 
 def test_packaged_network_as_drop_in_option():

@@ -421,3 +421,29 @@ def test_matvec_soa_equals_matvec(M, Nz, periodic):
         got = ys.permute(1, 2, 3, 0).cpu().numpy()
         assert _rel(got, y_ref.cpu().numpy()) < tol
     plan.close()
+
+
+@pytest.mark.parametrize("M,Nz,periodic", [(64, 3, True), (128, 2, True), (256, 2, True), (100, 2, False)])
+def test_complex64_matvec_large_planes(M, Nz, periodic):
+    """Planes the fused plane kernels do not hold: the inverse y pass on the register
+    four-step engine (Ly = 64, 128, 256; 100 x 100 aperiodic pads to 200, the shared-
+    memory tiles) against the complex128 path, and at M = 64 against the oracle."""
+    from multiplescatteringcalculations_b200 import SlabPlan, random_slab_material
+
+    g = SlabGeometry(M, Nz, 1.0)
+    mat = random_slab_material(g, REF, CONTRAST, 0.5, seed=M)
+    plan = SlabPlan(g, REF, periodic=periodic)
+    plan.build_t0(mat, OMEGA)
+    plan.build_g0(OMEGA)
+    torch.manual_seed(M)
+    x = torch.randn(Nz, M, M, 9, dtype=torch.complex128, device=plan.device)
+    y64 = plan.matvec(x, "complex128").cpu().numpy()
+    y32 = plan.matvec(x, "complex64").cpu().numpy()
+    assert _rel(y32, y64) < 5e-6
+    if M == 64:
+        t4 = O.t0_scalars(OMEGA, 1.0, REF.alpha, REF.beta, REF.rho, mat.Dlambda, mat.Dmu, mat.Drho)
+        kh = O.build_slab_kernels(M, Nz, 1.0, OMEGA, REF.alpha, REF.beta, REF.rho, periodic=periodic)
+        want = O.slab_matvec(x.cpu().numpy().ravel(), t4, kh, M, Nz, periodic=periodic).reshape(y64.shape)
+        assert _rel(y64, want) < 1e-10
+        assert _rel(y32, want) < 5e-6
+    plan.close()
