@@ -170,3 +170,21 @@ def test_packaged_network_runs_on_tensor_cores():
     net = _packaged_network()
     assert net.weights == "bf16_tc"
     assert net.degree == 4 and net.w.shape == (4, 27, 9, 9)
+
+
+def test_sphere_incident_columns_batched_equal_per_column():
+    """The 9 incident patterns of the sphere built at once equal the per-column form
+    (resonance_tmatrix.py:526-586 restated), bit for bit (CPU tensors)."""
+    import torch
+
+    from multiplescatteringcalculations_b200 import sphere as S
+
+    n = 6
+    mask, _, centres, a_sub = S.sphere_grid(0.5, n)
+    c1 = (-n / 2 + 0.5 + np.arange(n)) * (2 * a_sub)
+    pos = torch.stack(torch.meshgrid(*(torch.tensor(c1),) * 3, indexing="ij"), -1)
+    phase = torch.exp(1j * 5.0 * (pos @ torch.tensor([0.3, 0.4, np.sqrt(0.75)])))
+    xm = torch.tensor(centres.mean(axis=0))
+    mt = torch.from_numpy(mask)
+    a = torch.stack([S._incident_column(c, pos, mt, phase, xm) for c in range(9)])
+    assert torch.equal(a, S._incident_columns(pos, mt, phase, xm))
