@@ -15,8 +15,23 @@ template <> struct CxT<double> { using type = double2; };
 template <typename T> using cx = typename CxT<T>::type;
 
 template <typename T> __host__ __device__ __forceinline__ cx<T> mk(T a, T b) { cx<T> r; r.x = a; r.y = b; return r; }
-__host__ __device__ __forceinline__ float2 operator+(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
-__host__ __device__ __forceinline__ float2 operator-(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+// complex64 sums and differences as paired FP32 instructions on the device (each lane
+// rounds as the scalar operation does, so results are the same bits); a - b is
+// fma(b, -1, a), exact in the product
+__host__ __device__ __forceinline__ float2 operator+(float2 a, float2 b) {
+#if defined(__CUDA_ARCH__)
+  return __fadd2_rn(a, b);
+#else
+  return make_float2(a.x + b.x, a.y + b.y);
+#endif
+}
+__host__ __device__ __forceinline__ float2 operator-(float2 a, float2 b) {
+#if defined(__CUDA_ARCH__)
+  return __ffma2_rn(b, make_float2(-1.f, -1.f), a);
+#else
+  return make_float2(a.x - b.x, a.y - b.y);
+#endif
+}
 __host__ __device__ __forceinline__ float2 operator*(float2 a, float2 b) {
   return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
 }
@@ -27,9 +42,9 @@ __host__ __device__ __forceinline__ double2 operator*(double2 a, double2 b) {
   return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
 }
 __host__ __device__ __forceinline__ double2 operator*(double s, double2 a) { return make_double2(s * a.x, s * a.y); }
-__host__ __device__ __forceinline__ float2& operator+=(float2& a, float2 b) { a.x += b.x; a.y += b.y; return a; }
+__host__ __device__ __forceinline__ float2& operator+=(float2& a, float2 b) { a = a + b; return a; }
 __host__ __device__ __forceinline__ double2& operator+=(double2& a, double2 b) { a.x += b.x; a.y += b.y; return a; }
-__host__ __device__ __forceinline__ float2& operator-=(float2& a, float2 b) { a.x -= b.x; a.y -= b.y; return a; }
+__host__ __device__ __forceinline__ float2& operator-=(float2& a, float2 b) { a = a - b; return a; }
 __host__ __device__ __forceinline__ double2& operator-=(double2& a, double2 b) { a.x -= b.x; a.y -= b.y; return a; }
 
 template <typename C> __host__ __device__ __forceinline__ C conj_(C a) { a.y = -a.y; return a; }

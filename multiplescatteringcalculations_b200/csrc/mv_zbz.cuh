@@ -20,14 +20,34 @@
 
 namespace msc {
 
-template <typename C> __device__ __forceinline__ void reflect(C* v, int f) {
+// v <- S_f v: the sign flips as XORs of the sign bits (no compare and select per
+// component). sign_mask(f) holds bit c when component c is odd under the reflections
+// f (bit 0 x, bit 1 y, bit 2 z).
+__device__ __forceinline__ unsigned sign_mask(int f) {
+  unsigned m = 0;
 #pragma unroll
-  for (int c = 0; c < 9; ++c)
-    if (__popc(dof_parity(c) & f) & 1) {
-      v[c].x = -v[c].x;
-      v[c].y = -v[c].y;
-    }
+  for (int c = 0; c < 9; ++c) m |= (unsigned)(__popc(dof_parity(c) & f) & 1) << c;
+  return m;
 }
+__device__ __forceinline__ void reflect_mask(float2* v, unsigned m) {
+#pragma unroll
+  for (int c = 0; c < 9; ++c) {
+    if (dof_parity(c) == 0) continue;  // even under every reflection
+    const unsigned s = ((m >> c) & 1u) << 31;
+    v[c].x = __uint_as_float(__float_as_uint(v[c].x) ^ s);
+    v[c].y = __uint_as_float(__float_as_uint(v[c].y) ^ s);
+  }
+}
+__device__ __forceinline__ void reflect_mask(double2* v, unsigned m) {
+#pragma unroll
+  for (int c = 0; c < 9; ++c) {
+    if (dof_parity(c) == 0) continue;
+    const unsigned long long s = (unsigned long long)((m >> c) & 1u) << 63;
+    v[c].x = __longlong_as_double((long long)((unsigned long long)__double_as_longlong(v[c].x) ^ s));
+    v[c].y = __longlong_as_double((long long)((unsigned long long)__double_as_longlong(v[c].y) ^ s));
+  }
+}
+template <typename C> __device__ __forceinline__ void reflect(C* v, int f) { reflect_mask(v, sign_mask(f)); }
 
 // One field vector t multiplied by one kernel block, in place; ld(e) returns the
 // stored entry e. SYM (E = 45): entry e enumerates i <= j row-major and holds
@@ -256,122 +276,6 @@ __global__ void __launch_bounds__(ZBZ_THREADS, 2) k_zbz(cx<T>* __restrict__ W, c
   }
 }
 
-// Register-resident variant for short power-of-two Lz (octant spectrum): one thread
-// per line (component, column slot) loads its N_z layers into registers, transforms
-// along z in registers and writes the spectrum to one shared tile; after the block
-// multiply (as in k_zbz) it reads its line back, transforms inversely in registers
-// (computing only the N_z layers kept) and stores them. Two barriers instead of one
-// per FFT stage, one tile instead of two. NT = NL rounded up to whole warps (a
-// multiple of 8 KX, as the multiply's item walk needs).
-template <int KX> constexpr int zbz_reg_threads() { return ((36 * KX + 31) / 32) * 32; }
-
-//
-// nrhs > 1: as in k_zbz, the staged slice serves the same columns of nrhs vectors in
-// turn.
-template <typename T, int LC, int KXC, bool SYM>
-__global__ void __launch_bounds__(zbz_reg_threads<KXC>(), 3)
-    k_zbz_reg(cx<T>* __restrict__ W, const kent<T>* __restrict__ khat, Geo g, ZbzLayout lay,
-              const cx<T>* __restrict__ twg, const int* done, int nrhs) {
-  pdl_wait();
-  pdl_trigger();
-  if (done && *done) return;
-  using C = cx<T>;
-  using KE = kent<T>;
-  constexpr int KX = KXC, NC = 4 * KX, NL = 9 * NC, P = NL + 1, Lz = LC;
-  constexpr int NT = zbz_reg_threads<KXC>();
-  static_assert(NT % (8 * KX) == 0, "item walk of the multiply");
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  __shared__ long long loff[ZBZ_MAX_LINES];
-  __shared__ int sflag[ZBZ_MAX_LINES / 9];
-  const bool ksm = lay.ksm != 0;
-  KE* ks = reinterpret_cast<KE*>(smem_raw);
-  C* tw = reinterpret_cast<C*>(ks + (ksm ? lay.CS : 0));
-  C* ta = tw + Lz;
-  const int tid = threadIdx.x;
-  const long long plane = (long long)g.Ly * g.Lx;
-  const long long cstride = (long long)g.Nz * plane;
-  const int kyo = blockIdx.y;
-  const int x0 = blockIdx.x * KX;
-  const KE* kblk = khat + ((long long)kyo * lay.NXC + blockIdx.x) * lay.CS;
-  if (ksm) {
-    const int n16 = (int)(lay.CS * sizeof(KE) / 16);
-    for (int i = tid; i < n16; i += NT)
-      cp_async16(reinterpret_cast<unsigned char*>(ks) + 16 * i, reinterpret_cast<const unsigned char*>(kblk) + 16 * i);
-  }
-  if (tid < NC) {
-    const int s = tid;
-    const int q = s / KX, kxo = x0 + s % KX;
-    bool ok = kxo < g.Hx;
-    if (q & 1) ok = ok && kxo != 0 && 2 * kxo != g.Lx;  // kx_o has a distinct mirror
-    if (q & 2) ok = ok && kyo != 0 && 2 * kyo != g.Ly;
-    const int kx = (q & 1) ? g.Lx - kxo : kxo;
-    const int ky = (q & 2) ? g.Ly - kyo : kyo;
-    const long long col = ok ? (long long)ky * g.Lx + kx : -1;
-#pragma unroll
-    for (int c = 0; c < 9; ++c) loff[c * NC + s] = col >= 0 ? c * cstride + col : -1;
-    sflag[s] = q;
-  }
-  for (int t = tid; t < Lz; t += NT) tw[t] = twg[t];
-  __syncthreads();
-  const int line = tid;
-  const long long o0 = line < NL ? loff[line] : -1;
-  for (int rh = 0; rh < nrhs; ++rh) {
-  const long long o = o0 >= 0 ? o0 + (long long)rh * 9 * cstride : -1;
-  C v[Lz];
-  if (line < NL) {
-    // N_z <= Lz/2: only the first half of the line holds data
-#pragma unroll
-    for (int n = 0; n < Lz; ++n) v[n] = (n < Lz / 2 && o >= 0 && n < g.Nz) ? W[o + n * plane] : czero<C>();
-    fft_reg<Lz, -1>(v, tw);
-#pragma unroll
-    for (int k = 0; k < Lz; ++k) ta[k * P + line] = v[k];
-  }
-  cp_async_wait_all();
-  __syncthreads();
-  {
-    // item (j, q, side, kp): as in k_zbz
-    const int j = tid % KX, q = (tid / KX) & 3, side = (tid / (4 * KX)) & 1;
-    constexpr int kstep = NT / (8 * KX);
-    const int s = q * KX + j;
-    const int estr = g.Hz * KX;
-    const int f0 = sflag[s] | (side ? 4 : 0);
-    if (loff[s] >= 0) {
-      for (int kp = tid / (8 * KX); kp < g.Hz; kp += kstep) {
-        if (side && (kp == 0 || 2 * kp == Lz)) continue;
-        const int kz = side ? Lz - kp : kp;
-        const int ko = kp * KX + j;
-        C* ra = ta + kz * P + s;
-        C t[9];
-#pragma unroll
-        for (int c = 0; c < 9; ++c) t[c] = ra[c * NC];
-        reflect(t, f0);
-        if (ksm) {
-          auto ld = [&](int e) { return ks[e * estr + ko]; };
-          block_mul<SYM>(ld, t);
-        } else {
-          auto ld = [&](int e) { return __ldg(kblk + e * estr + ko); };
-          block_mul<SYM>(ld, t);
-        }
-        reflect(t, f0);
-#pragma unroll
-        for (int c = 0; c < 9; ++c) ra[c * NC] = t[c];
-      }
-    }
-  }
-  __syncthreads();
-  if (line < NL && o >= 0) {
-#pragma unroll
-    for (int k = 0; k < Lz; ++k) v[k] = ta[k * P + line];
-    fft_reg<Lz, +1>(v, tw);
-#pragma unroll
-    for (int n = 0; n < Lz / 2; ++n)
-      if (n < g.Nz) W[o + n * plane] = v[n];
-  }
-  // a thread writes and reads back only its own line of the tile outside the multiply,
-  // which the barriers around it separate: the next vector needs no barrier here
-  }
-}
-
 // Compile-time KX of a power-of-two Lz (the layout's choice for an octant spectrum).
 template <typename T> constexpr int zbz_kx_ct(int L, int E) { return zbz_layout<T>(L, L / 2 + 1, 1, E, true).KX; }
 
@@ -384,6 +288,10 @@ int launch_zbz(msc_plan* pl, cx<T>* W, const int* done, int nrhs) {
   if (lay.smem > (size_t)ZBZ_SMEM_LIMIT) {
     set_error("Lz=%d exceeds the shared memory of the fused z pass", g.Lz);
     return MSC_ERR_UNSUPPORTED;
+  }
+  if constexpr (sizeof(T) == 4) {
+    const int r = launch_zpass(pl, W, done, nrhs);
+    if (r != 1) return r;
   }
   const bool sym = pl->E == 45;
   dim3 grid(g.oct ? (unsigned)lay.NXC : (unsigned)((g.Lx + 4 * lay.KX - 1) / (4 * lay.KX)),
@@ -406,36 +314,6 @@ int launch_zbz(msc_plan* pl, cx<T>* W, const int* done, int nrhs) {
       default: break;
     }
 #undef CT_CASE
-  // complex64, Lz 16 or 32: the register-resident variant. (At Lz = 64 a thread's line
-  // needs 232 registers, 2 blocks of 3 warps per SM: 397 us against 372 us for the
-  // shared-memory tiles at 256 x 256 x 32, so Lz = 64 keeps the tiles.)
-  if constexpr (sizeof(T) == 4) {
-    if (g.oct && (g.Lz == 16 || g.Lz == 32)) {
-      const void* rk = nullptr;
-      int nt = 0;
-      size_t sm = 0;
-#define REG_CASE(LZ, SY, E)                                                                            \
-  if (g.Lz == LZ && sym == SY && lay.KX == zbz_kx_ct<T>(LZ, E)) {                                        \
-    rk = (const void*)k_zbz_reg<T, LZ, zbz_kx_ct<T>(LZ, E), SY>;                                          \
-    nt = zbz_reg_threads<zbz_kx_ct<T>(LZ, E)>();                                                          \
-    sm = (lay.ksm ? sizeof(kent<T>) * (size_t)lay.CS : 0) + sizeof(cx<T>) * (LZ + (size_t)LZ * (36 * lay.KX + 1)); \
-  }
-      REG_CASE(16, true, 45)
-      REG_CASE(16, false, 81)
-      REG_CASE(32, true, 45)
-      REG_CASE(32, false, 81)
-#undef REG_CASE
-      if (rk) {
-        MSC_CUDA(prep_kernel(rk));
-        Geo gg = g;
-        ZbzLayout ll = lay;
-        void* args[] = {(void*)&W, (void*)&kh, (void*)&gg, (void*)&ll, (void*)&tw, (void*)&done, (void*)&nrhs};
-        MSC_CUDA(launch_pdl(rk, grid, dim3(nt), args, sm, pl->stream));
-        ::msc::note_launch();
-        return MSC_OK;
-      }
-    }
-  }
   if (!kern) {
 #define RT(P2)                                                                                        \
   kern = sym ? (g.oct ? (const void*)k_zbz<T, 0, 0, true, true, P2> : (const void*)k_zbz<T, 0, 0, true, false, P2>) \

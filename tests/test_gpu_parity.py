@@ -142,6 +142,41 @@ def test_matvec_compiled_lengths_vs_oracle(M, Nz, per, va):
     assert _rel(got32, want) < 1e-5
 
 
+@pytest.mark.parametrize("M,Nz,per,va", [
+    (8, 20, 1, 0),     # Lz 64 periodic, two threads per z line
+    (6, 17, 0, 1),     # Lz 64 volume averaged (one octant kx per block)
+    (10, 32, 0, 0),    # Lz 64, N_z = Lz/2
+    (9, 9, 1, 1),      # Lz 32 volume averaged, Lxy 9 (octant kx chunks ragged)
+    (13, 16, 0, 0),    # Lz 32, N_z = Lz/2, Lxy 25
+    (7, 5, 1, 0),      # Lz 16
+    (5, 3, 0, 1),      # Lz 8 volume averaged
+])
+def test_matvec_register_z_pass_vs_oracle(M, Nz, per, va):
+    """The register form of the complex64 z pass (every power-of-two Lz up to 64,
+    point and volume-averaged kernels, ragged kx chunks) against the oracle, and one
+    and three right-hand sides against each other."""
+    rng = np.random.default_rng(M * 10 + Nz)
+    g = SlabGeometry(M, Nz, 1.0)
+    mat = random_slab_material(g, REF, CONTRAST, 0.5, seed=M * 3 + Nz)
+    t4 = O.t0_scalars(OMEGA, 1.0, REF.alpha, REF.beta, REF.rho, mat.Dlambda, mat.Dmu, mat.Drho)
+    kh = O.build_slab_kernels(M, Nz, 1.0, OMEGA, REF.alpha, REF.beta, REF.rho, periodic=bool(per),
+                              volume_averaged=bool(va))
+    x = rng.standard_normal(Nz * M * M * 9) + 1j * rng.standard_normal(Nz * M * M * 9)
+    want = O.slab_matvec(x, t4, kh, M, Nz, periodic=bool(per))
+    plan = SlabPlan(g, REF, periodic=bool(per))
+    plan.build_t0(mat, OMEGA)
+    plan.build_g0(OMEGA, volume_averaged=bool(va))
+    xt = torch.from_numpy(x.reshape(Nz, M, M, 9))
+    got32 = plan.matvec(xt, "complex64").cpu().numpy().ravel()
+    assert _rel(got32, want) < 5e-6
+    x3 = torch.stack([xt, 2j * xt, xt.conj()]).to(torch.complex64)
+    y3 = plan.matvec_multi(x3.permute(0, 4, 1, 2, 3).contiguous().to(plan.device), "complex64")
+    for r in range(3):
+        want_r = O.slab_matvec(x3[r].numpy().astype(np.complex128).ravel(), t4, kh, M, Nz, periodic=bool(per))
+        assert _rel(y3[r].permute(1, 2, 3, 0).cpu().numpy().ravel(), want_r) < 5e-6
+    plan.close()
+
+
 @pytest.mark.parametrize("M,Nz,Lxy,va", [
     (32, 5, 64, 0),    # M = L/2
     (30, 4, 64, 0),    # M < L/2, not a multiple of 4 (warps holding rows inside and outside the lattice)
