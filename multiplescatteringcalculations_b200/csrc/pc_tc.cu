@@ -225,9 +225,10 @@ __global__ void __launch_bounds__(TV_THREADS, 2)
     k_nf_tc(const float2* __restrict__ x, const double* scale, const float2* __restrict__ t4, float2* __restrict__ h,
             float2* __restrict__ acc, float2 ch, float2 c0, int init, const uint4* __restrict__ Bg, Geo g, int zc,
             const int* done, int* status, long long wait_limit, int inject_wait) {
-  pdl_wait();
-  pdl_trigger();
-  if (done && *done) return;
+  // Launched as a programmatic dependent of the previous layer: everything up to
+  // pdl_wait() (barrier set-up, tensor-memory allocation, the bulk copy of this layer's
+  // weights, which no kernel writes) overlaps the previous kernel's tail; the halo
+  // planes, x, acc, the scale and the done flag are read only after it.
   // The operands start on a 1024-byte boundary of the shared address space (with a 128-byte
   // static block ahead of the dynamic window, the MMA read its operands 16 bytes before
   // their start).
@@ -272,7 +273,6 @@ __global__ void __launch_bounds__(TV_THREADS, 2)
   tl.x0 = (col / nty) * TV_TX;
   tl.z0 = chunk * zc;
   tl.zc = min(zc, g.Nz - tl.z0);
-  const float s = scale ? (float)(*scale) : 1.f;
   if (warp == 8 && lane == 0) {
     // the layer's packed weights: one bulk copy into shared memory, completed on mb_w
     asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(mb_w), "r"(TV_B_BYTES)
@@ -282,6 +282,20 @@ __global__ void __launch_bounds__(TV_THREADS, 2)
         "l"(Bg), "r"(TV_B_BYTES), "r"(mb_w)
         : "memory");
   }
+  pdl_wait();
+  pdl_trigger();
+  if (done && *done) {
+    // nothing to compute: the weights' copy lands before the shared memory and the
+    // tensor memory are given back
+    if (warp == 8 && lane == 0) mbar_drain(mb_w, 0u, status);
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+    if (warp == 8)
+      asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(*tmem_slot), "r"(2 * TV_N)
+                   : "memory");
+    return;
+  }
+  const float s = scale ? (float)(*scale) : 1.f;
   // planes of the layers z0 - 1, z0, z0 + 1 (plane p of the chunk, layer z0 + p, lives in
   // slot (p + 1) & 3), staged by all 288 threads (the MMA warp has nothing to issue yet),
   // each thread's rows' loads in flight at once
@@ -486,10 +500,15 @@ int launch_nf_tc(msc_plan* pl, const float2* x, const double* scale, const float
   MSC_CUDA(prep_kernel((const void*)k_nf_tc));
   int* status = (int*)pl->status.p;
   const long long limit = pl->wait_limit > 0 ? pl->wait_limit : TV_WAIT_LIMIT;
-  k_nf_tc<<<nb, TV_THREADS, TV_SMEM, pl->stream>>>(x, scale, t4, h, acc, ch, c0, init, (const uint4*)Bpacked, g, zc,
-                                                   done, status, limit, pl->inject_wait);
+  const uint4* Bg = (const uint4*)Bpacked;
+  Geo gg = g;
+  int zcc = zc, inj = pl->inject_wait;
+  long long lim = limit;
+  void* args[] = {(void*)&x,  (void*)&scale, (void*)&t4,     (void*)&h,      (void*)&acc, (void*)&ch, (void*)&c0,
+                  (void*)&init, (void*)&Bg,  (void*)&gg,     (void*)&zcc,    (void*)&done, (void*)&status,
+                  (void*)&lim, (void*)&inj};
+  MSC_CUDA(launch_pdl((const void*)k_nf_tc, dim3((unsigned)nb), dim3(TV_THREADS), args, TV_SMEM, pl->stream));
   ::msc::note_launch();
-  MSC_CUDA(cudaGetLastError());
   return MSC_OK;
 }
 
