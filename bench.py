@@ -1113,8 +1113,16 @@ def main(argv=None) -> int:
                          "blocks and with BF16 blocks on the tensor cores (for kernel profiles)")
     ap.add_argument("--matvec-only", type=int, default=0, metavar="N",
                     help="build the plan and run N complex64 matvecs through msc_matvec (for kernel profiles)")
+    ap.add_argument("--lattice", default=None, metavar="M,N_Z",
+                    help="with --matvec-only or --precond-only: the workload's material and frequency on an "
+                         "M x M x N_z lattice (kernel profiles at sizes a full ncu capture can hold)")
     args = ap.parse_args(argv)
     wl = WORKLOADS[args.workload]
+    if args.lattice:
+        if not (args.matvec_only or args.precond_only):
+            raise SystemExit("--lattice applies to --matvec-only and --precond-only only")
+        m, nz = (int(v) for v in args.lattice.split(","))
+        wl = dict(wl, M=m, N_z=nz)
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
