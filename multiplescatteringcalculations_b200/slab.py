@@ -521,6 +521,15 @@ _HOST_POOL: list = []   # entries [ndarray, pinned tensor or None]
 _HOST_POOL_SIZE = 8
 _PINNED_MAX = 6
 _HOST_POOL_LOCK = threading.Lock()
+_COPY_STREAMS: dict = {}  # device index -> side stream for result copies that overlap the solve
+
+
+def _copy_stream(device: torch.device) -> torch.cuda.Stream:
+    i = device.index if device.index is not None else torch.cuda.current_device()
+    st = _COPY_STREAMS.get(i)
+    if st is None:
+        st = _COPY_STREAMS[i] = torch.cuda.Stream(device=device)
+    return st
 
 
 def _host_array(shape: tuple):
@@ -661,6 +670,19 @@ def compute_slab_scattering_gpu(
     plan.build_t0(material, omega)
     plan.build_g0(omega, kpar=kp, volume_averaged=volume_averaged, n_orders=n_orders)
     psi0 = plan.incident(omega, k_hat, wave_type)
+    t4 = plan.t0_scalars()
+    # psi0 and T0 are final before the solve: their device -> host copies into page-locked
+    # result arrays run on a side stream while GMRES runs (a result array that is not
+    # page-locked is copied after the solve)
+    cur = torch.cuda.current_stream(plan.device)
+    side = _copy_stream(plan.device)
+    side.wait_stream(cur)
+    early = [_host_array(tuple(t.shape)) for t in (psi0, t4)]
+    with torch.cuda.stream(side):
+        for (h, ht), t in zip(early, (psi0, t4)):
+            if ht is not None:
+                ht.copy_(t, non_blocking=True)
+                t.record_stream(side)
     if pc_mode is not None:
         if hasattr(preconditioner, "install"):
             preconditioner.install(plan)
@@ -675,19 +697,19 @@ def compute_slab_scattering_gpu(
             f"GPU GMRES did not converge: rel_res={st['residual']:.2e} after {st['n_matvec']} matvecs",
             stacklevel=2,
         )
-    t4 = plan.t0_scalars()
-    # device -> host into fresh numpy arrays that the result owns. numpy asks for
-    # transparent huge pages on large arrays, so the first touch costs a few faults per
-    # array instead of one per 4 KB page (23 MB at cfg2: 1.4 ms against 10 ms with
-    # torch.empty). Pinned buffers copy faster but results kept alive by the caller
-    # would each hold one, and every new block is a cudaHostAlloc of ~16 ms.
-    host = [_host_array(tuple(t.shape)) for t in (x, psi0, t4)]
-    for (h, ht), t in zip(host, (x, psi0, t4)):
+    # device -> host into result arrays from a small recycled pool: the first few are
+    # page-locked (asynchronous copies), the others plain numpy arrays, which ask for
+    # transparent huge pages, so the first touch costs a few faults per array instead of
+    # one per 4 KB page. A result array the caller still holds is never reused.
+    host = [_host_array(tuple(x.shape))] + early
+    for i, ((h, ht), t) in enumerate(zip(host, (x, psi0, t4))):
         if ht is not None:
-            ht.copy_(t, non_blocking=True)
+            if i == 0:
+                ht.copy_(t, non_blocking=True)
         else:
             torch.from_numpy(h).copy_(t)
-    torch.cuda.current_stream(plan.device).synchronize()
+    cur.synchronize()
+    side.synchronize()
     psi_h, psi0_h, t4_h = (h for h, _ in host)
     res = SlabResult(
         psi=psi_h,
