@@ -461,8 +461,9 @@ def cfg4_sample(dev, seeds=CFG4_SAMPLE_SEEDS, tol: float = 1e-8) -> dict:
 
 
 CFG5_BUDGETS = (100, 300, 1000)
-CFG5_MILD_STD = 0.15  # the converging companion of cfg5
-CFG5_MILD_MAXIT = 4000
+CFG5_MILD_STD = 0.15  # the ka 0.5 companion of cfg5
+CFG5_MILD_KA = 0.5
+CFG5_MILD_MAXIT = 1000
 
 
 def run_cfg5(args, wl, local_rank) -> int:
@@ -519,8 +520,10 @@ def run_cfg5(args, wl, local_rank) -> int:
                              "ms_per_matvec": ms / max(1, st["n_matvec"]), "pc_cycles": st["pc_cycles"],
                              "plain_cycles": st["plain_cycles"]})
             hist[name] = rows
-    # The same lattice, frequency and incidence at a contrast restarted GMRES does solve
-    # (GRF std 15 %): time to the workload's tolerance per solver setting.
+    # The same lattice and incidence at the 64 x 64 x 16 workload's frequency and contrast
+    # (ka 0.5, GRF std 15 %): per solver setting the time and residual at an equal matvec
+    # budget (this periodic 256 x 256 x 32 slab does not reach the tolerance within it
+    # either; at ka 1 it stalls at std 15 % as at 40 %).
     mild = {}
     with ClockSampler(local_rank) as clk_mild:
         from multiplescatteringcalculations_b200 import gaussian_random_field_material
@@ -528,12 +531,13 @@ def run_cfg5(args, wl, local_rank) -> int:
         m2 = gaussian_random_field_material(geom, ref, correlation_length=wl["mat"][1], std=CFG5_MILD_STD, seed=1000)
         m2d = type(m2)(torch.from_numpy(m2.Dlambda).to(dev), torch.from_numpy(m2.Dmu).to(dev),
                        torch.from_numpy(m2.Drho).to(dev), ref)
+        om2 = CFG5_MILD_KA * BETA / A
         for name, (prec, pc) in variants.items():
             torch.cuda.synchronize()
             e0.record(plan.stream)
-            plan.build_t0(m2d, omega)
-            plan.build_g0(omega)
-            b2 = plan.incident(omega, k_hat, wl["wave"])
+            plan.build_t0(m2d, om2)
+            plan.build_g0(om2)
+            b2 = plan.incident(om2, k_hat, wl["wave"])
             if pc is not None:
                 pc(plan)
             x, st = plan.solve(b2, tol=wl["tol"], max_iter=CFG5_MILD_MAXIT, restart=30, precision=prec,
@@ -554,8 +558,9 @@ def run_cfg5(args, wl, local_rank) -> int:
         "config": {"workload": "cfg5", **_cfg_desc(wl), "fft": list(plan.fft_sizes()), "unknowns": 9 * geom.N_z * geom.M ** 2},
         "gpu_launches": int(launches), "setup_ms": ms_setup, "roofline": roof, "converged": converged,
         "residual_history": hist, "clocks": clk.summary(),
-        "converging_companion": {"material": ["grf", wl["mat"][1], CFG5_MILD_STD],
-                                 "note": "same lattice, ka and incidence; T0, G0, incident and solve timed",
+        "companion_ka05": {"material": ["grf", wl["mat"][1], CFG5_MILD_STD], "ka": CFG5_MILD_KA,
+                           "max_matvec": CFG5_MILD_MAXIT,
+                           "note": "same lattice and incidence; T0, G0, incident and solve timed",
                                  "solves": mild, "clocks": clk_mild.summary()},
     }
     print(json.dumps(line), flush=True)
