@@ -17,7 +17,10 @@ int run(msc_plan* pl, float2* W, const int* done, int nrhs, int nxc) {
   const float2* tw = (const float2*)pl->tw32_z.p;
   Geo gg = g;
   int nx = nxc;
-  void* args[] = {(void*)&W, (void*)&kh, (void*)&gg, (void*)&nx, (void*)&tw, (void*)&done, (void*)&nrhs};
+  int* status = (int*)pl->status.p;
+  long long lim = pl->wait_limit > 0 ? pl->wait_limit : ZP_WAIT_LIMIT;
+  void* args[] = {(void*)&W,    (void*)&kh,   (void*)&gg,     (void*)&nx, (void*)&tw,
+                  (void*)&done, (void*)&nrhs, (void*)&status, (void*)&lim};
   MSC_CUDA(launch_pdl(kern, dim3((unsigned)nxc, (unsigned)g.Hy), dim3(Cf::NT), args, Cf::SMEM, pl->stream));
   ::msc::note_launch();
   return MSC_OK;

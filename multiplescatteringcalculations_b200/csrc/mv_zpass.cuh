@@ -13,10 +13,14 @@
 //
 // Phases: (1) each thread loads its line's N_z layers from W straight into
 // registers (the two threads of a line are adjacent lanes, so their loads coalesce
-// into one request) while the block stages its slice of the spectrum in shared
-// memory; (2) transform, spectrum rows to the tile; (3) the block multiply, one
+// into one request) while one bulk copy (cp.async.bulk, completing on an mbarrier)
+// brings the block's contiguous slice of the spectrum into shared memory; (2) transform,
+// spectrum rows to the tile; (3) once the slice has landed, the block multiply, one
 // wavevector per item, every offset into the staged slice a compile-time constant;
-// (4) the inverse transform from the tile, the N_z layers back to W.
+// (4) the inverse transform from the tile, the N_z layers back to W. The wait for the
+// slice is bounded (the plan's wait limit): when it runs out the kernel records a
+// timeout in the plan's status word and finishes without the slice; before the block
+// exits its first thread waits, with a fixed limit, for the copy to land.
 //
 // Measured alternatives that lost (B200, 64x64x16 and 256x256x32): the slice staged
 // pre-broadcast (re, re, im, im) to save the operand moves (two blocks per SM instead
@@ -52,10 +56,24 @@ template <int LZ, int KX, int S, bool SYM> struct ZpCfg {
   static constexpr int MINB = AUTO < 1 ? 1 : AUTO;
 };
 
+constexpr long long ZP_WAIT_LIMIT = 1ll << 22;  // mbarrier polls before a timeout is recorded
+
+__device__ __forceinline__ bool zp_try_wait(uint32_t addr, uint32_t phase) {
+  uint32_t ok = 0;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}\n"
+      : "=r"(ok)
+      : "r"(addr), "r"(phase)
+      : "memory");
+  return ok != 0;
+}
+
 template <int LZ, int KX, int S, bool SYM>
 __global__ void __launch_bounds__(ZpCfg<LZ, KX, S, SYM>::NT, ZpCfg<LZ, KX, S, SYM>::MINB)
     k_zpass(float2* __restrict__ W, const float2* __restrict__ khat, Geo g, int nxc, const float2* __restrict__ twg,
-            const int* done, int nrhs) {
+            const int* done, int nrhs, int* status, long long wait_limit) {
   using Cf = ZpCfg<LZ, KX, S, SYM>;
   constexpr int NC = Cf::NC, NL = Cf::NL, NT = Cf::NT, LH = Cf::LH, HZ = Cf::HZ, P = Cf::P;
   pdl_wait();
@@ -63,6 +81,7 @@ __global__ void __launch_bounds__(ZpCfg<LZ, KX, S, SYM>::NT, ZpCfg<LZ, KX, S, SY
   if (done && *done) return;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ int sq[NC];  // mirror flags of slot s (bit 0 kx, bit 1 ky), -1: slot unused
+  __shared__ __align__(8) unsigned long long kbar;  // completion of the slice's bulk copy
   float2* tw = reinterpret_cast<float2*>(smem_raw + Cf::TW_OFF);
   float2* tile = tw + LZ;
   const int tid = threadIdx.x;
@@ -91,18 +110,28 @@ __global__ void __launch_bounds__(ZpCfg<LZ, KX, S, SYM>::NT, ZpCfg<LZ, KX, S, SY
     if (col >= 0) o0 = (l / NC) * cstride + col;
   }
   if (tid < NC) sq[tid] = slot_col(tid) >= 0 ? tid / KX : -1;
+  const uint32_t kbar_a = (uint32_t)__cvta_generic_to_shared(&kbar);
+  if (tid == 0) {
+    // the slice: CS entries, 16-byte aligned at both ends (zbz_layout pads CS to even)
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(kbar_a) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(kbar_a), "r"((int)(8 * Cf::CS))
+                 : "memory");
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(
+                     (uint32_t)__cvta_generic_to_shared(smem_raw)),
+                 "l"(kblk), "r"((int)(8 * Cf::CS)), "r"(kbar_a)
+                 : "memory");
+  }
+  bool kready = false;
   for (int rh = 0; rh < nrhs; ++rh) {
     const long long o = o0 >= 0 ? o0 + (long long)rh * 9 * cstride : -1;
     float2 v[LH];
     // (1) the line's layers n < N_z <= Lz/2; the upper half of an S = 1 line is zero
 #pragma unroll
     for (int n = 0; n < LH; ++n) v[n] = (n < LZ / 2 && o >= 0 && n < g.Nz) ? W[o + n * plane] : czero<float2>();
-    if (rh == 0) {
-      for (int i = tid; i < Cf::CS / 2; i += NT) cp_async16(smem_raw + 16 * i, kblk + 2 * i);
+    if (rh == 0)
       for (int t = tid; t < LZ; t += NT) tw[t] = twg[t];
-      cp_async_wait_all();
-    }
-    // the previous vector's inverse reads of the tile are done; the slice is staged
+    // the previous vector's inverse reads of the tile are done; the barrier's init visible
     __syncthreads();
     // (2) forward transform, rows kz = S m + b of the tile
     if (S == 2 && b) {
@@ -113,6 +142,10 @@ __global__ void __launch_bounds__(ZpCfg<LZ, KX, S, SYM>::NT, ZpCfg<LZ, KX, S, SY
     if (lact) {
 #pragma unroll
       for (int m = 0; m < LH; ++m) tile[(S * m + b) * P + l] = v[m];
+    }
+    if (rh == 0) {
+      for (long long it = 0; it < wait_limit && !kready; ++it) kready = zp_try_wait(kbar_a, 0u);
+      if (!kready && status) atomicExch(status, 1);
     }
     __syncthreads();
     // (3) block multiply. Item (j, q, kpa, side, kph), j fastest: the point kz = kp
@@ -169,6 +202,12 @@ __global__ void __launch_bounds__(ZpCfg<LZ, KX, S, SYM>::NT, ZpCfg<LZ, KX, S, SY
         if ((S == 2 || m < LZ / 2) && n < g.Nz) W[o + n * plane] = v[m];
       }
     }
+  }
+  // a wait that ran out: the bulk copy still lands before the block's shared memory is
+  // given back
+  if (tid == 0 && !kready) {
+    for (long long it = 0; it < ZP_WAIT_LIMIT && !kready; ++it) kready = zp_try_wait(kbar_a, 0u);
+    if (!kready && status) atomicExch(status, 1);
   }
 }
 
