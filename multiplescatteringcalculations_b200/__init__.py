@@ -31,7 +31,13 @@ from .slab import (  # noqa: F401
     uniform_slab_material,
 )
 
-from .learned import NearFieldPreconditioner, fgmres_matvecs, solver_residuals, train_nearfield  # noqa: F401,E402
+from .learned import (  # noqa: F401,E402
+    NearFieldPreconditioner,
+    fgmres_matvecs,
+    solver_residuals,
+    train_nearfield,
+    train_nearfield_stream,
+)
 from .sphere import SphereDecompositionResult, compute_sphere_foldy_lax_fft_gpu, sphere_grid  # noqa: F401,E402
 
 __version__ = "0.1.0"

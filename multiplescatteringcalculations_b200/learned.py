@@ -36,6 +36,7 @@ __all__ = [
     "NearFieldPreconditioner",
     "solver_residuals",
     "train_nearfield",
+    "train_nearfield_stream",
     "fgmres_matvecs",
 ]
 
@@ -104,10 +105,12 @@ def solver_residuals(plan: SlabPlan, b: torch.Tensor, iterations=(2, 5, 10, 20, 
 
 
 def fgmres_matvecs(problems, preconditioner, *, tol: float = 1e-8, max_iter: int = 3000,
-                   precision: str = "mixed") -> list[int]:
+                   precision: str = "mixed", policy: str = "adaptive") -> list[int]:
     """Operator applications of the solve of each problem to ``tol`` with the given
     preconditioner (None: plain GMRES; "nearfield": the Neumann polynomial; a
-    NearFieldPreconditioner). A solve that does not converge counts ``max_iter``."""
+    NearFieldPreconditioner) under the cycle policy ``policy`` ("adaptive", whose choices
+    depend on measured cycle times, or "always", deterministic). A solve that does not
+    converge counts ``max_iter``."""
     out = []
     for p in problems:
         import warnings
@@ -116,7 +119,7 @@ def fgmres_matvecs(problems, preconditioner, *, tol: float = 1e-8, max_iter: int
             warnings.simplefilter("ignore")
             r = compute_slab_scattering_gpu(p.geometry, p.material, p.omega, p.k_hat, p.wave_type, gmres_tol=tol,
                                             max_iter=max_iter, precision=precision, periodic=p.periodic,
-                                            preconditioner=preconditioner)
+                                            preconditioner=preconditioner, pc_policy=policy)
         out.append(int(r.n_gmres_iter) if r.gmres_residual <= tol else int(max_iter))
     return out
 
@@ -165,3 +168,65 @@ def train_nearfield(train, validation=(), *, degree: int = 4, lr: float = 1e-4, 
             return kept
         net.history.append({"selected": "trained"})
     return net
+
+
+def train_nearfield_stream(problems, validation=(), *, n_pairs: int = 20000, degree: int = 4, lr: float = 3e-5,
+                           iterations=(2, 4, 8, 16, 32, 64), steps_per_residual: int = 1, check_every: int = 500,
+                           init: NearFieldPreconditioner | None = None, tol: float = 1e-8, max_iter: int = 3000,
+                           policy: str = "adaptive", verbose: bool = False) -> NearFieldPreconditioner:
+    """Train the learned near-field preconditioner on a stream of solver-generated
+    residuals, at a scale whose residuals could not all be held at once (20 000
+    residuals of a 64 x 64 x 16 slab are 94 GB in complex64).
+
+    ``problems`` is an iterable of BatchProblem (a generator is fine). For each slab the
+    residuals of FP64 GMRES after each count in ``iterations`` are generated on the
+    device, ``steps_per_residual`` Adam steps are taken per residual, and the residuals
+    are dropped; the stream stops after ``n_pairs`` residuals. Every ``check_every``
+    residuals, and at the end, the network is scored on the validation slabs (FGMRES
+    operator applications to ``tol`` under the cycle policy ``policy``); the best-scoring network seen,
+    the starting one included, is returned (model selection), with ``history`` holding
+    the losses and the validation scores."""
+    net = (init or NearFieldPreconditioner(degree)).copy()
+    best = (None, -1, net.copy())
+    scores = []
+
+    def score(tag):
+        nonlocal best
+        if not validation:
+            return
+        s = sum(fgmres_matvecs(validation, net, tol=tol, max_iter=max_iter, policy=policy))
+        scores.append((tag, s))
+        if verbose:
+            print(f"pairs {tag}: validation matvecs {s}", flush=True)
+        if best[0] is None or s < best[0]:
+            best = (s, tag, net.copy())
+
+    score(0)
+    losses = []
+    seen = 0
+    next_check = check_every
+    for p in problems:
+        if seen >= n_pairs:
+            break
+        if p.bloch:
+            raise ValueError("training slabs must not carry a Bloch phase")
+        plan = _plan_for(p)
+        plan.build_t0(p.material, p.omega)
+        plan.build_g0(p.omega)
+        b = plan.incident(p.omega, p.k_hat, p.wave_type)
+        res = solver_residuals(plan, b, iterations)
+        res = res[: max(0, n_pairs - seen)]
+        net.coef, net.w, net.adam, ls = plan.nf_train(res, net.coef, net.w, net.adam,
+                                                      int(res.shape[0]) * int(steps_per_residual), lr)
+        losses.extend(ls.tolist())
+        seen += int(res.shape[0])
+        del res
+        if seen >= next_check:
+            score(seen)
+            next_check += check_every
+    if not scores or scores[-1][0] != seen:
+        score(seen)
+    sel = best[2] if validation else net.copy()
+    sel.history = [{"losses": losses, "pairs": seen}, {"validation": scores},
+                   {"selected_at_pairs": best[1] if validation else seen}]
+    return sel
