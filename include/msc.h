@@ -57,7 +57,11 @@ typedef struct msc_slab_desc {
   double rho;        /* background density (ReferenceMedium.rho) */
   int32_t periodic;  /* 1 = circular convolution over M x M (reference periodic=True) */
   int32_t Lz;        /* padded z FFT length, 0 = automatic (>= 2 N_z - 1) */
-  int32_t Lxy;       /* padded lateral FFT length, 0 = automatic (>= 2M - 1; ignored if periodic) */
+  int32_t Lxy;       /* padded lateral FFT length (>= 2M - 1; ignored if periodic): 0 = automatic (the
+                        smallest 2,3,5,7-smooth length, or the next power of two when that is at
+                        most 1/16 longer); -1 = autotuned: of the smallest smooth length and the
+                        next power of two, the one whose complex64 operator runs faster on the
+                        current device, timed once per device and lattice shape in the process */
 } msc_slab_desc;
 
 typedef struct msc_solve_opts {
@@ -266,7 +270,8 @@ typedef struct msc_batch_item {
 /* Solve n independent slabs (uneven sizes, frequencies and incidences) on the
  * current device: T0 and G0 builds, incident field, solve with opts, R_PP and the
  * field, per item. `workers` host threads with a stream and a plan cache each run
- * items concurrently (0 = choose by timing the first items at 1, 2 and 4 workers;
+ * items concurrently (0 = choose by timing the first items at 1, 2 and 4 workers, and
+ * autotune the lateral FFT length of aperiodic items whose Lxy is 0, as Lxy = -1 does;
  * the count used is written to *workers_used when not NULL). Returns MSC_OK when
  * every item converged, MSC_NOT_CONVERGED when any item failed or did not converge
  * (its own status and message say which), negative only for errors of the call

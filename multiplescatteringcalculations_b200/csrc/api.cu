@@ -5,6 +5,8 @@
 #include <mutex>
 #include <cstdio>
 #include <cstring>
+#include <map>
+#include <tuple>
 
 #include "mv_common.cuh"
 #include "pc.cuh"
@@ -171,6 +173,91 @@ int read_status(msc_plan* pl, int* word) {
 
 using namespace msc;
 
+extern "C" int msc_plan_create(const msc_slab_desc* d, void* stream, msc_plan** out);
+
+namespace msc {
+namespace {
+
+// Microseconds per complex64 operator application of the descriptor's lattice padded to
+// L laterally: a throwaway plan with a zero spectrum and zero T0 (the kernels' timing does
+// not depend on the values), 2 untimed and 5 timed applications on the plan's stream.
+// Negative when the plan cannot be built.
+double time_lateral(const msc_slab_desc* d, int L, void* stream) {
+  msc_slab_desc dd = *d;
+  dd.Lxy = L;
+  msc_plan* t = nullptr;
+  if (msc_plan_create(&dd, stream, &t) != MSC_OK) return -1.0;
+  double us = -1.0;
+  const Geo& g = t->g;
+  DBuf x, y;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  t->E = 45;
+  bool ok = dalloc(t, t->khat32, sizeof(float2) * khat_elems_t<float>(g, 45)) == MSC_OK &&
+            dalloc(t, t->t4_32, sizeof(float2) * 4 * (size_t)g.nsite) == MSC_OK &&
+            dalloc(t, x, sizeof(float2) * field_elems(g)) == MSC_OK &&
+            dalloc(t, y, sizeof(float2) * field_elems(g)) == MSC_OK &&
+            cudaMemsetAsync(t->khat32.p, 0, t->khat32.bytes, t->stream) == cudaSuccess &&
+            cudaMemsetAsync(t->t4_32.p, 0, t->t4_32.bytes, t->stream) == cudaSuccess &&
+            cudaMemsetAsync(x.p, 0, x.bytes, t->stream) == cudaSuccess &&
+            cudaEventCreate(&e0) == cudaSuccess && cudaEventCreate(&e1) == cudaSuccess;
+  if (ok) {
+    t->has_t0 = t->has_g0 = true;
+    for (int i = 0; i < 7 && ok; ++i) {
+      if (i == 2) ok = cudaEventRecord(e0, t->stream) == cudaSuccess;
+      if (ok) ok = launch_matvec<float>(t, (const float2*)x.p, nullptr, (float2*)y.p, nullptr) == MSC_OK;
+    }
+    float ms = 0.f;
+    if (ok && cudaEventRecord(e1, t->stream) == cudaSuccess && cudaEventSynchronize(e1) == cudaSuccess &&
+        cudaEventElapsedTime(&ms, e0, e1) == cudaSuccess)
+      us = 1e3 * ms / 5.0;
+  }
+  cudaGetLastError();
+  if (e0) cudaEventDestroy(e0);
+  if (e1) cudaEventDestroy(e1);
+  dfree(t, x);
+  dfree(t, y);
+  msc_plan_destroy(t);
+  return us;
+}
+
+std::mutex g_tune_mu;
+std::map<std::tuple<int, int, int, int>, int> g_tune;  // (device, M, N_z, Lz) -> lateral length
+
+}  // namespace
+
+// The autotuned lateral FFT length of an aperiodic plan (descriptor Lxy = -1): the
+// smallest 2,3,5,7-smooth length >= 2M - 1 or the next power of two, whichever runs the
+// complex64 operator faster on this device (the power of two takes the compile-time,
+// register and fused plane kernels; the smooth length moves less data). Timed once per
+// device and lattice shape in the process and remembered.
+int tuned_lateral(const msc_slab_desc* d, int Lz, void* stream) {
+  const int n = 2 * d->M - 1;
+  const int p2 = pow2_at_least(n);
+  int smooth = n;
+  for (;; ++smooth) {
+    int r = smooth;
+    for (int p : {2, 3, 5, 7})
+      while (r % p == 0) r /= p;
+    if (r == 1) break;
+  }
+  if (smooth == p2) return p2;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  const auto key = std::make_tuple(dev, d->M, d->N_z, Lz);
+  {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    auto it = g_tune.find(key);
+    if (it != g_tune.end()) return it->second;
+  }
+  const double ts = time_lateral(d, smooth, stream), tp = time_lateral(d, p2, stream);
+  const int pick = (tp > 0 && (ts <= 0 || tp < ts)) ? p2 : smooth;
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  g_tune[key] = pick;
+  return pick;
+}
+
+}  // namespace msc
+
 extern "C" {
 
 const char* msc_status_string(int s) {
@@ -234,7 +321,12 @@ int msc_plan_create(const msc_slab_desc* d, void* stream, msc_plan** out) {
   int Lxy;
   if (d->periodic) Lxy = d->M;
   else {
-    Lxy = d->Lxy > 0 ? d->Lxy : nice_length(2 * d->M - 1);
+    if (d->Lxy < -1) {
+      delete pl;
+      set_error("Lxy must be >= -1 (-1: autotuned, 0: automatic), got %d", d->Lxy);
+      return MSC_ERR_INVALID;
+    }
+    Lxy = d->Lxy > 0 ? d->Lxy : d->Lxy == -1 ? tuned_lateral(d, Lz, stream) : nice_length(2 * d->M - 1);
     if (Lxy < 2 * d->M - 1) {
       delete pl;
       set_error("Lxy=%d is below 2*M-1=%d", Lxy, 2 * d->M - 1);

@@ -13,7 +13,9 @@
 // the device by DMA into one of the worker's two page-locked buffers; a copier thread
 // moves it into the caller's array while the workers carry on. With workers = 0 an
 // online autotuner times the first items at 1, 2 and 4 workers and finishes the batch
-// with the fastest. Items are independent: a failed item records its status and the
+// with the fastest, and the lateral FFT length of each aperiodic shape is autotuned (the
+// smallest 2,3,5,7-smooth length or the next power of two, timed once per shape:
+// msc_slab_desc.Lxy = -1). Items are independent: a failed item records its status and the
 // others continue.
 #include <algorithm>
 #include <atomic>
@@ -130,6 +132,7 @@ struct Copier {
 };
 
 struct Worker {
+  bool tune_fft = false;  // workers = 0: the lateral FFT length of aperiodic plans is autotuned
   cudaStream_t stream = nullptr;
   int device = 0;
   int index = 0;
@@ -212,7 +215,9 @@ struct Worker {
       plans.erase(it);
     }
     msc_plan* p = nullptr;
-    const int s = msc_plan_create(&d, stream, &p);
+    msc_slab_desc dd = d;
+    if (tune_fft && !dd.periodic && dd.Lxy == 0) dd.Lxy = -1;  // autotuned lateral FFT length
+    const int s = msc_plan_create(&dd, stream, &p);
     if (s != MSC_OK) return s;
     // a batch item is one short solve on a plan that is rarely reused: capturing and
     // instantiating its GMRES cycles costs more than it saves
@@ -352,7 +357,10 @@ extern "C" int msc_batch_solve(msc_batch_item* items, int n, const msc_solve_opt
   const int maxw = workers > 0 ? workers : 4;
   Copier copier(device);
   std::vector<Worker> pool(maxw);
-  for (int i = 0; i < maxw; ++i) MSC_TRY(pool[i].init(device, i, &copier));
+  for (int i = 0; i < maxw; ++i) {
+    MSC_TRY(pool[i].init(device, i, &copier));
+    pool[i].tune_fft = workers == 0;
+  }
   std::atomic<int> next{0};
   int chosen = workers;
   if (workers == 0) {

@@ -177,10 +177,14 @@ def _ptr(t: torch.Tensor) -> int:
 
 class SlabPlan:
     """Owns a native plan (FFT sizes, T0, G0 spectrum, workspaces) for one slab
-    geometry and background medium on one CUDA device."""
+    geometry and background medium on one CUDA device. ``Lxy`` (aperiodic only): the
+    padded lateral FFT length, 0 for the automatic rule, "auto" (or -1) for the timed
+    choice between the smallest 2,3,5,7-smooth length and the next power of two."""
 
     def __init__(self, geometry: SlabGeometry, ref: ReferenceMedium, *, periodic: bool = False, device=None,
-                 Lz: int = 0, Lxy: int = 0):
+                 Lz: int = 0, Lxy: int | str = 0):
+        if Lxy == "auto":
+            Lxy = -1
         self.lib = N.load()
         self.geometry = geometry
         self.ref = ref

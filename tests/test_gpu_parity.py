@@ -482,3 +482,33 @@ def test_complex64_matvec_large_planes(M, Nz, periodic):
         assert _rel(y64, want) < 1e-10
         assert _rel(y32, want) < 5e-6
     plan.close()
+
+
+def test_autotuned_lateral_length():
+    """Lxy="auto" (-1 in the C descriptor): the plan takes the smallest 2,3,5,7-smooth
+    length >= 2M - 1 or the next power of two, whichever runs the complex64 operator
+    faster; the choice is remembered for the shape, and the operator matches the oracle
+    either way. Values below -1 are refused; periodic plans keep Lxy = M."""
+    M, Nz = 24, 6
+    g = SlabGeometry(M, Nz, 1.0)
+    mat = random_slab_material(g, REF, CONTRAST, 0.5, seed=11)
+    plan = SlabPlan(g, REF, Lxy="auto")
+    L = plan.fft_sizes()[1]
+    assert L in (48, 64)
+    again = SlabPlan(g, REF, Lxy="auto")
+    assert again.fft_sizes()[1] == L
+    again.close()
+    plan.build_t0(mat, OMEGA)
+    plan.build_g0(OMEGA)
+    rng = np.random.default_rng(5)
+    x = rng.standard_normal(Nz * M * M * 9) + 1j * rng.standard_normal(Nz * M * M * 9)
+    t4 = O.t0_scalars(OMEGA, 1.0, REF.alpha, REF.beta, REF.rho, mat.Dlambda, mat.Dmu, mat.Drho)
+    kh = O.build_slab_kernels(M, Nz, 1.0, OMEGA, REF.alpha, REF.beta, REF.rho)
+    want = O.slab_matvec(x, t4, kh, M, Nz)
+    xt = torch.from_numpy(x.reshape(Nz, M, M, 9))
+    assert _rel(plan.matvec(xt, "complex128").cpu().numpy().ravel(), want) < 1e-12
+    assert _rel(plan.matvec(xt, "complex64").cpu().numpy().ravel(), want) < 5e-6
+    plan.close()
+    with pytest.raises(ValueError):
+        SlabPlan(g, REF, Lxy=-2)
+    assert SlabPlan(SlabGeometry(8, 2, 1.0), REF, periodic=True, Lxy="auto").fft_sizes()[1] == 8
