@@ -624,7 +624,8 @@ def run_ours(args, wl, rank, world, local_rank):
         if rank == 0:
             print(json.dumps({"metric": METRIC, "value": value, "unit": "solves/s", "ms_per_step": ms_max / args.steps,
                               "solve": {k: (v if not isinstance(v, complex) else [v.real, v.imag])
-                                        for k, v in stats.items()}, "gpu_launches": int(launches)}), flush=True)
+                                        for k, v in stats.items() if k != "x"},
+                              "gpu_launches": int(launches)}), flush=True)
         plan.close()
         return 0
 
