@@ -125,7 +125,7 @@ __global__ void __launch_bounds__(256) k_fft_rows_reg(const float2* __restrict__
     const int n = t + NTL * m;
     v[m] = (off >= 0 && n < n_in) ? in[off + n] : make_float2(0.f, 0.f);
   }
-  fft_reg<R1, DIR, L / R1>(v, twg);
+  fft_reg_c<R1, DIR>(v);
 #pragma unroll
   for (int k1 = 1; k1 < R1; ++k1) {
     float2 w = __ldg(twg + ((t * k1) & (L - 1)));
@@ -142,7 +142,7 @@ __global__ void __launch_bounds__(256) k_fft_rows_reg(const float2* __restrict__
 #pragma unroll
     for (int s = 0; s < NTL; ++s) u[c][s] = ls[(t * KPT + c) * RS + s];
 #pragma unroll
-  for (int c = 0; c < KPT; ++c) fft_reg<NTL, DIR, L / NTL>(u[c], twg);
+  for (int c = 0; c < KPT; ++c) fft_reg_c<NTL, DIR>(u[c]);
   if (off < 0) return;
   float2* o = out + off;
 #pragma unroll

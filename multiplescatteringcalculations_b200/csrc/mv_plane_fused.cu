@@ -38,7 +38,7 @@ __device__ __forceinline__ void line_fft(float2 (&v)[PlaneCfg<L>::R1], float2 (&
                                          float2* ls, int t, const float2* __restrict__ twg) {
   using PC = PlaneCfg<L>;
   constexpr int R1 = PC::R1, KPT = PC::KPT, RS = PC::RS;
-  fft_reg<R1, DIR, L / R1>(v, twg);
+  fft_reg_c<R1, DIR>(v);
 #pragma unroll
   for (int k1 = 1; k1 < R1; ++k1) {
     float2 w = __ldg(twg + ((t * k1) & (L - 1)));
@@ -54,7 +54,7 @@ __device__ __forceinline__ void line_fft(float2 (&v)[PlaneCfg<L>::R1], float2 (&
 #pragma unroll
     for (int s = 0; s < 8; ++s) u[c][s] = ls[(t * KPT + c) * RS + s];
 #pragma unroll
-  for (int c = 0; c < KPT; ++c) fft_reg<8, DIR, L / 8>(u[c], twg);
+  for (int c = 0; c < KPT; ++c) fft_reg_c<8, DIR>(u[c]);
 }
 
 __device__ __forceinline__ float2 tau_c(const float2* __restrict__ x, const float2* __restrict__ t4, int nsite,

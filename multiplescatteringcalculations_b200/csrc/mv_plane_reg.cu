@@ -41,7 +41,7 @@ __device__ __forceinline__ void four_step(float2 (&v)[YReg<L>::R1], float2 (&u)[
                                           float2* ls, int t, const float2* __restrict__ twg) {
   using Y = YReg<L>;
   constexpr int NTL = Y::NTL, R1 = Y::R1, KPT = Y::KPT, RS = Y::RS;
-  fft_reg<R1, DIR, L / R1>(v, twg);
+  fft_reg_c<R1, DIR>(v);
 #pragma unroll
   for (int k1 = 1; k1 < R1; ++k1) {
     float2 w = __ldg(twg + ((t * k1) & (L - 1)));
@@ -57,7 +57,7 @@ __device__ __forceinline__ void four_step(float2 (&v)[YReg<L>::R1], float2 (&u)[
 #pragma unroll
     for (int s = 0; s < NTL; ++s) u[c][s] = ls[(t * KPT + c) * RS + s];
 #pragma unroll
-  for (int c = 0; c < KPT; ++c) fft_reg<NTL, DIR, L / NTL>(u[c], twg);
+  for (int c = 0; c < KPT; ++c) fft_reg_c<NTL, DIR>(u[c]);
 }
 
 // C: blockIdx.x = chunk of LPB rows x, blockIdx.y = layer n, blockIdx.z = 9 rh + c.

@@ -129,16 +129,14 @@ __global__ void __launch_bounds__(ZpCfg<LZ, KX, S, SYM>::NT, ZpCfg<LZ, KX, S, SY
     // (1) the line's layers n < N_z <= Lz/2; the upper half of an S = 1 line is zero
 #pragma unroll
     for (int n = 0; n < LH; ++n) v[n] = (n < LZ / 2 && o >= 0 && n < g.Nz) ? W[o + n * plane] : czero<float2>();
-    if (rh == 0)
-      for (int t = tid; t < LZ; t += NT) tw[t] = twg[t];
     // the previous vector's inverse reads of the tile are done; the barrier's init visible
     __syncthreads();
     // (2) forward transform, rows kz = S m + b of the tile
     if (S == 2 && b) {
 #pragma unroll
-      for (int n = 0; n < LH; ++n) v[n] = v[n] * tw[n];
+      for (int n = 0; n < LH; ++n) v[n] = v[n] * ctw<LZ>(n);
     }
-    fft_reg<LH, -1, S>(v, tw);
+    fft_reg_c<LH, -1>(v);
     if (lact) {
 #pragma unroll
       for (int m = 0; m < LH; ++m) tile[(S * m + b) * P + l] = v[m];
@@ -191,11 +189,11 @@ __global__ void __launch_bounds__(ZpCfg<LZ, KX, S, SYM>::NT, ZpCfg<LZ, KX, S, SY
 #pragma unroll
         for (int k = 0; k < LH; ++k) {
           const float2 a = tile[k * P + l], c = tile[(k + LH) * P + l];
-          const float2 w = b ? tw[k] : make_float2(1.f, 0.f);
+          const float2 w = b ? ctw<LZ>(k) : make_float2(1.f, 0.f);
           v[k] = conj_mul(w, make_float2(fmaf(sg, c.x, a.x), fmaf(sg, c.y, a.y)));
         }
       }
-      fft_reg<LH, +1, S>(v, tw);
+      fft_reg_c<LH, +1>(v);
 #pragma unroll
       for (int m = 0; m < LH; ++m) {
         const int n = S * m + b;

@@ -1,5 +1,6 @@
 // Per-frequency setup on the device: twiddle tables, T0 (4 scalars per voxel),
 // the incident plane wave, layout conversions, and the G0 spectrum build.
+#include <mutex>
 #include <algorithm>
 #include <cstring>
 
@@ -25,7 +26,44 @@ __global__ void k_twiddles(double2* t64, float2* t32, int L) {
   t32[t] = make_float2((float)c, (float)-s);
 }
 
+__constant__ float2 c_tw256[256];
+
+// Fill the constant twiddle table of the current device once (k_twiddles at L = 256 into a
+// scratch buffer, then a device-to-device copy to the symbol).
+static int ensure_const_twiddles(msc_plan* pl) {
+  static std::mutex mu;
+  static bool ready[64] = {};
+  int dev = 0;
+  MSC_CUDA(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> lk(mu);
+  if (dev < 0 || dev >= 64) {
+    set_error("device index %d out of range", dev);
+    return MSC_ERR_INVALID;
+  }
+  if (ready[dev]) return MSC_OK;
+  DBuf t64, t32;
+  int s = dalloc(pl, t64, sizeof(double2) * 256);
+  if (s == MSC_OK) s = dalloc(pl, t32, sizeof(float2) * 256);
+  if (s == MSC_OK) {
+    k_twiddles<<<2, 128, 0, pl->stream>>>((double2*)t64.p, (float2*)t32.p, 256);
+    ::msc::note_launch();
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess)
+      e = cudaMemcpyToSymbolAsync(c_tw256, t32.p, sizeof(float2) * 256, 0, cudaMemcpyDeviceToDevice, pl->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(pl->stream);
+    if (e != cudaSuccess) {
+      set_error("constant twiddle table: %s", cudaGetErrorString(e));
+      s = MSC_ERR_CUDA;
+    }
+  }
+  dfree(pl, t64);
+  dfree(pl, t32);
+  if (s == MSC_OK) ready[dev] = true;
+  return s;
+}
+
 int build_twiddles(msc_plan* pl) {
+  MSC_TRY(ensure_const_twiddles(pl));
   const int Lz = pl->g.Lz, Lxy = pl->g.Lx;
   MSC_TRY(dalloc(pl, pl->tw64_z, sizeof(double2) * Lz));
   MSC_TRY(dalloc(pl, pl->tw32_z, sizeof(float2) * Lz));
