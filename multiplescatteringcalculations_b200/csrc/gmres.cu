@@ -15,6 +15,7 @@
 //    a step enqueued after convergence see the device `done` flag and return.
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <vector>
 
 #include "pc.cuh"
@@ -61,6 +62,10 @@ struct GmresWork {
     uint64_t gen = 0;
     int warm = 0;  // cycles of this kind run uncaptured (kernel attributes set, buffers allocated)
   } graph[2][2];
+  // While a cycle is captured with one conditional node per step: the handle that the
+  // step which ends the cycle sets to 0, so that the remaining steps are skipped.
+  unsigned long long cap_cond = 0;
+  int cap_cond_on = 0;
 };
 
 constexpr int NB = 592;     // blocks of the multi-vector kernels (4 per SM)
@@ -160,12 +165,84 @@ __device__ bool reduce_to(double2* sums, int nv, double2* __restrict__ part, int
 }
 
 // Chunked multi-vector kernels. A block of NTH threads covers chunks of NTH*EPT
-// consecutive elements (thread t holds elements t, t + NTH, ..., so each warp
-// access is coalesced); blocks stride over the chunks.
+// consecutive elements; thread t loads the CPL consecutive elements at
+// base + (u NTH + t) CPL + c (u < EPT/CPL), so each warp access is coalesced. CPL = 2
+// for complex64 vectors of even length (16-byte loads), else 1. Blocks stride over
+// the chunks.
 constexpr int EPT = 8;
 // vectors per load group in k_mdot / k_maxpy (memory-level parallelism: VG x EPT
 // independent loads per thread)
 constexpr int VG = 4;
+
+// Basis vectors i >= keep are read with the L2 evict-first policy. Every later step
+// of a cycle reads the first vectors again, and the matvec between two steps needs
+// its spectrum and workspace in L2: streaming the rest as evict-first keeps both
+// resident instead of cycling the whole basis through L2.
+__device__ __forceinline__ uint64_t l2_evict_first() {
+  uint64_t p;
+  asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(p));
+  return p;
+}
+template <typename T, int CPL> struct LdV;
+template <> struct LdV<float, 1> {
+  static __device__ __forceinline__ void run(const float2* p, float2* o, bool ef, uint64_t pol) {
+    if (ef)
+      asm volatile("ld.global.nc.L2::cache_hint.v2.f32 {%0,%1}, [%2], %3;"
+                   : "=f"(o[0].x), "=f"(o[0].y) : "l"(p), "l"(pol));
+    else
+      o[0] = __ldg(p);
+  }
+};
+template <> struct LdV<float, 2> {
+  static __device__ __forceinline__ void run(const float2* p, float2* o, bool ef, uint64_t pol) {
+    if (ef) {
+      asm volatile("ld.global.nc.L2::cache_hint.v4.f32 {%0,%1,%2,%3}, [%4], %5;"
+                   : "=f"(o[0].x), "=f"(o[0].y), "=f"(o[1].x), "=f"(o[1].y) : "l"(p), "l"(pol));
+    } else {
+      const float4 v = __ldg((const float4*)p);
+      o[0] = make_float2(v.x, v.y);
+      o[1] = make_float2(v.z, v.w);
+    }
+  }
+};
+template <> struct LdV<double, 1> {
+  static __device__ __forceinline__ void run(const double2* p, double2* o, bool ef, uint64_t pol) {
+    if (ef)
+      asm volatile("ld.global.nc.L2::cache_hint.v2.f64 {%0,%1}, [%2], %3;"
+                   : "=d"(o[0].x), "=d"(o[0].y) : "l"(p), "l"(pol));
+    else
+      o[0] = __ldg(p);
+  }
+};
+
+// a thread's EPT elements of one vector's chunk (zeros past n; n is a multiple of CPL)
+template <typename T, int CPL>
+__device__ __forceinline__ void ld_chunk(const cx<T>* p, size_t base, size_t n, cx<T>* o, bool ef, uint64_t pol) {
+#pragma unroll
+  for (int u = 0; u < EPT / CPL; ++u) {
+    const size_t k = base + ((size_t)u * NTH + threadIdx.x) * CPL;
+    if (k < n) {
+      LdV<T, CPL>::run(p + k, o + u * CPL, ef, pol);
+    } else {
+#pragma unroll
+      for (int c = 0; c < CPL; ++c) o[u * CPL + c] = czero<cx<T>>();
+    }
+  }
+}
+template <typename T, int CPL>
+__device__ __forceinline__ void st_chunk(cx<T>* p, size_t base, size_t n, const cx<T>* v) {
+#pragma unroll
+  for (int u = 0; u < EPT / CPL; ++u) {
+    const size_t k = base + ((size_t)u * NTH + threadIdx.x) * CPL;
+    if (k < n) {
+      if constexpr (CPL == 2)
+        *(float4*)(p + k) = make_float4((float)v[2 * u].x, (float)v[2 * u].y, (float)v[2 * u + 1].x,
+                                        (float)v[2 * u + 1].y);
+      else
+        p[k] = v[u];
+    }
+  }
+}
 
 // Thread i < nv of every block holds the block's total of row i; the last block
 // to finish sums the rows over blocks in a fixed order into out[i].
@@ -189,10 +266,10 @@ __device__ void reduce_rows(double2 mine, int nv, double2* __restrict__ part, in
 // out[i] = sum_k conj(s_i V_i[k]) w[k], i < nv. Per chunk and vector the
 // products of a warp are summed (FP32 within a thread's 8 elements, warp
 // shuffles), and lane 0 accumulates into the block's FP64 shared totals.
-template <typename T>
-__global__ void __launch_bounds__(NTH) k_mdot(const cx<T>* __restrict__ V, size_t n, int nv, const double* scale,
+template <typename T, int CPL>
+__global__ void __launch_bounds__(NTH, sizeof(T) == 4 ? 2 : 1) k_mdot(const cx<T>* __restrict__ V, size_t n, int nv, const double* scale,
                                               const cx<T>* __restrict__ w, double2* part, int* counter, double2* out,
-                                              const int* done) {
+                                              const int* done, int keep) {
   pdl_wait();
   pdl_trigger();
   if (done && *done) return;
@@ -200,25 +277,17 @@ __global__ void __launch_bounds__(NTH) k_mdot(const cx<T>* __restrict__ V, size_
   const int lane = threadIdx.x & 31, wp = threadIdx.x >> 5;
   for (int i = lane; i < nv; i += 32) sh[wp][i] = make_double2(0, 0);
   __syncwarp();
+  const uint64_t pol = l2_evict_first();
   const size_t chunk = (size_t)NTH * EPT;
   for (size_t base = (size_t)blockIdx.x * chunk; base < n; base += (size_t)gridDim.x * chunk) {
     cx<T> wr[EPT];
-#pragma unroll
-    for (int u = 0; u < EPT; ++u) {
-      const size_t k = base + (size_t)u * NTH + threadIdx.x;
-      wr[u] = k < n ? w[k] : czero<cx<T>>();
-    }
+    ld_chunk<T, CPL>(w, base, n, wr, false, pol);
     int i = 0;
     // groups of VG vectors: all VG x EPT loads are in flight before the first product
     for (; i + VG <= nv; i += VG) {
       cx<T> v[VG][EPT];
 #pragma unroll
-      for (int q = 0; q < VG; ++q)
-#pragma unroll
-        for (int u = 0; u < EPT; ++u) {
-          const size_t k = base + (size_t)u * NTH + threadIdx.x;
-          v[q][u] = k < n ? V[(size_t)(i + q) * n + k] : czero<cx<T>>();
-        }
+      for (int q = 0; q < VG; ++q) ld_chunk<T, CPL>(V + (size_t)(i + q) * n, base, n, v[q], i + q >= keep, pol);
       double ax[VG], ay[VG];
 #pragma unroll
       for (int q = 0; q < VG; ++q) {
@@ -245,16 +314,13 @@ __global__ void __launch_bounds__(NTH) k_mdot(const cx<T>* __restrict__ V, size_
         }
     }
     for (; i < nv; ++i) {
-      const cx<T>* Vi = V + (size_t)i * n;
+      cx<T> v[EPT];
+      ld_chunk<T, CPL>(V + (size_t)i * n, base, n, v, i >= keep, pol);
       cx<T> a = czero<cx<T>>();
 #pragma unroll
       for (int u = 0; u < EPT; ++u) {
-        const size_t k = base + (size_t)u * NTH + threadIdx.x;
-        if (k < n) {
-          const cx<T> v = Vi[k];
-          a.x += v.x * wr[u].x + v.y * wr[u].y;
-          a.y += v.x * wr[u].y - v.y * wr[u].x;
-        }
+        a.x += v[u].x * wr[u].x + v[u].y * wr[u].y;
+        a.y += v[u].x * wr[u].y - v[u].y * wr[u].x;
       }
       double ax = a.x, ay = a.y;
       for (int o = 16; o > 0; o >>= 1) {
@@ -284,7 +350,7 @@ __global__ void __launch_bounds__(NTH) k_mdot(const cx<T>* __restrict__ V, size_
 // last block of the normalising k_maxpy) right after ||w|| is known; the warp stages
 // the data in shared memory and lane 0 runs the sequential FP64 recurrences.
 __device__ __forceinline__ double cabs_(double2 a) { return hypot(a.x, a.y); }
-__device__ void givens_step(GState* st, HessPtr h, int m, int j, bool cgs2) {
+__device__ void givens_step(GState* st, HessPtr h, int m, int j, bool cgs2, unsigned long long cond, int cond_on) {
   __shared__ double2 col[33], sn[32];
   __shared__ double cs[32];
   __shared__ int stop;
@@ -380,16 +446,18 @@ __device__ void givens_step(GState* st, HessPtr h, int m, int j, bool cgs2) {
       }
       __threadfence();
       st->done = 1;
+      // a captured cycle skips its remaining steps
+      if (cond_on) cudaGraphSetConditional(cond, 0u);
     }
   }
 }
 
 // w -= sum_i coef_i s_i V_i (i < nv); optionally out_norm.x = ||w||^2
-template <typename T, bool NORM>
-__global__ void __launch_bounds__(NTH) k_maxpy(const cx<T>* __restrict__ V, size_t n, int nv, const double* scale,
+template <typename T, bool NORM, int CPL>
+__global__ void __launch_bounds__(NTH, sizeof(T) == 4 ? 2 : 1) k_maxpy(const cx<T>* __restrict__ V, size_t n, int nv, const double* scale,
                                                const double2* coef, cx<T>* __restrict__ w, double2* part, int* counter,
                                                double2* out_norm, const int* done, GState* st, HessPtr hp, int m,
-                                               int j, int cgs2) {
+                                               int j, int cgs2, unsigned long long cond, int cond_on, int keep) {
   pdl_wait();
   pdl_trigger();
   if (done && *done) return;
@@ -400,28 +468,28 @@ __global__ void __launch_bounds__(NTH) k_maxpy(const cx<T>* __restrict__ V, size
     cf[i] = i < nv ? mk<T>((T)(s * coef[i].x), (T)(s * coef[i].y)) : czero<cx<T>>();
   }
   __syncthreads();
+  const uint64_t pol = l2_evict_first();
   const size_t chunk = (size_t)NTH * EPT;
   double nrm = 0.0;
-  for (size_t base = (size_t)blockIdx.x * chunk; base < n; base += (size_t)gridDim.x * chunk) {
+  // The reverse of k_mdot's order, chunks and vectors alike: what k_mdot read last is
+  // still in L2 when this kernel reads it first.
+  const size_t nchunk = (n + chunk - 1) / chunk;
+  for (size_t c0 = blockIdx.x; c0 < nchunk; c0 += gridDim.x) {
+    const size_t rounds = (nchunk - 1 - blockIdx.x) / gridDim.x;  // this block's last round
+    const size_t base = ((size_t)blockIdx.x + (rounds - (c0 - blockIdx.x) / gridDim.x) * gridDim.x) * chunk;
     cx<T> wr[EPT];
-#pragma unroll
-    for (int u = 0; u < EPT; ++u) {
-      const size_t k = base + (size_t)u * NTH + threadIdx.x;
-      wr[u] = k < n ? w[k] : czero<cx<T>>();
-    }
+    ld_chunk<T, CPL>(w, base, n, wr, false, pol);
     int i = 0;
     for (; i + VG <= nv; i += VG) {
       cx<T> v[VG][EPT];
 #pragma unroll
-      for (int q = 0; q < VG; ++q)
-#pragma unroll
-        for (int u = 0; u < EPT; ++u) {
-          const size_t k = base + (size_t)u * NTH + threadIdx.x;
-          v[q][u] = k < n ? V[(size_t)(i + q) * n + k] : czero<cx<T>>();
-        }
+      for (int q = 0; q < VG; ++q) {
+        const int vi = nv - 1 - (i + q);
+        ld_chunk<T, CPL>(V + (size_t)vi * n, base, n, v[q], vi >= keep, pol);
+      }
 #pragma unroll
       for (int q = 0; q < VG; ++q) {
-        const cx<T> c = cf[i + q];
+        const cx<T> c = cf[nv - 1 - (i + q)];
 #pragma unroll
         for (int u = 0; u < EPT; ++u) {
           wr[u].x -= c.x * v[q][u].x - c.y * v[q][u].y;
@@ -430,26 +498,26 @@ __global__ void __launch_bounds__(NTH) k_maxpy(const cx<T>* __restrict__ V, size
       }
     }
     for (; i < nv; ++i) {
-      const cx<T>* Vi = V + (size_t)i * n;
-      const cx<T> c = cf[i];
+      cx<T> v[EPT];
+      const int vi = nv - 1 - i;
+      ld_chunk<T, CPL>(V + (size_t)vi * n, base, n, v, vi >= keep, pol);
+      const cx<T> c = cf[vi];
 #pragma unroll
       for (int u = 0; u < EPT; ++u) {
-        const size_t k = base + (size_t)u * NTH + threadIdx.x;
-        if (k < n) {
-          const cx<T> v = Vi[k];
-          wr[u].x -= c.x * v.x - c.y * v.y;
-          wr[u].y -= c.x * v.y + c.y * v.x;
-        }
+        wr[u].x -= c.x * v[u].x - c.y * v[u].y;
+        wr[u].y -= c.x * v[u].y + c.y * v[u].x;
       }
     }
+    st_chunk<T, CPL>(w, base, n, wr);
+    if (NORM)
 #pragma unroll
-    for (int u = 0; u < EPT; ++u) {
-      const size_t k = base + (size_t)u * NTH + threadIdx.x;
-      if (k < n) {
-        w[k] = wr[u];
-        if (NORM) nrm += (double)wr[u].x * wr[u].x + (double)wr[u].y * wr[u].y;
+      for (int u = 0; u < EPT / CPL; ++u) {
+        const size_t k = base + ((size_t)u * NTH + threadIdx.x) * CPL;
+        if (k < n)
+#pragma unroll
+          for (int c = 0; c < CPL; ++c)
+            nrm += (double)wr[u * CPL + c].x * wr[u * CPL + c].x + (double)wr[u * CPL + c].y * wr[u * CPL + c].y;
       }
-    }
   }
   if (NORM) {
     double2 a[1] = {make_double2(nrm, 0.0)};
@@ -457,7 +525,7 @@ __global__ void __launch_bounds__(NTH) k_maxpy(const cx<T>* __restrict__ V, size
     // the last block holds the final ||w||^2: it runs the step's Givens update
     if (last && st && threadIdx.x < 32) {
       __syncwarp();
-      givens_step(st, hp, m, j, cgs2 != 0);
+      givens_step(st, hp, m, j, cgs2 != 0, cond, cond_on);
     }
   }
 }
@@ -508,25 +576,47 @@ __global__ void k_cycle_init(GState* st, HessPtr h, int m, double tol_abs) {
 }
 
 
-// x += sum_{i<k} y_i s_i V_i, with k from the state (s_i = 1 when scale is null)
-template <typename T, typename TX, int NV>
-__global__ void __launch_bounds__(NTH) k_update_x(cx<TX>* __restrict__ x, const cx<T>* __restrict__ V, size_t n,
-                                                  const double* scale, const double2* y, const GState* st) {
-  __shared__ double2 cf[NV];
+// x += sum_{i<k} y_i s_i V_i, with k from the state (s_i = 1 when scale is null); the
+// chunked loads of the Arnoldi kernels, FP64 sums
+template <typename T, int CPL>
+__global__ void __launch_bounds__(NTH, sizeof(T) == 4 ? 2 : 1)
+    k_update_x(cx<T>* __restrict__ x, const cx<T>* __restrict__ V, size_t n, const double* scale,
+               const double2* y, const GState* st) {
+  __shared__ double2 cf[32];
   const int k = st->k;
-  if (threadIdx.x < NV)
+  if (threadIdx.x < 32)
     cf[threadIdx.x] = threadIdx.x < k ? (scale ? scale[threadIdx.x] : 1.0) * y[threadIdx.x] : make_double2(0, 0);
   __syncthreads();
   if (k == 0) return;
-  for (size_t e = (size_t)blockIdx.x * NTH + threadIdx.x; e < n; e += (size_t)gridDim.x * NTH) {
-    double2 xv = to_d(x[e]);
+  const size_t chunk = (size_t)NTH * EPT;
+  for (size_t base = (size_t)blockIdx.x * chunk; base < n; base += (size_t)gridDim.x * chunk) {
+    double2 acc[EPT];
 #pragma unroll
-    for (int i = 0; i < NV; ++i)
-      if (i < k) {
-        const double2 v = to_d(V[(size_t)i * n + e]);
-        xv += cf[i] * v;
+    for (int u = 0; u < EPT; ++u) acc[u] = make_double2(0, 0);
+    int i = 0;
+    for (; i + VG <= k; i += VG) {
+      cx<T> v[VG][EPT];
+#pragma unroll
+      for (int q = 0; q < VG; ++q) ld_chunk<T, CPL>(V + (size_t)(i + q) * n, base, n, v[q], false, 0);
+#pragma unroll
+      for (int q = 0; q < VG; ++q) {
+        const double2 c = cf[i + q];
+#pragma unroll
+        for (int u = 0; u < EPT; ++u) acc[u] += c * to_d(v[q][u]);
       }
-    x[e] = from_d<cx<TX>>(xv);
+    }
+    for (; i < k; ++i) {
+      cx<T> v[EPT];
+      ld_chunk<T, CPL>(V + (size_t)i * n, base, n, v, false, 0);
+      const double2 c = cf[i];
+#pragma unroll
+      for (int u = 0; u < EPT; ++u) acc[u] += c * to_d(v[u]);
+    }
+    cx<T> xv[EPT];
+    ld_chunk<T, CPL>(x, base, n, xv, false, 0);
+#pragma unroll
+    for (int u = 0; u < EPT; ++u) xv[u] = from_d<cx<T>>(to_d(xv[u]) + acc[u]);
+    st_chunk<T, CPL>(x, base, n, xv);
   }
 }
 
@@ -549,6 +639,29 @@ __global__ void k_sqrt(const double* a, double* b) {
 }
 
 // ---- host side ---------------------------------------------------------------------------
+// Captured cycles use conditional graph nodes unless MSC_GRAPH_CONDITIONAL=0.
+static bool graph_conditionals() {
+  static const bool on = [] {
+    const char* e = getenv("MSC_GRAPH_CONDITIONAL");
+    return !(e && e[0] == '0');
+  }();
+  return on;
+}
+
+// Basis vectors kept in L2 by the Arnoldi kernels: as many as fit in KEEP_BYTES
+// (64x64x16, complex64, 4.7 MB per vector: the first 8).
+constexpr double KEEP_BYTES = 40e6;
+template <typename T>
+static int keep_vectors(size_t n) {
+  const double k = KEEP_BYTES / ((double)n * sizeof(cx<T>));
+  return k < 1.0 ? 1 : (k > 32.0 ? 32 : (int)k);
+}
+// 16-byte loads of complex64 pairs when every vector starts on a 16-byte boundary
+template <typename T>
+static bool paired(const void* V, size_t n) {
+  return sizeof(T) == 4 && n % 2 == 0 && ((uintptr_t)V & 15) == 0;
+}
+
 template <typename T>
 static int mdot(msc_plan* pl, GmresWork* gw, const cx<T>* V, int nv, const double* scale, const cx<T>* w, double2* out,
                 const int* done) {
@@ -557,11 +670,15 @@ static int mdot(msc_plan* pl, GmresWork* gw, const cx<T>* V, int nv, const doubl
   const int nb = std::min<long long>(NB, ceil_div((long long)gw->n, (long long)NTH * EPT));
   size_t n = gw->n;
   int* counter = &st->counter[0];
-  void* args[] = {(void*)&V, (void*)&n, (void*)&nv, (void*)&scale, (void*)&w, (void*)&part, (void*)&counter,
-                  (void*)&out, (void*)&done};
+  int keep = keep_vectors<T>(n);
+  void* args[] = {(void*)&V,    (void*)&n,       (void*)&nv,  (void*)&scale, (void*)&w,   (void*)&part,
+                  (void*)&counter, (void*)&out, (void*)&done, (void*)&keep};
+  const void* kern = (const void*)k_mdot<T, 1>;
+  if constexpr (sizeof(T) == 4)
+    if (paired<T>(V, n)) kern = (const void*)k_mdot<T, 2>;
   // an ordinary launch: with programmatic dependent launch the Arnoldi kernels made the
   // cfg2 solve 8% slower (the matvec kernels, which gain from it, keep it)
-  MSC_CUDA(cudaLaunchKernel((const void*)k_mdot<T>, dim3(nb), dim3(NTH), args, 0, pl->stream));
+  MSC_CUDA(cudaLaunchKernel(kern, dim3(nb), dim3(NTH), args, 0, pl->stream));
   ::msc::note_launch();
   return MSC_OK;
 }
@@ -578,10 +695,16 @@ static int maxpy(msc_plan* pl, GmresWork* gw, const cx<T>* V, int nv, const doub
   GState* gst = giv_j >= 0 ? st : nullptr;
   HessPtr hp = hess_ptrs(gw);
   int c2 = cgs2 ? 1 : 0;
-  void* args[] = {(void*)&V, (void*)&n, (void*)&nv, (void*)&scale, (void*)&coef, (void*)&w, (void*)&part,
-                  (void*)&counter, (void*)&out_norm, (void*)&done, (void*)&gst, (void*)&hp, (void*)&m,
-                  (void*)&giv_j, (void*)&c2};
-  MSC_CUDA(cudaLaunchKernel((const void*)k_maxpy<T, NORM>, dim3(nb), dim3(NTH), args, 0, pl->stream));
+  unsigned long long cond = gw->cap_cond;
+  int cond_on = giv_j >= 0 ? gw->cap_cond_on : 0;
+  int keep = keep_vectors<T>(n);
+  void* args[] = {(void*)&V,       (void*)&n,        (void*)&nv,   (void*)&scale, (void*)&coef, (void*)&w,
+                  (void*)&part,    (void*)&counter,  (void*)&out_norm, (void*)&done, (void*)&gst, (void*)&hp,
+                  (void*)&m,       (void*)&giv_j,    (void*)&c2,   (void*)&cond,  (void*)&cond_on, (void*)&keep};
+  const void* kern = (const void*)k_maxpy<T, NORM, 1>;
+  if constexpr (sizeof(T) == 4)
+    if (paired<T>(V, n)) kern = (const void*)k_maxpy<T, NORM, 2>;
+  MSC_CUDA(cudaLaunchKernel(kern, dim3(nb), dim3(NTH), args, 0, pl->stream));
   ::msc::note_launch();
   return MSC_OK;
 }
@@ -778,15 +901,56 @@ static int gmres_core(msc_plan* pl, int m, const cx<T>* rhs, cx<T>* x, bool x_ze
         if (gr.exec) cudaGraphExecDestroy(gr.exec);
         gr.exec = nullptr;
         cudaGraph_t graph = nullptr;
-        MSC_CUDA(cudaStreamBeginCapture(pl->stream, cudaStreamCaptureModeThreadLocal));
         int cs = MSC_OK;
-        for (int j = 0; j < m && cs == MSC_OK; ++j) cs = step(j);
-        const cudaError_t ce = cudaStreamEndCapture(pl->stream, &graph);
-        if (cs != MSC_OK) {
-          if (graph) cudaGraphDestroy(graph);
-          return cs;
+        // One conditional (IF) node per step: the step that ends the cycle sets the
+        // handle to 0 and the graph skips the steps after it, instead of launching their
+        // kernels only for them to return at once. A plain capture is the fallback.
+        bool cond_ok = graph_conditionals() && cudaGraphCreate(&graph, 0) == cudaSuccess;
+        if (cond_ok) {
+          cudaGraphConditionalHandle hc = 0;
+          cond_ok = cudaGraphConditionalHandleCreate(&hc, graph, 1u, cudaGraphCondAssignDefault) == cudaSuccess;
+          gw->cap_cond = hc;
+          gw->cap_cond_on = 1;
+          cudaGraphNode_t prev = nullptr;
+          for (int j = 0; j < m && cond_ok && cs == MSC_OK; ++j) {
+            cudaGraphNodeParams cp = {};
+            cp.type = cudaGraphNodeTypeConditional;
+            cp.conditional.handle = hc;
+            cp.conditional.type = cudaGraphCondTypeIf;
+            cp.conditional.size = 1;
+            cudaGraphNode_t node = nullptr;
+            if (cudaGraphAddNode(&node, graph, prev ? &prev : nullptr, prev ? 1 : 0, &cp) != cudaSuccess ||
+                cudaStreamBeginCaptureToGraph(pl->stream, cp.conditional.phGraph_out[0], nullptr, nullptr, 0,
+                                              cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+              cond_ok = false;
+              break;
+            }
+            cs = step(j);
+            cudaGraph_t body = nullptr;
+            if (cudaStreamEndCapture(pl->stream, &body) != cudaSuccess) cond_ok = false;
+            prev = node;
+          }
+          gw->cap_cond_on = 0;
+          if (cs != MSC_OK || !cond_ok) {
+            cudaGraphDestroy(graph);
+            graph = nullptr;
+          }
+          if (cs != MSC_OK) return cs;
+          (void)cudaGetLastError();  // a refused conditional-node call is not the plain capture's error
+        } else if (graph) {
+          cudaGraphDestroy(graph);
+          graph = nullptr;
         }
-        MSC_CUDA(ce);
+        if (!cond_ok) {
+          MSC_CUDA(cudaStreamBeginCapture(pl->stream, cudaStreamCaptureModeThreadLocal));
+          for (int j = 0; j < m && cs == MSC_OK; ++j) cs = step(j);
+          const cudaError_t ce = cudaStreamEndCapture(pl->stream, &graph);
+          if (cs != MSC_OK) {
+            if (graph) cudaGraphDestroy(graph);
+            return cs;
+          }
+          MSC_CUDA(ce);
+        }
         const cudaError_t ie = cudaGraphInstantiate(&gr.exec, graph, 0);
         cudaGraphDestroy(graph);
         MSC_CUDA(ie);
@@ -840,9 +1004,15 @@ static int gmres_core(msc_plan* pl, int m, const cx<T>* rhs, cx<T>* x, bool x_ze
     if (pol && enq > 0) ++pol->cycles[use_pc ? 1 : 0];
     // x += V y (k columns), or Z y with the preconditioner
     if (cur.k > 0) {
-      const int nb = std::min<long long>(NB, ceil_div((long long)n, NTH));
-      if (use_pc) k_update_x<T, T, 32><<<nb, NTH, 0, pl->stream>>>(x, Z, n, nullptr, h.y, st);
-      else k_update_x<T, T, 32><<<nb, NTH, 0, pl->stream>>>(x, V, n, h.scale, h.y, st);
+      const int nb = std::min<long long>(NB, ceil_div((long long)n, (long long)NTH * EPT));
+      const cx<T>* B = use_pc ? Z : V;
+      const double* sc = use_pc ? nullptr : h.scale;
+      bool pair = false;
+      if constexpr (sizeof(T) == 4) {
+        pair = paired<T>(B, n) && paired<T>(x, n);
+        if (pair) k_update_x<T, 2><<<nb, NTH, 0, pl->stream>>>(x, B, n, sc, h.y, st);
+      }
+      if (!pair) k_update_x<T, 1><<<nb, NTH, 0, pl->stream>>>(x, B, n, sc, h.y, st);
       ::msc::note_launch();
       MSC_CUDA(cudaGetLastError());
     }
