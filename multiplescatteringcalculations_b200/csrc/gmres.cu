@@ -62,10 +62,6 @@ struct GmresWork {
     uint64_t gen = 0;
     int warm = 0;  // cycles of this kind run uncaptured (kernel attributes set, buffers allocated)
   } graph[2][2];
-  // While a cycle is captured with one conditional node per step: the handle that the
-  // step which ends the cycle sets to 0, so that the remaining steps are skipped.
-  unsigned long long cap_cond = 0;
-  int cap_cond_on = 0;
 };
 
 constexpr int NB = 592;     // blocks of the multi-vector kernels (4 per SM)
@@ -350,7 +346,7 @@ __global__ void __launch_bounds__(NTH, sizeof(T) == 4 ? 2 : 1) k_mdot(const cx<T
 // last block of the normalising k_maxpy) right after ||w|| is known; the warp stages
 // the data in shared memory and lane 0 runs the sequential FP64 recurrences.
 __device__ __forceinline__ double cabs_(double2 a) { return hypot(a.x, a.y); }
-__device__ void givens_step(GState* st, HessPtr h, int m, int j, bool cgs2, unsigned long long cond, int cond_on) {
+__device__ void givens_step(GState* st, HessPtr h, int m, int j, bool cgs2) {
   __shared__ double2 col[33], sn[32];
   __shared__ double cs[32];
   __shared__ int stop;
@@ -446,8 +442,6 @@ __device__ void givens_step(GState* st, HessPtr h, int m, int j, bool cgs2, unsi
       }
       __threadfence();
       st->done = 1;
-      // a captured cycle skips its remaining steps
-      if (cond_on) cudaGraphSetConditional(cond, 0u);
     }
   }
 }
@@ -457,7 +451,7 @@ template <typename T, bool NORM, int CPL>
 __global__ void __launch_bounds__(NTH, sizeof(T) == 4 ? 2 : 1) k_maxpy(const cx<T>* __restrict__ V, size_t n, int nv, const double* scale,
                                                const double2* coef, cx<T>* __restrict__ w, double2* part, int* counter,
                                                double2* out_norm, const int* done, GState* st, HessPtr hp, int m,
-                                               int j, int cgs2, unsigned long long cond, int cond_on, int keep) {
+                                               int j, int cgs2, int keep) {
   pdl_wait();
   pdl_trigger();
   if (done && *done) return;
@@ -525,7 +519,7 @@ __global__ void __launch_bounds__(NTH, sizeof(T) == 4 ? 2 : 1) k_maxpy(const cx<
     // the last block holds the final ||w||^2: it runs the step's Givens update
     if (last && st && threadIdx.x < 32) {
       __syncwarp();
-      givens_step(st, hp, m, j, cgs2 != 0, cond, cond_on);
+      givens_step(st, hp, m, j, cgs2 != 0);
     }
   }
 }
@@ -639,14 +633,6 @@ __global__ void k_sqrt(const double* a, double* b) {
 }
 
 // ---- host side ---------------------------------------------------------------------------
-// Captured cycles use conditional graph nodes unless MSC_GRAPH_CONDITIONAL=0.
-static bool graph_conditionals() {
-  static const bool on = [] {
-    const char* e = getenv("MSC_GRAPH_CONDITIONAL");
-    return !(e && e[0] == '0');
-  }();
-  return on;
-}
 
 // Basis vectors kept in L2 by the Arnoldi kernels: as many as fit in KEEP_BYTES
 // (64x64x16, complex64, 4.7 MB per vector: the first 8).
@@ -695,12 +681,10 @@ static int maxpy(msc_plan* pl, GmresWork* gw, const cx<T>* V, int nv, const doub
   GState* gst = giv_j >= 0 ? st : nullptr;
   HessPtr hp = hess_ptrs(gw);
   int c2 = cgs2 ? 1 : 0;
-  unsigned long long cond = gw->cap_cond;
-  int cond_on = giv_j >= 0 ? gw->cap_cond_on : 0;
   int keep = keep_vectors<T>(n);
   void* args[] = {(void*)&V,       (void*)&n,        (void*)&nv,   (void*)&scale, (void*)&coef, (void*)&w,
                   (void*)&part,    (void*)&counter,  (void*)&out_norm, (void*)&done, (void*)&gst, (void*)&hp,
-                  (void*)&m,       (void*)&giv_j,    (void*)&c2,   (void*)&cond,  (void*)&cond_on, (void*)&keep};
+                  (void*)&m,       (void*)&giv_j,    (void*)&c2,   (void*)&keep};
   const void* kern = (const void*)k_maxpy<T, NORM, 1>;
   if constexpr (sizeof(T) == 4)
     if (paired<T>(V, n)) kern = (const void*)k_maxpy<T, NORM, 2>;
@@ -902,55 +886,14 @@ static int gmres_core(msc_plan* pl, int m, const cx<T>* rhs, cx<T>* x, bool x_ze
         gr.exec = nullptr;
         cudaGraph_t graph = nullptr;
         int cs = MSC_OK;
-        // One conditional (IF) node per step: the step that ends the cycle sets the
-        // handle to 0 and the graph skips the steps after it, instead of launching their
-        // kernels only for them to return at once. A plain capture is the fallback.
-        bool cond_ok = graph_conditionals() && cudaGraphCreate(&graph, 0) == cudaSuccess;
-        if (cond_ok) {
-          cudaGraphConditionalHandle hc = 0;
-          cond_ok = cudaGraphConditionalHandleCreate(&hc, graph, 1u, cudaGraphCondAssignDefault) == cudaSuccess;
-          gw->cap_cond = hc;
-          gw->cap_cond_on = 1;
-          cudaGraphNode_t prev = nullptr;
-          for (int j = 0; j < m && cond_ok && cs == MSC_OK; ++j) {
-            cudaGraphNodeParams cp = {};
-            cp.type = cudaGraphNodeTypeConditional;
-            cp.conditional.handle = hc;
-            cp.conditional.type = cudaGraphCondTypeIf;
-            cp.conditional.size = 1;
-            cudaGraphNode_t node = nullptr;
-            if (cudaGraphAddNode(&node, graph, prev ? &prev : nullptr, prev ? 1 : 0, &cp) != cudaSuccess ||
-                cudaStreamBeginCaptureToGraph(pl->stream, cp.conditional.phGraph_out[0], nullptr, nullptr, 0,
-                                              cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
-              cond_ok = false;
-              break;
-            }
-            cs = step(j);
-            cudaGraph_t body = nullptr;
-            if (cudaStreamEndCapture(pl->stream, &body) != cudaSuccess) cond_ok = false;
-            prev = node;
-          }
-          gw->cap_cond_on = 0;
-          if (cs != MSC_OK || !cond_ok) {
-            cudaGraphDestroy(graph);
-            graph = nullptr;
-          }
-          if (cs != MSC_OK) return cs;
-          (void)cudaGetLastError();  // a refused conditional-node call is not the plain capture's error
-        } else if (graph) {
-          cudaGraphDestroy(graph);
-          graph = nullptr;
+        MSC_CUDA(cudaStreamBeginCapture(pl->stream, cudaStreamCaptureModeThreadLocal));
+        for (int j = 0; j < m && cs == MSC_OK; ++j) cs = step(j);
+        const cudaError_t ce = cudaStreamEndCapture(pl->stream, &graph);
+        if (cs != MSC_OK) {
+          if (graph) cudaGraphDestroy(graph);
+          return cs;
         }
-        if (!cond_ok) {
-          MSC_CUDA(cudaStreamBeginCapture(pl->stream, cudaStreamCaptureModeThreadLocal));
-          for (int j = 0; j < m && cs == MSC_OK; ++j) cs = step(j);
-          const cudaError_t ce = cudaStreamEndCapture(pl->stream, &graph);
-          if (cs != MSC_OK) {
-            if (graph) cudaGraphDestroy(graph);
-            return cs;
-          }
-          MSC_CUDA(ce);
-        }
+        MSC_CUDA(ce);
         const cudaError_t ie = cudaGraphInstantiate(&gr.exec, graph, 0);
         cudaGraphDestroy(graph);
         MSC_CUDA(ie);
