@@ -299,6 +299,71 @@ __global__ void __launch_bounds__(128) k_g0_spatial(double2* __restrict__ Ks, co
   }
 }
 
+// The same kernel for a mirror-symmetric spectrum (octant storage): one thread per
+// point of the octant z <= Lz/2, y <= Ly/2, x <= Lx/2, evaluated as above and written
+// to its mirror images too. Reflecting the axes in f (bit 0 x, 1 y, 2 z) negates the
+// image offsets and multiplies entry (a, b) by (-1)^popc((par_a ^ par_b) & f), par the
+// DOF parities; the mirror of index u is (L - u) mod L.
+__global__ void __launch_bounds__(128) k_g0_spatial_oct(double2* __restrict__ Ks, const double* __restrict__ vab,
+                                                        G0Params p) {
+  const Geo& g = p.g;
+  const long long npts = (long long)g.Lz * g.Ly * g.Lx;
+  const int qx = g.Lx / 2 + 1, qy = g.Ly / 2 + 1, qz = g.Lz / 2 + 1;
+  const long long gid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (gid >= (long long)qz * qy * qx) return;
+  const int x = (int)(gid % qx);
+  const int y = (int)((gid / qx) % qy);
+  const int z = (int)(gid / ((long long)qx * qy));
+  const long long pt = ((long long)z * g.Ly + y) * g.Lx + x;
+  int oz[2], ox[2], oy[2];
+  const int nz = axis_offsets(z, g.Lz, g.Nz, false, oz);
+  const int nx = axis_offsets(x, g.Lx, g.M, p.periodic, ox);
+  const int ny = axis_offsets(y, g.Ly, g.M, p.periodic, oy);
+  bool first = true;
+  for (int iz = 0; iz < nz; ++iz)
+    for (int ix = 0; ix < nx; ++ix)
+      for (int iy = 0; iy < ny; ++iy) {
+        const int dz = oz[iz], dx = ox[ix], dy = oy[iy];
+        if (dz == 0 && dx == 0 && dy == 0) continue;  // self term
+        const bool va = p.va && abs(dz) <= 1 && abs(dx) <= 1 && abs(dy) <= 1;
+        const double* vb = va ? vab + va_slot(dz, dx, dy) * 81 : nullptr;
+        PointProp pp;
+        if (!va) pp.init(dz * p.d, dx * p.d, dy * p.d, p.omega, p.alpha, p.beta, p.rho);
+        int e = 0;
+        for (int a = 0; a < 9; ++a)
+          for (int b = (p.E == 45 ? a : 0); b < 9; ++b, ++e) {
+            double2 v = va ? make_double2(vb[a * 9 + b], 0.0) : pp.entry(a, b);
+            if (p.E == 45 && b >= 6) v = 2.0 * v;  // (K D)_ij = K_ij D_j
+            v = p.scale * v;
+            double2* dst = Ks + (size_t)e * npts + pt;
+            if (first) *dst = v;
+            else *dst = *dst + v;
+          }
+        first = false;
+      }
+  // the mirror images: distinct indices per axis, and the reflections that reach them
+  const int mz = z == 0 || 2 * z == g.Lz ? 1 : 2;
+  const int my = y == 0 || 2 * y == g.Ly ? 1 : 2;
+  const int mx = x == 0 || 2 * x == g.Lx ? 1 : 2;
+  int e = 0;
+  for (int a = 0; a < 9; ++a)
+    for (int b = (p.E == 45 ? a : 0); b < 9; ++b, ++e) {
+      double2* base = Ks + (size_t)e * npts;
+      const double2 v = first ? make_double2(0, 0) : base[pt];
+      if (first) base[pt] = v;
+      const int par = dof_parity(a) ^ dof_parity(b);
+      for (int rz = 0; rz < mz; ++rz)
+        for (int ry = 0; ry < my; ++ry)
+          for (int rx = 0; rx < mx; ++rx) {
+            const int f = rx | (ry << 1) | (rz << 2);
+            if (f == 0) continue;
+            const int zz = rz ? g.Lz - z : z, yy = ry ? g.Ly - y : y, xx = rx ? g.Lx - x : x;
+            const double sg = (__popc(par & f) & 1) ? -1.0 : 1.0;
+            base[((long long)zz * g.Ly + yy) * g.Lx + xx] = make_double2(sg * v.x, sg * v.y);
+          }
+    }
+}
+
 template <typename T>
 int launch_fft_strided(msc_plan* pl, const cx<T>* in, long long es, long long S1, long long S2, cx<T>* out,
                        long long eo, long long O1, long long O2, float2* out32, int ncol, int n1, int n2, int n_in,
@@ -387,7 +452,15 @@ int launch_g0(msc_plan* pl, double omega, const double* kpar, int va, int n_orde
   p.kx = kpar ? kpar[0] : 0.0;
   p.ky = kpar ? kpar[1] : 0.0;
   p.scale = 1.0 / ((double)g.Lz * g.Lx * g.Ly);
-  k_g0_spatial<<<(unsigned)ceil_div(npts, 128), 128, 0, pl->stream>>>((double2*)ks.p, (const double*)pl->va_blocks.p, p); ::msc::note_launch();
+  if (g.oct) {
+    const long long noct = (long long)(g.Lz / 2 + 1) * (g.Ly / 2 + 1) * (g.Lx / 2 + 1);
+    k_g0_spatial_oct<<<(unsigned)ceil_div(noct, 128), 128, 0, pl->stream>>>((double2*)ks.p,
+                                                                           (const double*)pl->va_blocks.p, p);
+  } else {
+    k_g0_spatial<<<(unsigned)ceil_div(npts, 128), 128, 0, pl->stream>>>((double2*)ks.p, (const double*)pl->va_blocks.p,
+                                                                        p);
+  }
+  ::msc::note_launch();
   MSC_CUDA(cudaGetLastError());
   double2* K = (double2*)ks.p;
   // near-field blocks for the preconditioner, before the transforms overwrite K
