@@ -387,7 +387,7 @@ int msc_plan_destroy(msc_plan* pl) {
     pl->nf = nullptr;
   }
   DBuf* bufs[] = {&pl->tw64_z, &pl->tw64_xy, &pl->tw32_z, &pl->tw32_xy, &pl->t4_64, &pl->t4_32, &pl->khat64,
-                  &pl->khat32, &pl->va_blocks, &pl->g0_scratch, &pl->W64, &pl->W32, &pl->Wm64, &pl->Wm32, &pl->f64a, &pl->f64b, &pl->f32a, &pl->f32b,
+                  &pl->khat32, &pl->va_blocks, &pl->g0_scratch, &pl->g0_near, &pl->W64, &pl->W32, &pl->Wm64, &pl->Wm32, &pl->f64a, &pl->f64b, &pl->f32a, &pl->f32b,
                   &pl->red, &pl->status};
   for (DBuf* b : bufs) dfree(pl, *b);
   cudaStreamSynchronize(pl->stream);
@@ -559,6 +559,7 @@ int msc_set_nearfield_weights(msc_plan* pl, int format) {
 int msc_nearfield_blocks(const msc_plan* pl, double* out) {
   if (!pl || !out) { set_error("null argument"); return MSC_ERR_INVALID; }
   if (!pl->nf || !pl->nf->ready) { set_error("the near-field blocks need build_g0 first"); return MSC_ERR_STATE; }
+  MSC_TRY(nf_host_sync(pl));
   for (int i = 0; i < NF_OFFS * 81; ++i) {
     out[2 * i] = pl->nf->g64[i].x;
     out[2 * i + 1] = pl->nf->g64[i].y;

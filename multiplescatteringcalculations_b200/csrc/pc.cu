@@ -50,7 +50,7 @@ __global__ void k_nf_extract(const double2* __restrict__ K, Geo g, int E, double
   out[t] = inv_scale * v;
 }
 
-int nearfield_extract(msc_plan* pl, const double2* Ks, double scale) {
+int nearfield_extract(msc_plan* pl, const double2* Ks, double scale, const Geo* box) {
   if (!pl->nf) pl->nf = new NearField();
   NearField* nf = pl->nf;
   MSC_TRY(dalloc(pl, nf->g64_dev, sizeof(double2) * (size_t)(NF_MAXL + 1) * NF_OFFS * 81));
@@ -58,14 +58,25 @@ int nearfield_extract(msc_plan* pl, const double2* Ks, double scale) {
   MSC_TRY(dalloc(pl, nf->g16_dev, sizeof(__nv_bfloat162) * (size_t)(NF_MAXL + 1) * NF_OFFS * 81));
   MSC_TRY(dalloc(pl, nf->gtc_dev, (size_t)NF_MAXL * NF_TC_LAYER_BYTES));
   double2* dst = (double2*)nf->g64_dev.p;
-  k_nf_extract<<<ceil_div(NF_OFFS * 81, 256), 256, 0, pl->stream>>>(Ks, pl->g, pl->E, 1.0 / scale, dst);
+  k_nf_extract<<<ceil_div(NF_OFFS * 81, 256), 256, 0, pl->stream>>>(Ks, box ? *box : pl->g, pl->E, 1.0 / scale, dst);
   ::msc::note_launch();
   MSC_CUDA(cudaGetLastError());
-  nf->g64.resize((size_t)NF_OFFS * 81);
-  MSC_CUDA(cudaMemcpyAsync(nf->g64.data(), dst, sizeof(double2) * NF_OFFS * 81, cudaMemcpyDeviceToHost, pl->stream));
-  MSC_CUDA(cudaStreamSynchronize(pl->stream));
+  if (!nf->pin) MSC_CUDA(cudaMallocHost((void**)&nf->pin, sizeof(double2) * NF_OFFS * 81));
+  if (!nf->ev) MSC_CUDA(cudaEventCreateWithFlags(&nf->ev, cudaEventDisableTiming));
+  MSC_CUDA(cudaMemcpyAsync(nf->pin, dst, sizeof(double2) * NF_OFFS * 81, cudaMemcpyDeviceToHost, pl->stream));
+  MSC_CUDA(cudaEventRecord(nf->ev, pl->stream));
+  nf->host_pending = true;
   nf->ready = true;
   nf->dirty = true;
+  return MSC_OK;
+}
+
+int nf_host_sync(const msc_plan* pl) {
+  NearField* nf = pl->nf;
+  if (!nf || !nf->host_pending) return MSC_OK;
+  MSC_CUDA(cudaEventSynchronize(nf->ev));
+  nf->g64.assign(nf->pin, nf->pin + (size_t)NF_OFFS * 81);
+  nf->host_pending = false;
   return MSC_OK;
 }
 
@@ -219,6 +230,7 @@ __global__ void __launch_bounds__(256) k_nf64(const double2* __restrict__ x, con
 int nearfield_refresh(msc_plan* pl) {
   NearField* nf = pl->nf;
   if (!nf->dirty) return MSC_OK;
+  MSC_TRY(nf_host_sync(pl));
   const int L = std::max(1, std::min(nf->L, NF_MAXL));
   const size_t nb = (size_t)L * NF_OFFS * 81;
   nf->h64.resize(nb);

@@ -40,11 +40,23 @@ struct NearField {
   std::vector<uint16_t> htc;
   DBuf tmp32, tmp64;           // two field-size work vectors per precision
   bool dirty = true;           // layer blocks to rebuild from g64, dg
+  // g64 arrives by an asynchronous copy into `pin` (page-locked), complete at `ev`: the
+  // G0 build does not wait for it; nf_host_sync finishes it before g64 is read.
+  double2* pin = nullptr;
+  cudaEvent_t ev = nullptr;
+  bool host_pending = false;
+  ~NearField() {
+    if (pin) cudaFreeHost(pin);
+    if (ev) cudaEventDestroy(ev);
+  }
 };
 
+// Completes the host copy g64 of the near-field blocks (waits for the copy's event).
+int nf_host_sync(const msc_plan* pl);
+
 // Extract the near-field blocks from the spatial kernel of the G0 build (values
-// times `scale`).
-int nearfield_extract(msc_plan* pl, const double2* Ks_spatial, double scale);
+// times `scale`), laid out on the padded box of the plan's geometry or on `box`.
+int nearfield_extract(msc_plan* pl, const double2* Ks_spatial, double scale, const Geo* box = nullptr);
 // Upload the per-layer blocks after a change (synchronises the plan's stream; must not
 // run while a graph is being captured).
 int nearfield_refresh(msc_plan* pl);

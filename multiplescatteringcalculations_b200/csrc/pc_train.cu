@@ -343,6 +343,7 @@ struct Trainer {
   }
 
   int scale_from_blocks() {
+    MSC_TRY(nf_host_sync(pl));
     s = 0;
     for (const double2& v : pl->nf->g64) s = std::max(s, std::hypot(v.x, v.y));
     if (!(s > 0)) {
@@ -356,6 +357,7 @@ struct Trainer {
   template <typename T, typename P>
   int layers(const P* w, typename WType<T>::type* dst) {
     using WT = typename WType<T>::type;
+    MSC_TRY(nf_host_sync(pl));
     std::vector<WT> h((size_t)L * NF_OFFS * 81);
     for (int l = 0; l < L; ++l)
       for (int i = 0; i < NF_OFFS * 81; ++i) {
@@ -538,6 +540,7 @@ extern "C" {
 
 double msc_nearfield_scale(const msc_plan* pl) {
   if (!pl || !pl->nf || !pl->nf->ready) return 0.0;
+  if (nf_host_sync(pl) != MSC_OK) return 0.0;
   double s = 0;
   for (const double2& v : pl->nf->g64) s = std::max(s, std::hypot(v.x, v.y));
   return s;

@@ -80,6 +80,7 @@ struct msc_plan {
   msc::DBuf khat64, khat32;
   msc::DBuf va_blocks;     // [26][81] double
   msc::DBuf g0_scratch;    // [E][Lz][Ly][Lx] complex128, the spectrum build's work array
+  msc::DBuf g0_near;       // [E][27] spatial kernel within one cell of the origin (fused G0 build)
   // matvec workspace [9][Nz][Ly][Lx] (y and x transformed, z in space)
   msc::DBuf W64, W32;
   // boundary scratch: SoA copies of in/out fields

@@ -3,6 +3,7 @@
 #include <mutex>
 #include <algorithm>
 #include <cstring>
+#include <cstdlib>
 
 #include "physics.cuh"
 #include "mv_common.cuh"
@@ -364,6 +365,119 @@ __global__ void __launch_bounds__(128) k_g0_spatial_oct(double2* __restrict__ Ks
     }
 }
 
+// Aperiodic, mirror-symmetric kernels: the spatial evaluation fused with the x
+// transform, so the spatial box (377 MB at 64x64x16) is neither stored nor read back.
+// One block per row (z <= Lz/2, y <= Ly/2) of the octant; the E entries in groups of
+// G0X_EG lines. Thread x <= Lx/2 evaluates the row's point x (aperiodic: at most one
+// image) into a shared tile of Lx points and fills the mirror point Lx - x with the
+// entry's x-parity sign; the tile is transformed along x and kx < Hx is stored for the
+// row and for its y and z mirror rows, with the entry's y and z parity signs. Points
+// within one cell of the origin also go, with all their mirror images, to the 3x3x3 box
+// Kn[e][27] ((d + 3) % 3 per axis) from which the near-field blocks are taken.
+constexpr int G0X_EG = 16;
+constexpr int G0X_NT = 256;
+
+template <bool POW2>
+__global__ void __launch_bounds__(G0X_NT, 2) k_g0_x(double2* __restrict__ K, double2* __restrict__ Kn,
+                                                 const double* __restrict__ vab, G0Params p, FftPlan1D f,
+                                                 const double2* __restrict__ twg) {
+  const Geo& g = p.g;
+  constexpr int P = G0X_EG + 1;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int L = g.Lx;
+  double2* tw = reinterpret_cast<double2*>(smem_raw);
+  double2* ta = tw + L;
+  double2* tb = ta + (size_t)L * P;
+  __shared__ unsigned char ea[81], eb[81], epar[81];
+  const int tid = threadIdx.x;
+  const int y = blockIdx.x, z = blockIdx.y;
+  for (int t = tid; t < L; t += G0X_NT) tw[t] = twg[t];
+  if (tid < p.E) {
+    int a = tid / 9, b = tid % 9;
+    if (p.E == 45) {  // upper triangle, row by row
+      int e = tid;
+      a = 0;
+      while (e >= 9 - a) {
+        e -= 9 - a;
+        ++a;
+      }
+      b = a + e;
+    }
+    ea[tid] = (unsigned char)a;
+    eb[tid] = (unsigned char)b;
+    epar[tid] = (unsigned char)(dof_parity(a) ^ dof_parity(b));
+  }
+  const int x = tid, qx = L / 2 + 1;
+  int oz[2], ox[2], oy[2];
+  const int nz = axis_offsets(z, g.Lz, g.Nz, false, oz);
+  const int ny = axis_offsets(y, g.Ly, g.M, false, oy);
+  const int nx = x < qx ? axis_offsets(x, L, g.M, false, ox) : 0;
+  const bool has = nz == 1 && ny == 1 && nx == 1 && !(oz[0] == 0 && oy[0] == 0 && ox[0] == 0);
+  const int dz = has ? oz[0] : 0, dy = has ? oy[0] : 0, dx = has ? ox[0] : 0;
+  const bool va = has && p.va && abs(dz) <= 1 && abs(dx) <= 1 && abs(dy) <= 1;
+  const double* vb = va ? vab + va_slot(dz, dx, dy) * 81 : nullptr;
+  PointProp pp;
+  if (has && !va) pp.init(dz * p.d, dx * p.d, dy * p.d, p.omega, p.alpha, p.beta, p.rho);
+  const bool near = x < qx && x <= 1 && y <= 1 && z <= 1;
+  const int mx = (x == 0 || 2 * x == L) ? 1 : 2;
+  const int my = (y == 0 || 2 * y == g.Ly) ? 1 : 2;
+  const int mz = (z == 0 || 2 * z == g.Lz) ? 1 : 2;
+  __syncthreads();
+  for (int e0 = 0; e0 < p.E; e0 += G0X_EG) {
+    const int ne = min(G0X_EG, p.E - e0);
+    if (x < qx) {
+      for (int q = 0; q < ne; ++q) {
+        const int e = e0 + q;
+        double2 v = make_double2(0.0, 0.0);
+        if (has) {
+          const int a = ea[e], b = eb[e];
+          v = va ? make_double2(vb[a * 9 + b], 0.0) : pp.entry(a, b);
+          if (p.E == 45 && b >= 6) v = 2.0 * v;  // (K D)_ij = K_ij D_j
+          v = p.scale * v;
+        }
+        const int par = epar[e];
+        ta[x * P + q] = v;
+        if (mx == 2) {
+          const double sx = (par & 1) ? -1.0 : 1.0;
+          ta[(L - x) * P + q] = make_double2(sx * v.x, sx * v.y);
+        }
+        if (near)
+          for (int rz = 0; rz < (z ? 2 : 1); ++rz)
+            for (int ry = 0; ry < (y ? 2 : 1); ++ry)
+              for (int rx = 0; rx < (x ? 2 : 1); ++rx) {
+                const int fl = rx | (ry << 1) | (rz << 2);
+                const double sg = (__popc(par & fl) & 1) ? -1.0 : 1.0;
+                const int iz = rz ? 3 - z : z, iy = ry ? 3 - y : y, ix = rx ? 3 - x : x;  // (d + 3) % 3
+                Kn[(size_t)e * 27 + (iz % 3 * 3 + iy % 3) * 3 + ix % 3] = make_double2(sg * v.x, sg * v.y);
+              }
+      }
+    }
+    __syncthreads();
+    const double2* res = fft_tile<-1, POW2>(ta, tb, P, ne, f, tw, tid, G0X_NT);
+    for (int it = tid; it < ne * g.Hx; it += G0X_NT) {
+      const int q = it / g.Hx, k = it - q * g.Hx;
+      const int e = e0 + q, par = epar[e];
+      const double2 v = res[k * P + q];
+      for (int rz = 0; rz < mz; ++rz)
+        for (int ry = 0; ry < my; ++ry) {
+          const int zz = rz ? g.Lz - z : z, yy = ry ? g.Ly - y : y;
+          const double sg = ((((par >> 1) & 1) & ry) ^ (((par >> 2) & 1) & rz)) ? -1.0 : 1.0;
+          K[(((size_t)e * g.Lz + zz) * g.Ly + yy) * L + k] = make_double2(sg * v.x, sg * v.y);
+        }
+    }
+    __syncthreads();
+  }
+}
+
+// The G0 build fuses the spatial evaluation with the x pass where it applies, unless
+// MSC_G0_FUSED=0 (the unfused passes, kept for the kernels it does not cover).
+static bool g0_fused() {
+  const char* e = getenv("MSC_G0_FUSED");
+  return !(e && e[0] == '0');
+}
+
+static size_t g0x_smem(int L) { return sizeof(double2) * ((size_t)L + 2 * (size_t)L * (G0X_EG + 1)); }
+
 template <typename T>
 int launch_fft_strided(msc_plan* pl, const cx<T>* in, long long es, long long S1, long long S2, cx<T>* out,
                        long long eo, long long O1, long long O2, float2* out32, int ncol, int n1, int n2, int n_in,
@@ -452,25 +566,49 @@ int launch_g0(msc_plan* pl, double omega, const double* kpar, int va, int n_orde
   p.kx = kpar ? kpar[0] : 0.0;
   p.ky = kpar ? kpar[1] : 0.0;
   p.scale = 1.0 / ((double)g.Lz * g.Lx * g.Ly);
-  if (g.oct) {
-    const long long noct = (long long)(g.Lz / 2 + 1) * (g.Ly / 2 + 1) * (g.Lx / 2 + 1);
-    k_g0_spatial_oct<<<(unsigned)ceil_div(noct, 128), 128, 0, pl->stream>>>((double2*)ks.p,
-                                                                           (const double*)pl->va_blocks.p, p);
-  } else {
-    k_g0_spatial<<<(unsigned)ceil_div(npts, 128), 128, 0, pl->stream>>>((double2*)ks.p, (const double*)pl->va_blocks.p,
-                                                                        p);
-  }
-  ::msc::note_launch();
-  MSC_CUDA(cudaGetLastError());
   double2* K = (double2*)ks.p;
-  // near-field blocks for the preconditioner, before the transforms overwrite K
-  MSC_TRY(nearfield_extract(pl, K, p.scale));
   const double2* twxy = (const double2*)pl->tw64_xy.p;
   const double2* twz = (const double2*)pl->tw64_z.p;
   const long long plane = (long long)g.Ly * g.Lx, vol = (long long)g.Lz * plane;
-  // x pass (contiguous lines), in place; keep kx < Hx
-  int s = launch_fft_contig<double>(pl, K, K, (long long)E * g.Lz * g.Ly, (long long)E * g.Lz * g.Ly, 0, g.Lx, g.Lx,
-                                    g.Hx, pl->fxy, twxy, -1, nullptr);
+  int s = MSC_OK;
+  // aperiodic mirror-symmetric kernel: spatial evaluation fused with the x pass
+  const bool fused = g.oct && !p.periodic && g0_fused() && g.Lx >= 8 && g.Lx / 2 + 1 <= G0X_NT &&
+                     g0x_smem(g.Lx) <= 200 * 1024;
+  if (fused) {
+    MSC_TRY(dalloc(pl, pl->g0_near, sizeof(double2) * 81 * 27));
+    double2* Kn = (double2*)pl->g0_near.p;
+    const size_t sm = g0x_smem(g.Lx);
+    const dim3 grid((unsigned)(g.Ly / 2 + 1), (unsigned)(g.Lz / 2 + 1));
+    const double* vab = (const double*)pl->va_blocks.p;
+    const FftPlan1D& f = pl->fxy;
+#define CALL(P2)                                                                                 \
+  {                                                                                              \
+    MSC_CUDA(prep_kernel((const void*)k_g0_x<P2>));                                              \
+    k_g0_x<P2><<<grid, G0X_NT, sm, pl->stream>>>(K, Kn, vab, p, f, twxy);                        \
+  }
+    MSC_POW2_DISPATCH(f.pow2, CALL);
+#undef CALL
+    ::msc::note_launch();
+    MSC_CUDA(cudaGetLastError());
+    // near-field blocks from the 3x3x3 box
+    Geo box = g;
+    box.Lz = box.Ly = box.Lx = 3;
+    MSC_TRY(nearfield_extract(pl, Kn, p.scale, &box));
+  } else {
+    if (g.oct) {
+      const long long noct = (long long)(g.Lz / 2 + 1) * (g.Ly / 2 + 1) * (g.Lx / 2 + 1);
+      k_g0_spatial_oct<<<(unsigned)ceil_div(noct, 128), 128, 0, pl->stream>>>(K, (const double*)pl->va_blocks.p, p);
+    } else {
+      k_g0_spatial<<<(unsigned)ceil_div(npts, 128), 128, 0, pl->stream>>>(K, (const double*)pl->va_blocks.p, p);
+    }
+    ::msc::note_launch();
+    MSC_CUDA(cudaGetLastError());
+    // near-field blocks for the preconditioner, before the transforms overwrite K
+    MSC_TRY(nearfield_extract(pl, K, p.scale));
+    // x pass (contiguous lines), in place; keep kx < Hx
+    s = launch_fft_contig<double>(pl, K, K, (long long)E * g.Lz * g.Ly, (long long)E * g.Lz * g.Ly, 0, g.Lx, g.Lx,
+                                  g.Hx, pl->fxy, twxy, -1, nullptr);
+  }
   // y pass: axis stride Lx, columns kx < Hx, slabs (z, e); keep ky < Hy
   if (s == MSC_OK)
     s = launch_fft_strided<double>(pl, K, g.Lx, plane, vol, K, g.Lx, plane, vol, nullptr, g.Hx, g.Lz, E, g.Ly, g.Hy,
