@@ -135,10 +135,14 @@ int launch_fft_contig(msc_plan* pl, const cx<T>* in, cx<T>* out, long long nline
 template <typename T>
 int launch_t0_fft_y(msc_plan* pl, const cx<T>* x, const double* scale, cx<T>* W, const cx<T>* tw, const int* done,
                     int nrhs);
+// odd (two words, optional): mirror-symmetric input lines of length f.L stored for
+// idx < n_in = f.L/2 + 1 only; idx >= n_in is read as s in[f.L - idx], s = -1 when bit
+// blockIdx.z (the slab index s2, an entry of the G0 build) of the 128-bit mask is set.
 template <typename T>
 int launch_fft_strided(msc_plan* pl, const cx<T>* in, long long es, long long S1, long long S2, cx<T>* out,
                        long long eo, long long O1, long long O2, float2* out32, int ncol, int n1, int n2, int n_in,
-                       int n_out, const FftPlan1D& f, const cx<T>* tw, int dir, const int* done);
+                       int n_out, const FftPlan1D& f, const cx<T>* tw, int dir, const int* done,
+                       const unsigned long long* odd = nullptr);
 template <typename T>
 int launch_zbz(msc_plan* pl, cx<T>* W, const int* done, int nrhs);
 // the register form of the complex64 z pass (mv_zpass.cu); 1 = not applicable to the

@@ -11,11 +11,12 @@
 
 namespace msc {
 
-template <typename T, int DIR, bool POW2>
+template <typename T, int DIR, bool POW2, bool MIRROR>
 __global__ void __launch_bounds__(256, 3) k_fft_strided(const cx<T>* in, long long es, long long S1, long long S2,
                                                         cx<T>* out, long long eo, long long O1, long long O2,
                                                         float2* out32, int ncol, int TC, int n_in, int n_out,
-                                                        FftPlan1D pl, const cx<T>* __restrict__ twg, const int* done) {
+                                                        FftPlan1D pl, const cx<T>* __restrict__ twg, const int* done,
+                                                        unsigned long long odd_lo, unsigned long long odd_hi) {
   pdl_wait();
   pdl_trigger();
   if (done && *done) return;
@@ -32,9 +33,25 @@ __global__ void __launch_bounds__(256, 3) k_fft_strided(const cx<T>* in, long lo
   const long long ob = (long long)blockIdx.y * O1 + (long long)blockIdx.z * O2 + col0;
   for (int t = tid; t < pl.L; t += nthr) tw[t] = twg[t];
   {
+    // MIRROR: idx >= n_in is the sign-flipped (odd entry) or plain mirror L - idx
+    const int sl = blockIdx.z;
+    const bool odd = MIRROR && ((sl < 64 ? (odd_lo >> sl) : (odd_hi >> (sl - 64))) & 1ull);
     QR w(tid, nthr, TC);  // (idx, column)
-    for (int it = tid; it < TC * pl.L; it += nthr, w.next())
-      ta[w.q * P + w.r] = (w.r < nc && w.q < n_in) ? in[ib + (long long)w.q * es + w.r] : czero<C>();
+    for (int it = tid; it < TC * pl.L; it += nthr, w.next()) {
+      C v = czero<C>();
+      if (w.r < nc) {
+        if (w.q < n_in) {
+          v = in[ib + (long long)w.q * es + w.r];
+        } else if (MIRROR) {
+          v = in[ib + (long long)(pl.L - w.q) * es + w.r];
+          if (odd) {
+            v.x = -v.x;
+            v.y = -v.y;
+          }
+        }
+      }
+      ta[w.q * P + w.r] = v;
+    }
   }
   __syncthreads();
   const C* res = fft_tile<DIR, POW2>(ta, tb, P, TC, pl, tw, tid, nthr);
@@ -61,8 +78,14 @@ template <typename T> static int strided_columns(int L, int ncol) {
 template <typename T>
 int launch_fft_strided(msc_plan* pl, const cx<T>* in, long long es, long long S1, long long S2, cx<T>* out,
                        long long eo, long long O1, long long O2, float2* out32, int ncol, int n1, int n2, int n_in,
-                       int n_out, const FftPlan1D& f, const cx<T>* tw, int dir, const int* done) {
+                       int n_out, const FftPlan1D& f, const cx<T>* tw, int dir, const int* done,
+                       const unsigned long long* odd) {
   const int TC = strided_columns<T>(f.L, ncol);
+  if (odd && (n_in != f.L / 2 + 1 || n2 > 128)) {
+    set_error("mirrored strided FFT: %d stored inputs of %d, %d slabs", n_in, f.L, n2);
+    return MSC_ERR_UNSUPPORTED;
+  }
+  const unsigned long long olo = odd ? odd[0] : 0ull, ohi = odd ? odd[1] : 0ull;
   const int nthr = 256;
   if (TC > nthr) {
     set_error("strided FFT tile of %d columns exceeds the block", TC);
@@ -72,10 +95,11 @@ int launch_fft_strided(msc_plan* pl, const cx<T>* in, long long es, long long S1
   dim3 grid((unsigned)((ncol + TC - 1) / TC), (unsigned)n1, (unsigned)n2);
 #define CALL(P2)                                                                                              \
   {                                                                                                           \
-    auto kern = (dir < 0) ? k_fft_strided<T, -1, P2> : k_fft_strided<T, +1, P2>;                              \
+    auto kern = odd ? ((dir < 0) ? k_fft_strided<T, -1, P2, true> : k_fft_strided<T, +1, P2, true>)            \
+                    : ((dir < 0) ? k_fft_strided<T, -1, P2, false> : k_fft_strided<T, +1, P2, false>);         \
     MSC_CUDA(prep_kernel((const void*)kern));                                                                 \
     kern<<<grid, nthr, sm, pl->stream>>>(in, es, S1, S2, out, eo, O1, O2, out32, ncol, TC, n_in, n_out, f, tw, \
-                                         done);                                                               \
+                                         done, olo, ohi);                                                     \
     ::msc::note_launch();                                                                                     \
   }
   MSC_POW2_DISPATCH(f.pow2, CALL);
@@ -85,9 +109,10 @@ int launch_fft_strided(msc_plan* pl, const cx<T>* in, long long es, long long S1
 }
 template int launch_fft_strided<float>(msc_plan*, const float2*, long long, long long, long long, float2*, long long,
                                        long long, long long, float2*, int, int, int, int, int, const FftPlan1D&,
-                                       const float2*, int, const int*);
+                                       const float2*, int, const int*, const unsigned long long*);
 template int launch_fft_strided<double>(msc_plan*, const double2*, long long, long long, long long, double2*,
                                         long long, long long, long long, float2*, int, int, int, int, int,
-                                        const FftPlan1D&, const double2*, int, const int*);
+                                        const FftPlan1D&, const double2*, int, const int*,
+                                        const unsigned long long*);
 
 }  // namespace msc

@@ -370,10 +370,11 @@ __global__ void __launch_bounds__(128) k_g0_spatial_oct(double2* __restrict__ Ks
 // One block per row (z <= Lz/2, y <= Ly/2) of the octant; the E entries in groups of
 // G0X_EG lines. Thread x <= Lx/2 evaluates the row's point x (aperiodic: at most one
 // image) into a shared tile of Lx points and fills the mirror point Lx - x with the
-// entry's x-parity sign; the tile is transformed along x and kx < Hx is stored for the
-// row and for its y and z mirror rows, with the entry's y and z parity signs. Points
+// entry's x-parity sign; the tile is transformed along x and kx < Hx is stored. Points
 // within one cell of the origin also go, with all their mirror images, to the 3x3x3 box
-// Kn[e][27] ((d + 3) % 3 per axis) from which the near-field blocks are taken.
+// Kn[e][27] ((d + 3) % 3 per axis) from which the near-field blocks are taken. Only the
+// octant rows are stored: the y and z passes read the mirror rows' values through the
+// entries' parity signs (launch_fft_strided with a parity mask).
 constexpr int G0X_EG = 16;
 constexpr int G0X_NT = 256;
 
@@ -420,8 +421,6 @@ __global__ void __launch_bounds__(G0X_NT, 2) k_g0_x(double2* __restrict__ K, dou
   if (has && !va) pp.init(dz * p.d, dx * p.d, dy * p.d, p.omega, p.alpha, p.beta, p.rho);
   const bool near = x < qx && x <= 1 && y <= 1 && z <= 1;
   const int mx = (x == 0 || 2 * x == L) ? 1 : 2;
-  const int my = (y == 0 || 2 * y == g.Ly) ? 1 : 2;
-  const int mz = (z == 0 || 2 * z == g.Lz) ? 1 : 2;
   __syncthreads();
   for (int e0 = 0; e0 < p.E; e0 += G0X_EG) {
     const int ne = min(G0X_EG, p.E - e0);
@@ -456,14 +455,7 @@ __global__ void __launch_bounds__(G0X_NT, 2) k_g0_x(double2* __restrict__ K, dou
     const double2* res = fft_tile<-1, POW2>(ta, tb, P, ne, f, tw, tid, G0X_NT);
     for (int it = tid; it < ne * g.Hx; it += G0X_NT) {
       const int q = it / g.Hx, k = it - q * g.Hx;
-      const int e = e0 + q, par = epar[e];
-      const double2 v = res[k * P + q];
-      for (int rz = 0; rz < mz; ++rz)
-        for (int ry = 0; ry < my; ++ry) {
-          const int zz = rz ? g.Lz - z : z, yy = ry ? g.Ly - y : y;
-          const double sg = ((((par >> 1) & 1) & ry) ^ (((par >> 2) & 1) & rz)) ? -1.0 : 1.0;
-          K[(((size_t)e * g.Lz + zz) * g.Ly + yy) * L + k] = make_double2(sg * v.x, sg * v.y);
-        }
+      K[(((size_t)(e0 + q) * g.Lz + z) * g.Ly + y) * L + k] = res[k * P + q];
     }
     __syncthreads();
   }
@@ -477,11 +469,6 @@ static bool g0_fused() {
 }
 
 static size_t g0x_smem(int L) { return sizeof(double2) * ((size_t)L + 2 * (size_t)L * (G0X_EG + 1)); }
-
-template <typename T>
-int launch_fft_strided(msc_plan* pl, const cx<T>* in, long long es, long long S1, long long S2, cx<T>* out,
-                       long long eo, long long O1, long long O2, float2* out32, int ncol, int n1, int n2, int n_in,
-                       int n_out, const FftPlan1D& f, const cx<T>* tw, int dir, const int* done);
 
 // Copy the spectrum box kz < Hz, ky < Hy, kx < Hx of the transformed work array
 // K[e][z][y][x] into the stored layout of element type T (entries kent<T>): blocked slices of the
@@ -609,14 +596,24 @@ int launch_g0(msc_plan* pl, double omega, const double* kpar, int va, int n_orde
     s = launch_fft_contig<double>(pl, K, K, (long long)E * g.Lz * g.Ly, (long long)E * g.Lz * g.Ly, 0, g.Lx, g.Lx,
                                   g.Hx, pl->fxy, twxy, -1, nullptr);
   }
-  // y pass: axis stride Lx, columns kx < Hx, slabs (z, e); keep ky < Hy
+  // y pass: axis stride Lx, columns kx < Hx, slabs (z, e); keep ky < Hy. After k_g0_x
+  // only the octant rows are stored: slabs z <= Lz/2, inputs y <= Ly/2, the rest mirrored.
+  unsigned long long odd_y[2] = {0, 0}, odd_z[2] = {0, 0};
+  for (int a = 0, e = 0; a < 9; ++a)
+    for (int b = (E == 45 ? a : 0); b < 9; ++b, ++e) {
+      const int par = dof_parity(a) ^ dof_parity(b);
+      if (par & 2) odd_y[e >> 6] |= 1ull << (e & 63);
+      if (par & 4) odd_z[e >> 6] |= 1ull << (e & 63);
+    }
   if (s == MSC_OK)
-    s = launch_fft_strided<double>(pl, K, g.Lx, plane, vol, K, g.Lx, plane, vol, nullptr, g.Hx, g.Lz, E, g.Ly, g.Hy,
-                                   pl->fxy, twxy, -1, nullptr);
+    s = launch_fft_strided<double>(pl, K, g.Lx, plane, vol, K, g.Lx, plane, vol, nullptr, g.Hx,
+                                   fused ? g.Lz / 2 + 1 : g.Lz, E, fused ? g.Ly / 2 + 1 : g.Ly, g.Hy, pl->fxy, twxy,
+                                   -1, nullptr, fused ? odd_y : nullptr);
   // z pass: axis stride Ly*Lx, columns kx < Hx, slabs (ky < Hy, e); keep kz < Hz, in place
   if (s == MSC_OK)
-    s = launch_fft_strided<double>(pl, K, plane, g.Lx, vol, K, plane, g.Lx, vol, nullptr, g.Hx, g.Hy, E, g.Lz, g.Hz,
-                                   pl->fz, twz, -1, nullptr);
+    s = launch_fft_strided<double>(pl, K, plane, g.Lx, vol, K, plane, g.Lx, vol, nullptr, g.Hx, g.Hy, E,
+                                   fused ? g.Lz / 2 + 1 : g.Lz, g.Hz, pl->fz, twz, -1, nullptr,
+                                   fused ? odd_z : nullptr);
   // stored layouts of the fused z pass, complex128 and complex64
   if (s == MSC_OK) s = launch_khat_pack<double>(pl, K, (double2*)pl->khat64.p, E);
   if (s == MSC_OK) s = launch_khat_pack<float>(pl, K, (float2*)pl->khat32.p, E);
