@@ -16,7 +16,7 @@ namespace msc {
 __host__ __device__ constexpr int voigt_p(int a) { return a < 3 ? a : (a == 3 ? 1 : 0); }
 __host__ __device__ constexpr int voigt_q(int a) { return a < 3 ? a : (a == 3 ? 2 : (a == 4 ? 2 : 1)); }
 
-__device__ __forceinline__ double2 cmulr(double s, double2 a) { return make_double2(s * a.x, s * a.y); }
+__host__ __device__ __forceinline__ double2 cmulr(double s, double2 a) { return make_double2(s * a.x, s * a.y); }
 __device__ __forceinline__ double kd(int i, int j) { return i == j ? 1.0 : 0.0; }
 
 // ---------------------------------------------------------------------------
@@ -281,7 +281,9 @@ __host__ __device__ inline double2 cpow_i(double k, int m) {
   }
 }
 
-__device__ inline CubeConst cube_constants(double omega, double a, double alpha, double beta, double rho) {
+// Evaluated on the host once per T0 build (a serial FP64 recurrence that, run by one thread
+// per block, had dominated the T0 kernel) and passed to it by value.
+__host__ __device__ inline CubeConst cube_constants(double omega, double a, double alpha, double beta, double rho) {
   constexpr int N = 8;
   const double a0 = (alpha * alpha + beta * beta) / (8.0 * M_PI * rho * alpha * alpha * beta * beta);
   const double b0 = (alpha * alpha - beta * beta) / (8.0 * M_PI * rho * alpha * alpha * beta * beta);

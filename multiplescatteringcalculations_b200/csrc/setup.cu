@@ -79,10 +79,7 @@ int build_twiddles(msc_plan* pl) {
 // ---- T0 --------------------------------------------------------------------------------
 __global__ void k_t0(const double* __restrict__ dl, const double* __restrict__ dm, const double* __restrict__ dr,
                      double2* __restrict__ t64, float2* __restrict__ t32, int nsite, double omega, double a,
-                     double alpha, double beta, double rho) {
-  __shared__ CubeConst cc;
-  if (threadIdx.x == 0) cc = cube_constants(omega, a, alpha, beta, rho);
-  __syncthreads();
+                     CubeConst cc) {
   const int s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= nsite) return;
   double2 t[4];
@@ -98,9 +95,9 @@ int launch_t0(msc_plan* pl, const double* dlam, const double* dmu, const double*
   const Geo& g = pl->g;
   MSC_TRY(dalloc(pl, pl->t4_64, sizeof(double2) * 4 * g.nsite));
   MSC_TRY(dalloc(pl, pl->t4_32, sizeof(float2) * 4 * g.nsite));
+  const CubeConst cc = cube_constants(omega, pl->desc.a, pl->desc.alpha, pl->desc.beta, pl->desc.rho);
   k_t0<<<ceil_div(g.nsite, 256), 256, 0, pl->stream>>>(dlam, dmu, drho, (double2*)pl->t4_64.p, (float2*)pl->t4_32.p,
-                                                       g.nsite, omega, pl->desc.a, pl->desc.alpha, pl->desc.beta,
-                                                       pl->desc.rho); ::msc::note_launch();
+                                                       g.nsite, omega, pl->desc.a, cc); ::msc::note_launch();
   MSC_CUDA(cudaGetLastError());
   return MSC_OK;
 }
