@@ -344,43 +344,54 @@ __device__ __forceinline__ void fft_reg(C* v, const C* __restrict__ tw) {
 // transform every twiddle index is a compile-time constant, so each twiddle is a
 // constant-bank operand of the arithmetic instead of a load.
 extern __constant__ float2 c_tw256[256];
+extern __constant__ double2 c_tw256d[256];
 template <int L> __device__ __forceinline__ float2 ctw(int t) {
   static_assert(L >= 1 && L <= 256 && 256 % L == 0, "a power-of-two length up to 256");
   return c_tw256[t * (256 / L)];
 }
+template <int L> __device__ __forceinline__ double2 ctwd(int t) {
+  static_assert(L >= 1 && L <= 256 && 256 % L == 0, "a power-of-two length up to 256");
+  return c_tw256d[t * (256 / L)];
+}
+// the constant-table twiddle of the element type
+template <int L, typename C> __device__ __forceinline__ C ctw_t(int t) {
+  if constexpr (sizeof(C) == 8) return ctw<L>(t);
+  else return ctwd<L>(t);
+}
 
-template <int L, int S, int DIR>
-__device__ __forceinline__ void fft_reg_c_stages(float2* v) {
+template <int L, int S, int DIR, typename C>
+__device__ __forceinline__ void fft_reg_c_stages(C* v) {
   using PL = Pow2Plan<L>;
   if constexpr (S < PL::NSTAGES) {
     constexpr int R = PL::radix(S), NS = PL::ns(S), NB = L / R, TSTEP = L / (NS * R);
-    float2 out[L];
+    C out[L];
 #pragma unroll
     for (int j = 0; j < NB; ++j) {
       const int kk = j % NS;
-      float2 u[R];
+      C u[R];
 #pragma unroll
       for (int r = 0; r < R; ++r) u[r] = v[j + r * NB];
       if (kk != 0) {
 #pragma unroll
         for (int r = 1; r < R; ++r) {
-          float2 w = ctw<L>(r * kk * TSTEP);
+          C w = ctw_t<L, C>(r * kk * TSTEP);
           if (DIR > 0) w.y = -w.y;
           u[r] = u[r] * w;
         }
       }
-      Dft<R, DIR, float2>::run(u);
+      Dft<R, DIR, C>::run(u);
       const int idxD = (j - kk) * R + kk;
 #pragma unroll
       for (int r = 0; r < R; ++r) out[idxD + r * NS] = u[r];
     }
 #pragma unroll
     for (int i = 0; i < L; ++i) v[i] = out[i];
-    fft_reg_c_stages<L, S + 1, DIR>(v);
+    fft_reg_c_stages<L, S + 1, DIR, C>(v);
   }
 }
 
-// fft_reg with the twiddles from the constant table (complex64, L a power of two <= 256)
+// fft_reg with the twiddles from the constant tables (L a power of two <= 256)
 template <int L, int DIR> __device__ __forceinline__ void fft_reg_c(float2* v) { fft_reg_c_stages<L, 0, DIR>(v); }
+template <int L, int DIR> __device__ __forceinline__ void fft_reg_c(double2* v) { fft_reg_c_stages<L, 0, DIR>(v); }
 
 }  // namespace msc

@@ -145,9 +145,10 @@ int launch_fft_strided(msc_plan* pl, const cx<T>* in, long long es, long long S1
                        const unsigned long long* odd = nullptr);
 template <typename T>
 int launch_zbz(msc_plan* pl, cx<T>* W, const int* done, int nrhs);
-// the register form of the complex64 z pass (mv_zpass.cu); 1 = not applicable to the
+// the register form of the z pass (mv_zpass.cu); 1 = not applicable to the
 // plan's shape (nothing launched), else a status
-int launch_zpass(msc_plan* pl, float2* W, const int* done, int nrhs);
+template <typename T>
+int launch_zpass(msc_plan* pl, cx<T>* W, const int* done, int nrhs);
 template <typename T>
 int launch_fft_y_out(msc_plan* pl, const cx<T>* W, const cx<T>* x, const double* scale, cx<T>* y, const cx<T>* tw,
                      const int* done, int nrhs);

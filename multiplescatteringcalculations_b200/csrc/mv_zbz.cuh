@@ -289,8 +289,8 @@ int launch_zbz(msc_plan* pl, cx<T>* W, const int* done, int nrhs) {
     set_error("Lz=%d exceeds the shared memory of the fused z pass", g.Lz);
     return MSC_ERR_UNSUPPORTED;
   }
-  if constexpr (sizeof(T) == 4) {
-    const int r = launch_zpass(pl, W, done, nrhs);
+  {
+    const int r = launch_zpass<T>(pl, W, done, nrhs);
     if (r != 1) return r;
   }
   const bool sym = pl->E == 45;

@@ -32,9 +32,11 @@
 
 namespace msc {
 
-template <int LZ, int KX, int S, bool SYM> struct ZpCfg {
+template <typename T, int LZ, int KX, int S, bool SYM> struct ZpCfg {
+  using C = cx<T>;
   static_assert(S == 1 || S == 2, "one or two threads per line");
   static_assert(LZ >= 8 && LZ <= 64 && (LZ & (LZ - 1)) == 0, "power-of-two Lz");
+  static_assert(sizeof(T) == 4 || LZ / S <= 16, "complex128 lines of at most 16 points per thread");
   static constexpr int NC = 4 * KX;                   // column slots: 4 mirrors x KX
   static constexpr int NL = 9 * NC;                   // lines
   static constexpr int NT = ((S * NL + 31) / 32) * 32;
@@ -42,16 +44,19 @@ template <int LZ, int KX, int S, bool SYM> struct ZpCfg {
   static constexpr int HZ = LZ / 2 + 1;               // stored kz rows (octant)
   static constexpr int E = SYM ? 45 : 81;
   static constexpr int KE = E * HZ * KX;              // entries of a block's slice
-  static constexpr int CS = (KE + 1) / 2 * 2;         // the slice's stride in khat (zbz_layout)
-  // tile pitch: the S = 2 forward stores of a half warp cover rows k and k + 1 of 8
-  // lines; a pitch of 8 mod 16 elements puts them in disjoint banks
-  static constexpr int P = S == 1 ? NL : NL + (8 - NL % 16 + 16) % 16;
-  static constexpr size_t KBYTES = (size_t)8 * CS;
+  // the slice's stride in khat (zbz_layout: complex64 slices padded to 16 bytes)
+  static constexpr int CS = sizeof(T) == 4 ? (KE + 1) / 2 * 2 : KE;
+  // tile pitch: the complex64 S = 2 forward stores of a half warp cover rows k and k + 1
+  // of 8 lines; a pitch of 8 mod 16 elements puts them in disjoint banks (a complex128
+  // row of 8 lines already fills the 32 banks)
+  static constexpr int P = (S == 1 || sizeof(T) == 8) ? NL : NL + (8 - NL % 16 + 16) % 16;
+  static constexpr size_t ES = sizeof(C);
+  static constexpr size_t KBYTES = ES * CS;
   static constexpr size_t TW_OFF = (KBYTES + 15) / 16 * 16;
-  static constexpr size_t SMEM = TW_OFF + 8 * (size_t)LZ + 8 * (size_t)LZ * P;
+  static constexpr size_t SMEM = TW_OFF + ES * (size_t)LZ + ES * (size_t)LZ * P;
   static_assert(SMEM <= 227 * 1024 - 1024, "shared memory of one block");
   static constexpr int BLK_SMEM = (int)((228 * 1024) / (SMEM + 1024 + 16 * NC));
-  static constexpr int BLK_REG = 65536 / (NT * 96);
+  static constexpr int BLK_REG = 65536 / (NT * (sizeof(T) == 4 ? 96 : 128));
   static constexpr int AUTO = BLK_SMEM < BLK_REG ? BLK_SMEM : BLK_REG;
   static constexpr int MINB = AUTO < 1 ? 1 : AUTO;
 };
@@ -70,11 +75,12 @@ __device__ __forceinline__ bool zp_try_wait(uint32_t addr, uint32_t phase) {
   return ok != 0;
 }
 
-template <int LZ, int KX, int S, bool SYM>
-__global__ void __launch_bounds__(ZpCfg<LZ, KX, S, SYM>::NT, ZpCfg<LZ, KX, S, SYM>::MINB)
-    k_zpass(float2* __restrict__ W, const float2* __restrict__ khat, Geo g, int nxc, const float2* __restrict__ twg,
+template <typename T, int LZ, int KX, int S, bool SYM>
+__global__ void __launch_bounds__(ZpCfg<T, LZ, KX, S, SYM>::NT, ZpCfg<T, LZ, KX, S, SYM>::MINB)
+    k_zpass(cx<T>* __restrict__ W, const cx<T>* __restrict__ khat, Geo g, int nxc, const cx<T>* __restrict__ twg,
             const int* done, int nrhs, int* status, long long wait_limit) {
-  using Cf = ZpCfg<LZ, KX, S, SYM>;
+  using Cf = ZpCfg<T, LZ, KX, S, SYM>;
+  using C = cx<T>;
   constexpr int NC = Cf::NC, NL = Cf::NL, NT = Cf::NT, LH = Cf::LH, HZ = Cf::HZ, P = Cf::P;
   pdl_wait();
   pdl_trigger();
@@ -82,14 +88,14 @@ __global__ void __launch_bounds__(ZpCfg<LZ, KX, S, SYM>::NT, ZpCfg<LZ, KX, S, SY
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ int sq[NC];  // mirror flags of slot s (bit 0 kx, bit 1 ky), -1: slot unused
   __shared__ __align__(8) unsigned long long kbar;  // completion of the slice's bulk copy
-  float2* tw = reinterpret_cast<float2*>(smem_raw + Cf::TW_OFF);
-  float2* tile = tw + LZ;
+  C* tw = reinterpret_cast<C*>(smem_raw + Cf::TW_OFF);
+  C* tile = tw + LZ;
   const int tid = threadIdx.x;
   const long long plane = (long long)g.Ly * g.Lx;
   const long long cstride = (long long)g.Nz * plane;
   const int kyo = blockIdx.y;
   const int x0 = blockIdx.x * KX;
-  const float2* kblk = khat + ((long long)kyo * nxc + blockIdx.x) * Cf::CS;
+  const C* kblk = khat + ((long long)kyo * nxc + blockIdx.x) * Cf::CS;
   // the column of slot s: q = s / KX (mirror flags), kx_o = x0 + s % KX; -1 when the
   // mirror coincides with another slot's column or kx_o lies beyond the octant
   auto slot_col = [&](int s) -> long long {
@@ -115,26 +121,26 @@ __global__ void __launch_bounds__(ZpCfg<LZ, KX, S, SYM>::NT, ZpCfg<LZ, KX, S, SY
     // the slice: CS entries, 16-byte aligned at both ends (zbz_layout pads CS to even)
     asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(kbar_a) : "memory");
     asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(kbar_a), "r"((int)(8 * Cf::CS))
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(kbar_a), "r"((int)Cf::KBYTES)
                  : "memory");
     asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(
                      (uint32_t)__cvta_generic_to_shared(smem_raw)),
-                 "l"(kblk), "r"((int)(8 * Cf::CS)), "r"(kbar_a)
+                 "l"(kblk), "r"((int)Cf::KBYTES), "r"(kbar_a)
                  : "memory");
   }
   bool kready = false;
   for (int rh = 0; rh < nrhs; ++rh) {
     const long long o = o0 >= 0 ? o0 + (long long)rh * 9 * cstride : -1;
-    float2 v[LH];
+    C v[LH];
     // (1) the line's layers n < N_z <= Lz/2; the upper half of an S = 1 line is zero
 #pragma unroll
-    for (int n = 0; n < LH; ++n) v[n] = (n < LZ / 2 && o >= 0 && n < g.Nz) ? W[o + n * plane] : czero<float2>();
+    for (int n = 0; n < LH; ++n) v[n] = (n < LZ / 2 && o >= 0 && n < g.Nz) ? W[o + n * plane] : czero<C>();
     // the previous vector's inverse reads of the tile are done; the barrier's init visible
     __syncthreads();
     // (2) forward transform, rows kz = S m + b of the tile
     if (S == 2 && b) {
 #pragma unroll
-      for (int n = 0; n < LH; ++n) v[n] = v[n] * ctw<LZ>(n);
+      for (int n = 0; n < LH; ++n) v[n] = v[n] * ctw_t<LZ, C>(n);
     }
     fft_reg_c<LH, -1>(v);
     if (lact) {
@@ -163,13 +169,13 @@ __global__ void __launch_bounds__(ZpCfg<LZ, KX, S, SYM>::NT, ZpCfg<LZ, KX, S, SY
         const int f = q | (side << 2);
         const int kz = side ? LZ - kp : kp;
         const int ko = kp * KX + j;
-        float2* ra = tile + kz * P + s;
-        float2 t[9];
+        C* ra = tile + kz * P + s;
+        C t[9];
 #pragma unroll
         for (int c = 0; c < 9; ++c) t[c] = ra[c * NC];
         const unsigned sm = sign_mask(f);
         reflect_mask(t, sm);
-        const float2* k2 = reinterpret_cast<const float2*>(smem_raw) + ko;
+        const C* k2 = reinterpret_cast<const C*>(smem_raw) + ko;
         block_mul<SYM>([&](int e) { return k2[e * HZ * KX]; }, t);
         reflect_mask(t, sm);
 #pragma unroll
@@ -185,12 +191,12 @@ __global__ void __launch_bounds__(ZpCfg<LZ, KX, S, SYM>::NT, ZpCfg<LZ, KX, S, SY
       } else {
         // b = 0: X[k] + X[k + Lz/2]; b = 1: W^{-k} (X[k] - X[k + Lz/2]) (branch free:
         // the two threads of a line are adjacent lanes)
-        const float sg = b ? -1.f : 1.f;
+        const T sg = b ? (T)-1 : (T)1;
 #pragma unroll
         for (int k = 0; k < LH; ++k) {
-          const float2 a = tile[k * P + l], c = tile[(k + LH) * P + l];
-          const float2 w = b ? ctw<LZ>(k) : make_float2(1.f, 0.f);
-          v[k] = conj_mul(w, make_float2(fmaf(sg, c.x, a.x), fmaf(sg, c.y, a.y)));
+          const C a = tile[k * P + l], c = tile[(k + LH) * P + l];
+          const C w = b ? ctw_t<LZ, C>(k) : mk<T>((T)1, (T)0);
+          v[k] = conj_mul(w, mk<T>(fma(sg, c.x, a.x), fma(sg, c.y, a.y)));
         }
       }
       fft_reg_c<LH, +1>(v);

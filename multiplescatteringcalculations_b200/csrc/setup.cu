@@ -28,9 +28,10 @@ __global__ void k_twiddles(double2* t64, float2* t32, int L) {
 }
 
 __constant__ float2 c_tw256[256];
+__constant__ double2 c_tw256d[256];
 
-// Fill the constant twiddle table of the current device once (k_twiddles at L = 256 into a
-// scratch buffer, then a device-to-device copy to the symbol).
+// Fill the constant twiddle tables (complex64 and complex128) of the current device once
+// (k_twiddles at L = 256 into scratch buffers, then device-to-device copies to the symbols).
 static int ensure_const_twiddles(msc_plan* pl) {
   static std::mutex mu;
   static bool ready[64] = {};
@@ -51,6 +52,8 @@ static int ensure_const_twiddles(msc_plan* pl) {
     cudaError_t e = cudaGetLastError();
     if (e == cudaSuccess)
       e = cudaMemcpyToSymbolAsync(c_tw256, t32.p, sizeof(float2) * 256, 0, cudaMemcpyDeviceToDevice, pl->stream);
+    if (e == cudaSuccess)
+      e = cudaMemcpyToSymbolAsync(c_tw256d, t64.p, sizeof(double2) * 256, 0, cudaMemcpyDeviceToDevice, pl->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(pl->stream);
     if (e != cudaSuccess) {
       set_error("constant twiddle table: %s", cudaGetErrorString(e));
