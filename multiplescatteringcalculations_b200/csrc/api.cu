@@ -160,11 +160,22 @@ static int nice_length(int n) {
   }
 }
 
+int read_small(msc_plan* pl, const void* dev, void* out, size_t bytes) {
+  if (bytes > 64) {
+    set_error("internal: a small read of %zu bytes", bytes);
+    return MSC_ERR_STATE;
+  }
+  if (!pl->hpin) MSC_CUDA(cudaMallocHost(&pl->hpin, 64));
+  MSC_CUDA(cudaMemcpyAsync(pl->hpin, dev, bytes, cudaMemcpyDeviceToHost, pl->stream));
+  MSC_CUDA(cudaStreamSynchronize(pl->stream));
+  memcpy(out, pl->hpin, bytes);
+  return MSC_OK;
+}
+
 int read_status(msc_plan* pl, int* word) {
   *word = 0;
   if (!pl->status.p) return MSC_OK;
-  MSC_CUDA(cudaMemcpyAsync(word, pl->status.p, sizeof(int), cudaMemcpyDeviceToHost, pl->stream));
-  MSC_CUDA(cudaStreamSynchronize(pl->stream));
+  MSC_TRY(read_small(pl, pl->status.p, word, sizeof(int)));
   if (*word) MSC_CUDA(cudaMemsetAsync(pl->status.p, 0, sizeof(int), pl->stream));
   return MSC_OK;
 }
@@ -394,6 +405,7 @@ int msc_plan_destroy(msc_plan* pl) {
   if (pl->ev_in) cudaEventDestroy(pl->ev_in);
   if (pl->ev_out) cudaEventDestroy(pl->ev_out);
   if (pl->stream) cudaStreamDestroy(pl->stream);
+  if (pl->hpin) cudaFreeHost(pl->hpin);
   delete pl;
   return MSC_OK;
 }

@@ -51,6 +51,7 @@ struct GmresWork {
   DBuf hess;              // H[(m+1) x m], cs[m], sn[m], g[m+1], y[m], scale[m+1], h1[m+1], h2[m+1], nrm[2]
   DBuf part;              // partial sums [NB][33]
   GState* hstate = nullptr;  // pinned host mirror
+  double* hd = nullptr;      // pinned scalar readback
   cudaEvent_t ev[2] = {nullptr, nullptr};
   cudaEvent_t tev[2] = {nullptr, nullptr};  // timing of a cycle (preconditioner policy)
   // captured Arnoldi cycles, [precision][preconditioned]
@@ -693,6 +694,15 @@ static int maxpy(msc_plan* pl, GmresWork* gw, const cx<T>* V, int nv, const doub
   return MSC_OK;
 }
 
+// One FP64 scalar to the host through page-locked memory: into a pageable destination the
+// copy waits for the host's staging path with the device idle.
+static int read_scalar(msc_plan* pl, GmresWork* gw, const double* d, double* out) {
+  MSC_CUDA(cudaMemcpyAsync(gw->hd, d, sizeof(double), cudaMemcpyDeviceToHost, pl->stream));
+  MSC_CUDA(cudaStreamSynchronize(pl->stream));
+  *out = *gw->hd;
+  return MSC_OK;
+}
+
 template <typename T>
 static int resid_norm(msc_plan* pl, GmresWork* gw, const cx<T>* b, const cx<T>* ax, cx<T>* r, double* out_nrm2) {
   GState* st = (GState*)gw->state.p;
@@ -734,6 +744,7 @@ static int ensure_work(msc_plan* pl, int m) {
     MSC_TRY(dalloc(pl, gw->state, sizeof(GState)));
     MSC_CUDA(cudaMemsetAsync(gw->state.p, 0, sizeof(GState), pl->stream));
     MSC_CUDA(cudaMallocHost((void**)&gw->hstate, sizeof(GState) * 2));
+    MSC_CUDA(cudaMallocHost((void**)&gw->hd, sizeof(double) * 4));
     MSC_CUDA(cudaEventCreateWithFlags(&gw->ev[0], cudaEventDisableTiming));
     MSC_CUDA(cudaEventCreateWithFlags(&gw->ev[1], cudaEventDisableTiming));
     MSC_CUDA(cudaEventCreate(&gw->tev[0]));
@@ -748,6 +759,7 @@ void gmres_free(msc_plan* pl) {
   dfree(pl, gw->V32); dfree(pl, gw->V64); dfree(pl, gw->Z32); dfree(pl, gw->Z64); dfree(pl, gw->x64); dfree(pl, gw->r64); dfree(pl, gw->ax64);
   dfree(pl, gw->d32); dfree(pl, gw->r32); dfree(pl, gw->state); dfree(pl, gw->hess); dfree(pl, gw->part);
   if (gw->hstate) cudaFreeHost(gw->hstate);
+  if (gw->hd) cudaFreeHost(gw->hd);
   for (auto& row : gw->graph)
     for (auto& gr : row)
       if (gr.exec) cudaGraphExecDestroy(gr.exec);
@@ -1033,8 +1045,7 @@ static int solve_core(msc_plan* pl, const double2* b, double2* x, double bnorm, 
     s.n_matvec64 += 1;
     MSC_TRY(resid_norm<double>(pl, gw, b, ax, r, dn));
     double rn2 = 0;
-    MSC_CUDA(cudaMemcpyAsync(&rn2, dn, sizeof(double), cudaMemcpyDeviceToHost, pl->stream));
-    MSC_CUDA(cudaStreamSynchronize(pl->stream));
+    MSC_TRY(read_scalar(pl, gw, dn, &rn2));
     s.residual = std::sqrt(rn2) / bnorm;
     if (s.status != MSC_ERR_NONFINITE) s.status = s.residual <= tol ? MSC_OK : MSC_NOT_CONVERGED;
   } else {
@@ -1050,8 +1061,7 @@ static int solve_core(msc_plan* pl, const double2* b, double2* x, double bnorm, 
       ++s.n_matvec64;
       MSC_TRY(resid_norm<double>(pl, gw, b, ax, r, dn));
       double rn2 = 0;
-      MSC_CUDA(cudaMemcpyAsync(&rn2, dn, sizeof(double), cudaMemcpyDeviceToHost, pl->stream));
-      MSC_CUDA(cudaStreamSynchronize(pl->stream));
+      MSC_TRY(read_scalar(pl, gw, dn, &rn2));
       res = std::sqrt(rn2) / bnorm;
       if (!(res == res)) {
         s.status = MSC_ERR_NONFINITE;
@@ -1142,8 +1152,7 @@ int solve(msc_plan* pl, const double2* b_ref, double2* x_ref, const msc_solve_op
   double* dn = &h.nrm[1].x;
   MSC_TRY(resid_norm<double>(pl, gw, b, nullptr, nullptr, dn));
   double bn2 = 0;
-  MSC_CUDA(cudaMemcpyAsync(&bn2, dn, sizeof(double), cudaMemcpyDeviceToHost, pl->stream));
-  MSC_CUDA(cudaStreamSynchronize(pl->stream));
+  MSC_TRY(read_scalar(pl, gw, dn, &bn2));
   msc_solve_stats s{};
   MSC_TRY(solve_core(pl, b, x, std::sqrt(bn2), o->tol > 0 ? o->tol : 1e-6, o, s));
   // x back to the caller's layout (and physical frame)
@@ -1202,8 +1211,7 @@ int solve_multi(msc_plan* pl, int R, const double2* b_ref, double2* x_ref, const
     if (pl->bloch) MSC_TRY(bloch_modulate(pl, br, -1));
     MSC_TRY(norm2_n(pl, gw, br, nf, dn));
     double v = 0;
-    MSC_CUDA(cudaMemcpyAsync(&v, dn, sizeof(double), cudaMemcpyDeviceToHost, pl->stream));
-    MSC_CUDA(cudaStreamSynchronize(pl->stream));
+    MSC_TRY(read_scalar(pl, gw, dn, &v));
     bn[r] = std::sqrt(v);
     if (bn[r] > 0) {
       k_scale_field<<<nbk, NTH, 0, pl->stream>>>(br, nf, 1.0 / bn[r]);
@@ -1228,8 +1236,7 @@ int solve_multi(msc_plan* pl, int R, const double2* b_ref, double2* x_ref, const
   for (int r = 0; r < R; ++r) {
     MSC_TRY(norm2_n(pl, gw, res + (size_t)r * nf, nf, dn));
     double v = 0;
-    MSC_CUDA(cudaMemcpyAsync(&v, dn, sizeof(double), cudaMemcpyDeviceToHost, pl->stream));
-    MSC_CUDA(cudaStreamSynchronize(pl->stream));
+    MSC_TRY(read_scalar(pl, gw, dn, &v));
     rr[r] = bn[r] > 0 ? std::sqrt(v) : 0.0;
     double2* xr = x + (size_t)r * nf;
     k_scale_field<<<nbk, NTH, 0, pl->stream>>>(xr, nf, bn[r]);

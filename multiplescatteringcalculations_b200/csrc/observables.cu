@@ -127,8 +127,7 @@ int rpp_periodic(msc_plan* pl, const double2* psi, double omega, double p, int f
                                   (flags & MSC_RPP_PLANE_WAVE_MOMENT) ? 1 : 0, res); ::msc::note_launch();
   MSC_CUDA(cudaGetLastError());
   double2 h;
-  MSC_CUDA(cudaMemcpyAsync(&h, res, sizeof(double2), cudaMemcpyDeviceToHost, pl->stream));
-  MSC_CUDA(cudaStreamSynchronize(pl->stream));
+  MSC_TRY(read_small(pl, res, &h, sizeof(double2)));
   out[0] = h.x;
   out[1] = h.y;
   return MSC_OK;

@@ -62,6 +62,7 @@ struct msc_plan {
   cudaStream_t stream = nullptr;
   cudaStream_t user = nullptr;
   cudaEvent_t ev_in = nullptr, ev_out = nullptr;
+  void* hpin = nullptr;  // 64 page-locked bytes for small device-to-host reads
   int device = 0;
   msc::FftPlan1D fz, fxy;
   // twiddles exp(-2 pi i t / L) for Lz and Lxy
@@ -131,6 +132,10 @@ struct StreamFence {
 };
 
 int dalloc(msc_plan* pl, DBuf& b, size_t bytes);
+// Reads `bytes` (<= 64) from the device on the plan's stream into `out` through the plan's
+// page-locked scratch (a pageable destination makes the copy wait for the host's staging
+// path with the device idle); synchronises the stream.
+int read_small(msc_plan* pl, const void* dev, void* out, size_t bytes);
 void dfree(msc_plan* pl, DBuf& b);
 // stream-ordered allocation from the library's memory pool of `device`
 cudaError_t pool_alloc(void** p, size_t bytes, int device, cudaStream_t st);
