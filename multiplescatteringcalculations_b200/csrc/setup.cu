@@ -378,6 +378,17 @@ __global__ void __launch_bounds__(128) k_g0_spatial_oct(double2* __restrict__ Ks
 constexpr int G0X_EG = 16;
 constexpr int G0X_NT = 256;
 
+// A row point of k_g0_x: the propagator's per-point state (or the VA table slot), shared by
+// the threads that evaluate its entries. Padded to an odd number of 16-byte units (the
+// struct's alignment), which spreads consecutive points over the shared-memory banks.
+struct G0Pt {
+  PointProp pp;
+  int slot;  // VA table block (-1: the point propagator)
+  int has;   // the point has an image (aperiodic: at most one)
+  double pad[2];
+};
+static_assert(sizeof(G0Pt) % 16 == 0 && (sizeof(G0Pt) / 16) % 2 == 1, "odd stride in 16-byte units");
+
 template <bool POW2>
 __global__ void __launch_bounds__(G0X_NT, 2) k_g0_x(double2* __restrict__ K, double2* __restrict__ Kn,
                                                  const double* __restrict__ vab, G0Params p, FftPlan1D f,
@@ -389,9 +400,11 @@ __global__ void __launch_bounds__(G0X_NT, 2) k_g0_x(double2* __restrict__ K, dou
   double2* tw = reinterpret_cast<double2*>(smem_raw);
   double2* ta = tw + L;
   double2* tb = ta + (size_t)L * P;
+  G0Pt* pts = reinterpret_cast<G0Pt*>(tb + (size_t)L * P);
   __shared__ unsigned char ea[81], eb[81], epar[81];
   const int tid = threadIdx.x;
   const int y = blockIdx.x, z = blockIdx.y;
+  const int qx = L / 2 + 1;
   for (int t = tid; t < L; t += G0X_NT) tw[t] = twg[t];
   if (tid < p.E) {
     int a = tid / 9, b = tid % 9;
@@ -408,48 +421,55 @@ __global__ void __launch_bounds__(G0X_NT, 2) k_g0_x(double2* __restrict__ K, dou
     eb[tid] = (unsigned char)b;
     epar[tid] = (unsigned char)(dof_parity(a) ^ dof_parity(b));
   }
-  const int x = tid, qx = L / 2 + 1;
-  int oz[2], ox[2], oy[2];
-  const int nz = axis_offsets(z, g.Lz, g.Nz, false, oz);
-  const int ny = axis_offsets(y, g.Ly, g.M, false, oy);
-  const int nx = x < qx ? axis_offsets(x, L, g.M, false, ox) : 0;
-  const bool has = nz == 1 && ny == 1 && nx == 1 && !(oz[0] == 0 && oy[0] == 0 && ox[0] == 0);
-  const int dz = has ? oz[0] : 0, dy = has ? oy[0] : 0, dx = has ? ox[0] : 0;
-  const bool va = has && p.va && abs(dz) <= 1 && abs(dx) <= 1 && abs(dy) <= 1;
-  const double* vb = va ? vab + va_slot(dz, dx, dy) * 81 : nullptr;
-  PointProp pp;
-  if (has && !va) pp.init(dz * p.d, dx * p.d, dy * p.d, p.omega, p.alpha, p.beta, p.rho);
-  const bool near = x < qx && x <= 1 && y <= 1 && z <= 1;
-  const int mx = (x == 0 || 2 * x == L) ? 1 : 2;
+  // the row's points x <= Lx/2: one thread each sets up the point's propagator
+  {
+    int oz[2], oy[2];
+    const int nz = axis_offsets(z, g.Lz, g.Nz, false, oz);
+    const int ny = axis_offsets(y, g.Ly, g.M, false, oy);
+    for (int x = tid; x < qx; x += G0X_NT) {
+      int ox[2];
+      const int nx = axis_offsets(x, L, g.M, false, ox);
+      const bool has = nz == 1 && ny == 1 && nx == 1 && !(oz[0] == 0 && oy[0] == 0 && ox[0] == 0);
+      G0Pt& pt = pts[x];
+      pt.has = has ? 1 : 0;
+      pt.slot = -1;
+      if (has) {
+        const int dz = oz[0], dy = oy[0], dx = ox[0];
+        if (p.va && abs(dz) <= 1 && abs(dx) <= 1 && abs(dy) <= 1) pt.slot = va_slot(dz, dx, dy);
+        else pt.pp.init(dz * p.d, dx * p.d, dy * p.d, p.omega, p.alpha, p.beta, p.rho);
+      }
+    }
+  }
   __syncthreads();
   for (int e0 = 0; e0 < p.E; e0 += G0X_EG) {
     const int ne = min(G0X_EG, p.E - e0);
-    if (x < qx) {
-      for (int q = 0; q < ne; ++q) {
-        const int e = e0 + q;
-        double2 v = make_double2(0.0, 0.0);
-        if (has) {
-          const int a = ea[e], b = eb[e];
-          v = va ? make_double2(vb[a * 9 + b], 0.0) : pp.entry(a, b);
-          if (p.E == 45 && b >= 6) v = 2.0 * v;  // (K D)_ij = K_ij D_j
-          v = p.scale * v;
-        }
-        const int par = epar[e];
-        ta[x * P + q] = v;
-        if (mx == 2) {
-          const double sx = (par & 1) ? -1.0 : 1.0;
-          ta[(L - x) * P + q] = make_double2(sx * v.x, sx * v.y);
-        }
-        if (near)
-          for (int rz = 0; rz < (z ? 2 : 1); ++rz)
-            for (int ry = 0; ry < (y ? 2 : 1); ++ry)
-              for (int rx = 0; rx < (x ? 2 : 1); ++rx) {
-                const int fl = rx | (ry << 1) | (rz << 2);
-                const double sg = (__popc(par & fl) & 1) ? -1.0 : 1.0;
-                const int iz = rz ? 3 - z : z, iy = ry ? 3 - y : y, ix = rx ? 3 - x : x;  // (d + 3) % 3
-                Kn[(size_t)e * 27 + (iz % 3 * 3 + iy % 3) * 3 + ix % 3] = make_double2(sg * v.x, sg * v.y);
-              }
+    // every thread: (point, entry) items of the group, points fastest
+    for (int it = tid; it < qx * ne; it += G0X_NT) {
+      const int q = it / qx, x = it - q * qx;
+      const int e = e0 + q;
+      const G0Pt& pt = pts[x];
+      double2 v = make_double2(0.0, 0.0);
+      if (pt.has) {
+        const int a = ea[e], b = eb[e];
+        v = pt.slot >= 0 ? make_double2(vab[pt.slot * 81 + a * 9 + b], 0.0) : pt.pp.entry(a, b);
+        if (p.E == 45 && b >= 6) v = 2.0 * v;  // (K D)_ij = K_ij D_j
+        v = p.scale * v;
       }
+      const int par = epar[e];
+      ta[x * P + q] = v;
+      if (x != 0 && 2 * x != L) {
+        const double sx = (par & 1) ? -1.0 : 1.0;
+        ta[(L - x) * P + q] = make_double2(sx * v.x, sx * v.y);
+      }
+      if (x <= 1 && y <= 1 && z <= 1)
+        for (int rz = 0; rz < (z ? 2 : 1); ++rz)
+          for (int ry = 0; ry < (y ? 2 : 1); ++ry)
+            for (int rx = 0; rx < (x ? 2 : 1); ++rx) {
+              const int fl = rx | (ry << 1) | (rz << 2);
+              const double sg = (__popc(par & fl) & 1) ? -1.0 : 1.0;
+              const int iz = rz ? 3 - z : z, iy = ry ? 3 - y : y, ix = rx ? 3 - x : x;  // (d + 3) % 3
+              Kn[(size_t)e * 27 + (iz % 3 * 3 + iy % 3) * 3 + ix % 3] = make_double2(sg * v.x, sg * v.y);
+            }
     }
     __syncthreads();
     const double2* res = fft_tile<-1, POW2>(ta, tb, P, ne, f, tw, tid, G0X_NT);
@@ -468,7 +488,9 @@ static bool g0_fused() {
   return !(e && e[0] == '0');
 }
 
-static size_t g0x_smem(int L) { return sizeof(double2) * ((size_t)L + 2 * (size_t)L * (G0X_EG + 1)); }
+static size_t g0x_smem(int L) {
+  return sizeof(double2) * ((size_t)L + 2 * (size_t)L * (G0X_EG + 1)) + sizeof(G0Pt) * (size_t)(L / 2 + 1);
+}
 
 // Copy the spectrum box kz < Hz, ky < Hy, kx < Hx of the transformed work array
 // K[e][z][y][x] into the stored layout of element type T (entries kent<T>): blocked slices of the
