@@ -1,9 +1,8 @@
 """CPU restatement of the two-thread z-line transform of the register z pass
 (csrc/mv_zpass.cuh; complex64 at Lz = 64, complex128 at Lz = 32): each thread b of a line
-computes the outputs
-X[2m + b] as one Lz/2-point FFT of the twiddled input x[n] W^{nb} (the line holds data
-only at n < N_z <= Lz/2), and the inverse keeps the layers 2n + b from one Lz/2-point
-inverse FFT of W^{-bk} (X[k] + (-1)^b X[k + Lz/2]). Checked against the full
+computes the outputs X[2m + b] as one Lz/2-point FFT of the twiddled input x[n] W^{nb} (the
+line holds data only at n < N_z <= Lz/2), and the inverse keeps the layers 2n + b from one
+Lz/2-point inverse FFT of W^{-bk} (X[k] + (-1)^b X[k + Lz/2]). Checked against the full
 zero-padded transforms with numpy, with the kernel's own index arithmetic."""
 
 import numpy as np
